@@ -1,0 +1,477 @@
+#!/usr/bin/env python
+"""Benchmark of the GeoFLOW spectral-element hot path on B200.
+
+Headline workload (one GPU): the 3-d Helmholtz solve (alpha M + nu K) u = f
+on the unit cube, 32^3 hexahedral elements at p = 7 (16.8 M element-local
+nodes), homogeneous Dirichlet boundaries, alpha = nu = 1, right-hand side a
+seeded sum of 8 sinusoidal modes (wavenumbers 1..8, N(0,1) amplitudes),
+b = M_L f.  Jacobi-preconditioned CG to a relative residual of 1e-10
+(||r||_2 <= 1e-10 ||b||_2 on the assembled, masked residual).  One "step"
+is one complete solve from x = 0.  `value` is the time to solution of the
+mixed-precision path (FP32 operator applies, FP64 residual and iterative
+refinement) with inputs resident in HBM; the plain FP64 path is timed on
+the same problem and reported beside it.
+
+Also reported: RK-stage throughput (GDOF/s) of 3-d Burgers with SSP-RK3 on
+a periodic 64^3-element p = 5 box in FP32 and FP64, the roofline of the
+fused Helmholtz apply, an end-to-end solve through the host-buffer C ABI
+entry point, and the CPU oracle timed on a bounded sample.
+
+Usage: python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Multi-GPU (torchrun): every rank solves its own replica (the path does not
+partition across GPUs in this build); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GDOF/s per RK stage and CG time-to-1e-10: FP32+refine vs plain FP64, same B200"
+SEED = 20261203
+L2_BYTES = 126 * 2 ** 20
+# iterations the reference's FP64 Jacobi-PCG (the algorithm of GCG::solve_impl,
+# preconditioned) needs on the headline problem, as measured by the device
+# FP64 path of the same algorithm; used to project the CPU time to solution
+REF_ITERS_32_P7 = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ne", type=int, default=32)
+    ap.add_argument("--p", type=int, default=7)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--rk-ne", type=int, default=64)
+    ap.add_argument("--rk-p", type=int, default=5)
+    ap.add_argument("--no-rk", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample-ne", type=int, default=8)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms",
+                 "200", "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
+def rhs_modes(rng, nmodes=8):
+    k = rng.integers(1, 9, size=(nmodes, 3))
+    a = rng.standard_normal(nmodes)
+    return k, a
+
+
+def make_helmholtz_problem(ctx, ne, p):
+    import torch
+    from geoflow_b200 import GGFX, GMass, GridBox, Problem
+    g = GridBox(3, [ne] * 3, p)
+    prob = Problem(ctx, g)
+    rng = np.random.default_rng(SEED + 2)
+    k, a = rhs_modes(rng)
+    dev = ctx.torch_device
+    x, y, z = (torch.from_numpy(c).to(dev) for c in g.xyz)
+    f = torch.zeros_like(x)
+    for m in range(len(a)):
+        f += a[m] * torch.sin(np.pi * k[m, 0] * x) * torch.sin(np.pi * k[m, 1] * y) * \
+            torch.sin(np.pi * k[m, 2] * z)
+    del x, y, z
+    b = prob.zeros()
+    GMass(prob).opVec_prod(f, None, b)
+    return g, prob, b
+
+
+def time_solves(ctx, prob, H, b, traits, steps, warmup):
+    import torch
+    from geoflow_b200 import GCG
+    cg = GCG(traits, prob)
+    xb = prob.zeros()
+    x = prob.zeros()
+    for _ in range(warmup):
+        x.zero_()
+        rc = cg.solve(H, b, xb, x)
+    torch.cuda.synchronize()
+    times, iters = [], []
+    for _ in range(steps):
+        x.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        rc = cg.solve(H, b, xb, x)
+        e.record()
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e) / 1e3)
+        iters.append(cg.get_iteration_count())
+    return times, iters, rc, x
+
+
+def kernel_roofline(ctx, prob, peaks, reps=20):
+    """Average duration of the fused FP32 and FP64 3-d Helmholtz applies on
+    the headline grid, each launch timed alone after an L2 flush."""
+    import torch
+    from geoflow_b200 import _abi as A
+    lib = A.load()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=ctx.torch_device)
+    res = {}
+    g = prob.grid
+    for name, dt, code in (("f32", torch.float32, A.GF_F32), ("f64", torch.float64, A.GF_F64)):
+        u = torch.randn(prob.nlocal, dtype=dt, device=ctx.torch_device)
+        uo = torch.empty_like(u)
+        for _ in range(3):
+            ctx.check(lib.gf_helmholtz_apply(prob.handle, code, 1.0, None, 1.0, None, 1, A.ptr(u),
+                                             A.ptr(uo)))
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            ctx.check(lib.gf_helmholtz_apply(prob.handle, code, 1.0, None, 1.0, None, 1, A.ptr(u),
+                                             A.ptr(uo)))
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e) / 1e3)
+        t = statistics.mean(ts)
+        s_ = 4 if dt == torch.float32 else 8
+        alg = prob.nlocal * 2 * s_ + g.nelems * (3 + 1) * s_
+        res[name] = {"ms": t * 1e3, "alg_bytes": alg, "gbs": alg / t / 1e9,
+                     "gdofs": prob.nlocal / t / 1e9}
+    return res
+
+
+def dss_timing(ctx, prob, reps=10):
+    import torch
+    from geoflow_b200 import _abi as A
+    lib = A.load()
+    out = {}
+    for name, dt, code in (("f32", torch.float32, A.GF_F32), ("f64", torch.float64, A.GF_F64)):
+        u = torch.randn(prob.nlocal, dtype=dt, device=ctx.torch_device)
+        ctx.check(lib.gf_dss(prob.handle, code, A.GF_DSS_SUM, A.ptr(u)))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            ctx.check(lib.gf_dss(prob.handle, code, A.GF_DSS_SUM, A.ptr(u)))
+        e.record()
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e) / 1e3 / reps
+        s_ = 4 if dt == torch.float32 else 8
+        alg = prob.nlocal * (2 * s_ + 4) + prob.grid.nclass * 4
+        out[name] = {"ms": t * 1e3, "gbs": alg / t / 1e9}
+    return out
+
+
+def e2e_solve(ctx, prob, H, b, traits, reps=2):
+    """Solve through gf_cg_solve_host with pinned host buffers."""
+    import ctypes as C
+    import torch
+    from geoflow_b200 import _abi as A
+    lib = A.load()
+    bh = b.cpu().pin_memory()
+    xh = torch.zeros_like(bh).pin_memory()
+    xbh = torch.zeros_like(bh).pin_memory()
+    tr = traits.to_c()
+    P = A.P_double
+    times = []
+    for i in range(reps + 1):
+        xh.zero_()
+        it, rn = C.c_int(), C.c_double()
+        t0 = time.perf_counter()
+        rc = lib.gf_cg_solve_host(prob.handle, C.byref(tr), 1.0, 1.0, 1,
+                                  C.cast(bh.data_ptr(), P), C.cast(xbh.data_ptr(), P),
+                                  C.cast(xh.data_ptr(), P), C.byref(it), C.byref(rn))
+        t1 = time.perf_counter()
+        ctx.check(rc, "gf_cg_solve_host")
+        if i > 0:
+            times.append(t1 - t0)
+    n = prob.nlocal * 8
+    return statistics.mean(times), 3 * n, n
+
+
+# ---------------------------------------------------------------------------
+def rk_stage_bench(ctx, ne, p, steps=3, warmup=2):
+    """SSP-RK3 Burgers on a periodic box; returns GDOF/s per stage."""
+    import torch
+    from geoflow_b200 import GBurgers, GridBox, Problem
+    from geoflow_b200 import _abi as A
+    g = GridBox(3, [ne] * 3, p, length=[2 * np.pi] * 3, periodic=[1, 1, 1])
+    prob = Problem(ctx, g, dirichlet_mask=False)
+    dev = ctx.torch_device
+    rng = np.random.default_rng(SEED + 3)
+    x, y, z = (torch.from_numpy(c).to(dev) for c in g.xyz)
+    u = [torch.zeros_like(x) for _ in range(3)]
+    # random Fourier modes 1 <= |k| <= 6, amplitude |k|^(-5/3), random phases
+    # and directions, zero mean (4 modes per integer shell)
+    for kk in range(1, 7):
+        for _ in range(4):
+            kv = rng.standard_normal(3)
+            kv = np.round(kv / np.linalg.norm(kv) * kk).astype(int)
+            if not kv.any():
+                kv[0] = kk
+            amp = np.linalg.norm(kv) ** (-5.0 / 3.0)
+            ph = rng.uniform(0, 2 * np.pi)
+            d = rng.standard_normal(3)
+            arg = kv[0] * x + kv[1] * y + kv[2] * z + ph
+            s = torch.sin(arg)
+            for c in range(3):
+                u[c] += amp * d[c] * s
+    del x, y, z
+    umax = max(float(t.abs().max()) for t in u)
+    h = 2 * np.pi / ne
+    xi = g.xi
+    hmin = h * 0.5 * (xi[1] - xi[0])
+    dt_cfl = 0.3 * hmin / (p * p * umax)
+    out = {"workload": f"3d Burgers, periodic {ne}^3 elements p={p}, SSP-RK3, nu=1e-3",
+           "n_local": prob.nlocal, "dt": dt_cfl}
+    for name, dtp in (("f32", torch.float32), ("f64", torch.float64)):
+        uu = [t.to(dtp).contiguous() for t in u]
+        B = GBurgers(prob, GBurgers.BURGERS, 1e-3, scheme=A.GF_SSP33)
+        for _ in range(warmup):
+            B.step(uu, None, dt=dt_cfl, nsteps=1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        B.step(uu, None, dt=dt_cfl, nsteps=steps)
+        e.record()
+        torch.cuda.synchronize()
+        t_stage = s.elapsed_time(e) / 1e3 / (3 * steps)
+        out[name] = {"ms_per_stage": t_stage * 1e3,
+                     "gdofs_per_stage": 3 * prob.nlocal / t_stage / 1e9}
+        del uu
+    prob.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+def cpu_oracle_iteration_time(sample_ne, p, iters=6):
+    """Seconds per FP64 Jacobi-PCG iteration of the CPU oracle (a plain-C
+    restatement of GCG::solve_impl + GHelmholtz::reg_prod + GGFX::doOp) on a
+    sample box of sample_ne^3 elements, per element-local node."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    g = O.OracleBox(3, [sample_ne] * 3, p)
+    rng = np.random.default_rng(SEED + 2)
+    b = g.mass * rng.standard_normal(g.N)
+    dinv = 1.0 / g.helmholtz_diag(1.0, np.ones(g.N))
+    q = np.ones(g.N)
+    zb = np.zeros(g.N)
+    t0 = time.perf_counter()
+    g.cg_solve(b, np.zeros(g.N), p=1.0, q_vec=q, xb=zb, maxit=1, tol=0.0, dinv=dinv)
+    t1 = time.perf_counter()
+    g.cg_solve(b, np.zeros(g.N), p=1.0, q_vec=q, xb=zb, maxit=1 + iters, tol=0.0, dinv=dinv)
+    t2 = time.perf_counter()
+    per_iter = ((t2 - t1) - (t1 - t0)) / iters
+    return per_iter / g.N, g.N, (t2 - t0)
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    # bounded samples: each step times CG iterations of the oracle on a
+    # sample box and projects to the full problem per node
+    n_full = (args.ne ** 3) * (args.p + 1) ** 3
+    per_node = []
+    for _ in range(args.warmup):
+        cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, iters=2)
+    nsample = 0
+    for _ in range(args.steps):
+        t, nsample, _w = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, iters=3)
+        per_node.append(t)
+    t_iter = statistics.mean(per_node) * n_full
+    iters = REF_ITERS_32_P7 if (args.ne, args.p) == (32, 7) and REF_ITERS_32_P7 else None
+    value = t_iter * iters if iters else None
+    cfg = {"workload": f"3d Helmholtz (M+K)u=f, unit cube {args.ne}^3 hex p={args.p}, Dirichlet, "
+                       f"Jacobi-PCG to {args.tol:g} relative residual",
+           "n_local": n_full}
+    sample = (f"oracle FP64 Jacobi-PCG iterations on a {args.cpu_sample_ne}^3-element p={args.p} "
+              f"sub-box ({nsample} nodes), per node scaled to {n_full} nodes"
+              + (f", times {iters} iterations to 1e-10" if iters else ""))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": value * 1e3 if value else None, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfg, "seconds_per_cg_iteration": t_iter,
+            "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    from geoflow_b200 import CGTraits, Context, GHelmholtz
+    from geoflow_b200 import _abi as A
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ctx = Context(local)
+    peaks = measured_peaks()
+    g, prob, b = make_helmholtz_problem(ctx, args.ne, args.p)
+    H = GHelmholtz(prob)
+    H.set_Lap_scalar(1.0)
+    H.set_mass_scalar(1.0)
+    common = dict(maxit=50000, normtype=A.GF_NORM_EUC, tol=args.tol, precond=A.GF_PRECOND_JACOBI,
+                  check_every=32, relative=1)
+    tr_mix = CGTraits(precision=A.GF_CG_MIXED, inner_tol=1e-5, max_refine=60, **common)
+    tr_64 = CGTraits(precision=A.GF_CG_FP64, **common)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if ws == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=ctx.torch_device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up of both paths, then the timed region of the headline (mixed)
+    launches0 = C_stats(prob)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    t_mix, it_mix, rc_mix, x_mix = time_solves(ctx, prob, H, b, tr_mix, args.steps, args.warmup)
+    barrier()
+    clk = clocks.stop()
+    launches = C_stats(prob) - launches0
+    per_step_launches = launches // (args.steps + args.warmup)
+    t_64, it_64, rc_64, x_64 = time_solves(ctx, prob, H, b, tr_64, args.steps, min(args.warmup, 1))
+    value = max_over_ranks(statistics.mean(t_mix))
+    t64 = max_over_ranks(statistics.mean(t_64))
+    diff = float((x_mix - x_64).abs().max() / x_64.abs().max())
+    roof = kernel_roofline(ctx, prob, peaks)
+    dss = dss_timing(ctx, prob)
+    e2e_t, h2d, d2h = e2e_solve(ctx, prob, H, b, tr_mix)
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    rk = None
+    if not args.no_rk:
+        rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        t_node, nsample, wall = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p)
+        t_cpu = t_node * prob.nlocal * statistics.mean(it_64)
+        cpu = {"value": t_cpu, "unit": "s", "cores": 1, "kind": "port",
+               "sample": (f"oracle FP64 Jacobi-PCG iterations on a {args.cpu_sample_ne}^3-element "
+                          f"p={args.p} sub-box ({nsample} nodes, {wall:.1f} s of CPU work), "
+                          f"per node scaled to {prob.nlocal} nodes and {int(statistics.mean(it_64))} "
+                          f"iterations (the FP64 iteration count)")}
+    f32 = roof["f32"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": (f"3d Helmholtz (M+K)u=f, unit cube {args.ne}^3 hex p={args.p}, "
+                                f"Dirichlet, Jacobi-PCG to {args.tol:g} relative residual, "
+                                "FP32 applies + FP64 refinement"),
+                   "n_local": prob.nlocal, "n_unique": g.nclass, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (16.8M-node vectors); apply timings flush L2"},
+        "fp64_plain": {"value": t64, "unit": "s", "iterations": it_64[-1]},
+        "mixed": {"iterations": it_mix[-1], "rc": rc_mix},
+        "speedup_mixed_vs_fp64": t64 / value,
+        "solution_rel_diff_mixed_vs_fp64": diff,
+        "cg_gdofs_mixed": prob.nlocal * it_mix[-1] / value / 1e9,
+        "roofline": {"kernel": f"k_helm3d<float,{args.p + 1}> (fused Helmholtz apply)",
+                     "bound": "hbm", "achieved": f32["gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": f32["gbs"] / hbm, "peak_source": peak_src,
+                     "alg_bytes_per_launch": f32["alg_bytes"], "ms_per_launch": f32["ms"],
+                     "traffic": None},
+        "kernels": {"helm3d": roof, "dss_sum": dss},
+        "rk_stage": rk,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": per_step_launches * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def C_stats(prob):
+    import ctypes as C
+    from geoflow_b200 import _abi as A
+    v = C.c_int64()
+    A.load().gf_problem_stats(prob.handle, C.byref(v))
+    return v.value
+
+
+if __name__ == "__main__":
+    main()

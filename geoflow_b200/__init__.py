@@ -1,0 +1,12 @@
+"""geoflow_b200 -- B200-native (sm_100a) GeoFLOW spectral-element hot path.
+
+The compute lives in libgfgpu.so (C ABI, include/gfgpu.h); this package is
+the Python host-side mirror of the reference interfaces over that ABI.
+"""
+from . import _abi
+from ._abi import GFError, load
+from .sem import (CGTraits, Context, GBurgers, GCG, GGFX, GHelmholtz, GMass, GridBox, Problem,
+                  gll_basis)
+
+__all__ = ["GFError", "load", "CGTraits", "Context", "GBurgers", "GCG", "GGFX", "GHelmholtz",
+           "GMass", "GridBox", "Problem", "gll_basis", "_abi"]

@@ -1,0 +1,347 @@
+// api_rk.cu -- explicit Runge-Kutta steps of GExRKStepper
+// (pdes/gexrk_stepper.ipp) on the GBurgers right-hand side, with the DSS
+// Smooth calls exactly where the reference places them:
+//   Butcher step_b (1)  (gexrk_stepper.ipp:252-341), tableau of
+//                       GButcherRK::computeCoeffs (gbutcherrk.ipp:69-125)
+//   SSP22 / SSP33 / SSP34 (gexrk_stepper.ipp:533-780), step_euler (809-819)
+// and GBurgers::step_impl (gburgers.ipp:275-333): uold = u; step(uold -> u).
+//
+// Per stage: one fused element kernel for the RHS (k_dudt*), one class
+// kernel for Smooth, and elementwise stage combinations.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "gf_common.cuh"
+#include "k_dss.cuh"
+#include "k_vec.cuh"
+#include "ops_launch.cuh"
+#include "rk_common.cuh"
+
+using namespace gfk;
+
+namespace gfrk {
+
+void butcher(int order, double *alpha, double beta[4][4], double *c) {
+  std::memset(beta, 0, sizeof(double) * 16);
+  for (int i = 0; i < 4; i++) alpha[i] = c[i] = 0.0;
+  if (order == 1) {
+    c[0] = 1.0;
+  } else if (order == 2) {
+    c[0] = 0.5;
+    alpha[1] = 1.0;
+    c[1] = 0.5;
+    beta[1][0] = 1.0;
+  } else if (order == 3) {
+    c[0] = 0.25;
+    alpha[1] = 1.0 / 3.0;
+    c[1] = 0.0;
+    alpha[2] = 2.0 / 3.0;
+    c[2] = 0.75;
+    beta[1][0] = 1.0 / 3.0;
+    beta[2][1] = 2.0 / 3.0;
+  } else {
+    c[0] = 1.0 / 6.0;
+    alpha[1] = 0.5;
+    c[1] = 1.0 / 3.0;
+    alpha[2] = 0.5;
+    c[2] = 1.0 / 3.0;
+    alpha[3] = 1.0;
+    c[3] = 1.0 / 6.0;
+    beta[1][0] = 0.5;
+    beta[2][1] = 0.5;
+    beta[3][2] = 1.0;
+  }
+}
+
+// y = uin + ((0 + b0 K0) + b1 K1 + ...)   (isum accumulation of step_b)
+template <typename T>
+__global__ void k_stage_sum(int64_t n, const T *__restrict__ uin, int nk, const T *__restrict__ K0,
+                            const T *__restrict__ K1, const T *__restrict__ K2, T b0, T b1, T b2,
+                            T *__restrict__ y) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T s = T(0);
+    if (nk > 0) s = T(1) * s + b0 * K0[i];
+    if (nk > 1) s = T(1) * s + b1 * K1[i];
+    if (nk > 2) s = T(1) * s + b2 * K2[i];
+    T v = uin[i];
+    v += s;
+    y[i] = v;
+  }
+}
+
+// uout += K * ch
+template <typename T>
+__global__ void k_accum(int64_t n, const T *__restrict__ K, T ch, T *__restrict__ uout) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T s = K[i];
+    s *= ch;
+    uout[i] += s;
+  }
+}
+
+// x = dt*x + 1*uin (step_euler), then x = a*x + b*y (saxpby) when a != 1 || y
+template <typename T>
+__global__ void k_euler(int64_t n, T *__restrict__ x, T dt, const T *__restrict__ uin, T a,
+                        const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T v = dt * x[i] + T(1) * uin[i];
+    if (y) v = a * v + b * y[i];
+    if (y2) v = a2 * v + b2 * y2[i];
+    x[i] = v;
+  }
+}
+
+template <typename T>
+int Stepper<T>::rhs(T *const *u, T *const *K) {
+  const T *f[4] = {nullptr, nullptr, nullptr, nullptr};
+  T *o[3] = {nullptr, nullptr, nullptr};
+  if (eqn == GF_EQN_ADVECT) {
+    f[0] = u[0];
+    for (int k = 0; k < prob->dim; k++) f[1 + k] = c[k];
+    o[0] = K[0];
+    return launch_dudt<T>(prob, eqn, 0, nu, f, o, st);
+  }
+  if (eqn == GF_EQN_HEAT) {
+    for (int k = 0; k < nstate; k++) {
+      const T *fk[4] = {u[k], nullptr, nullptr, nullptr};
+      T *ok[3] = {K[k], nullptr, nullptr};
+      int rc = launch_dudt<T>(prob, eqn, 0, nu, fk, ok, st);
+      if (rc) return rc;
+    }
+    return GF_OK;
+  }
+  for (int k = 0; k < prob->dim; k++) {
+    f[k] = u[k];
+    o[k] = K[k];
+  }
+  return launch_dudt<T>(prob, eqn, 0, nu, f, o, st);
+}
+
+template <typename T>
+void Stepper<T>::smooth(T *v) {
+  launch_dss<T>(prob, GF_DSS_SMOOTH, v, st);
+}
+
+template <typename T>
+bool Stepper<T>::alloc() {
+  const size_t bytes = sizeof(T) * n;
+  int slot = 30 + (sizeof(T) == 8 ? 0 : 20);
+  for (int k = 0; k < nstate; k++) {
+    uold[k] = (T *)gf_work(prob, slot++, bytes);
+    utmp[k] = (T *)gf_work(prob, slot++, bytes);
+    for (int j = 0; j < 3; j++) K[j][k] = (T *)gf_work(prob, slot++, bytes);
+    if (!uold[k] || !utmp[k] || !K[0][k] || !K[1][k] || !K[2][k]) return false;
+  }
+  return true;
+}
+
+// One step uin -> uout (uout may not alias uin).
+template <typename T>
+int Stepper<T>::step(T *const *uin, T *const *uout, T dt) {
+  const unsigned g = grid_for(n, 256, prob->ctx->sm_count * 8);
+  int rc;
+  if (scheme >= 1 && scheme <= 4) {
+    double alpha[4], beta[4][4], cc[4];
+    butcher(scheme, alpha, beta, cc);
+    const int ns = scheme;
+    const T h = dt;
+    for (int k = 0; k < nstate; k++)
+      cudaMemcpyAsync(uout[k], uin[k], sizeof(T) * n, cudaMemcpyDeviceToDevice, st);
+    for (int m = 0; m < ns - 1; m++) {
+      for (int k = 0; k < nstate; k++) {
+        prob->launches++;
+        k_stage_sum<T><<<g, 256, 0, st>>>(n, uin[k], m, K[0][k], K[1][k], K[2][k],
+                                          (T)beta[m][0] * h, (T)beta[m][1] * h,
+                                          (T)beta[m][2] * h, utmp[k]);
+      }
+      if ((rc = rhs(utmp, K[m]))) return rc;
+      for (int k = 0; k < nstate; k++) {
+        smooth(K[m][k]);
+        prob->launches++;
+        k_accum<T><<<g, 256, 0, st>>>(n, K[m][k], (T)cc[m] * h, uout[k]);
+      }
+    }
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_stage_sum<T><<<g, 256, 0, st>>>(n, uin[k], ns - 1, K[0][k], K[1][k], K[2][k],
+                                        (T)beta[ns - 1][0] * h, (T)beta[ns - 1][1] * h,
+                                        (T)beta[ns - 1][2] * h, utmp[k]);
+      smooth(utmp[k]);
+    }
+    // the final stage result goes to the last K slot (K[0] in the
+    // reference, whose earlier content is no longer needed)
+    T *const *Kf = K[0];
+    if ((rc = rhs(utmp, Kf))) return rc;
+    for (int k = 0; k < nstate; k++) smooth(Kf[k]);
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_accum<T><<<g, 256, 0, st>>>(n, Kf[k], (T)cc[ns - 1] * h, uout[k]);
+      smooth(uout[k]);
+    }
+    return GF_OK;
+  }
+  const T one = T(1);
+  if (scheme == GF_SSP22) {
+    if ((rc = rhs(uin, K[0]))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
+      smooth(K[0][k]);
+    }
+    if ((rc = rhs(K[0], uout))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, uout[k], dt, K[0][k], T(0.5), uin[k], T(0.5), one, nullptr,
+                                    T(0));
+      smooth(uout[k]);
+    }
+    return GF_OK;
+  }
+  if (scheme == GF_SSP33) {
+    if ((rc = rhs(uin, K[0]))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
+      smooth(K[0][k]);
+    }
+    if ((rc = rhs(K[0], K[1]))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, K[1][k], dt, K[0][k], T(0.25), uin[k], T(0.75), one,
+                                    nullptr, T(0));
+      smooth(K[1][k]);
+    }
+    if ((rc = rhs(K[1], uout))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, uout[k], dt, K[1][k], T(2.0 / 3.0), uin[k], T(1.0 / 3.0),
+                                    one, nullptr, T(0));
+      smooth(uout[k]);
+    }
+    return GF_OK;
+  }
+  if (scheme == GF_SSP34) {
+    if ((rc = rhs(uin, K[0]))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, K[0][k], dt, uin[k], T(0.5), uin[k], T(0.5), one, nullptr,
+                                    T(0));
+      smooth(K[0][k]);
+    }
+    if ((rc = rhs(K[0], K[1]))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, K[1][k], dt, K[0][k], T(0.5), K[0][k], T(0.5), one, nullptr,
+                                    T(0));
+      smooth(K[1][k]);
+    }
+    if ((rc = rhs(K[1], K[2]))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, K[2][k], dt, K[1][k], T(1.0 / 6.0), K[1][k], T(1.0 / 6.0),
+                                    one, uin[k], T(2.0 / 3.0));
+      smooth(K[2][k]);
+    }
+    if ((rc = rhs(K[2], uout))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      prob->launches++;
+      k_euler<T><<<g, 256, 0, st>>>(n, uout[k], dt, K[2][k], T(0.5), K[2][k], T(0.5), one, nullptr,
+                                    T(0));
+      smooth(uout[k]);
+    }
+    return GF_OK;
+  }
+  return GF_ERR_ARG;
+}
+
+template struct Stepper<double>;
+template struct Stepper<float>;
+
+int check_traits(gf_problem *prob, const gf_rk_traits *tr, const void *const *u, const void *const *c) {
+  gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, tr && u, "traits and u are required");
+  GF_REQUIRE(ctx, tr->eqn == GF_EQN_ADVECT || tr->eqn == GF_EQN_BURGERS || tr->eqn == GF_EQN_HEAT,
+             "unknown equation %d", tr->eqn);
+  const int s = tr->scheme;
+  GF_REQUIRE(ctx, (s >= 1 && s <= 4) || s == GF_SSP22 || s == GF_SSP33 || s == GF_SSP34,
+             "unknown RK scheme %d", s);
+  if (tr->eqn == GF_EQN_BURGERS)
+    GF_REQUIRE(ctx, tr->nstate == prob->dim, "Burgers evolves dim components");
+  else if (tr->eqn == GF_EQN_ADVECT)
+    GF_REQUIRE(ctx, tr->nstate == 1 && c, "pure advection: one component and dim velocities");
+  else
+    GF_REQUIRE(ctx, tr->nstate >= 1 && tr->nstate <= 3, "heat: 1..3 components");
+  for (int k = 0; k < tr->nstate; k++) GF_REQUIRE(ctx, u[k], "state component %d missing", k);
+  if (tr->eqn == GF_EQN_ADVECT)
+    for (int k = 0; k < prob->dim; k++) GF_REQUIRE(ctx, c[k], "velocity component %d missing", k);
+  return GF_OK;
+}
+
+template <typename T>
+int advance(gf_problem *prob, const gf_rk_traits *tr, void *const *u, const void *const *c,
+            double dt, int nsteps) {
+  gf_context *ctx = prob->ctx;
+  Stepper<T> S(prob, tr, c);
+  if (!S.alloc()) return gf_fail(ctx, GF_ERR_NOMEM, "RK work allocation failed");
+  T *uu[3] = {nullptr, nullptr, nullptr};
+  for (int k = 0; k < tr->nstate; k++) uu[k] = (T *)u[k];
+  for (int s = 0; s < nsteps; s++) {
+    for (int k = 0; k < tr->nstate; k++)
+      cudaMemcpyAsync(S.uold[k], uu[k], sizeof(T) * S.n, cudaMemcpyDeviceToDevice, S.st);
+    int rc = S.step(S.uold, uu, (T)dt);
+    if (rc) return gf_fail(ctx, rc, "RK step failed");
+  }
+  GF_CHECK_LAUNCH(ctx);
+  return GF_OK;
+}
+
+}  // namespace gfrk
+
+using namespace gfrk;
+
+extern "C" int gf_rk_advance(gf_problem_t prob, int dtype, const gf_rk_traits *tr, void *const *u,
+                             const void *const *c, double t0, double dt, int nsteps) {
+  if (!prob) return GF_ERR_ARG;
+  (void)t0;
+  int rc = check_traits(prob, tr, (const void *const *)u, c);
+  if (rc) return rc;
+  GF_REQUIRE(prob->ctx, nsteps >= 0, "nsteps must be >= 0");
+  if (dtype == GF_F64) return advance<double>(prob, tr, u, c, dt, nsteps);
+  if (dtype == GF_F32) return advance<float>(prob, tr, u, c, dt, nsteps);
+  return gf_fail(prob->ctx, GF_ERR_ARG, "unknown dtype %d", dtype);
+}
+
+extern "C" int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *tr,
+                                  void *const *u, const void *const *c, double t0, double dt,
+                                  int nsteps) {
+  if (!prob) return GF_ERR_ARG;
+  gf_context *ctx = prob->ctx;
+  int rc = check_traits(prob, tr, (const void *const *)u, c);
+  if (rc) return rc;
+  const size_t bytes = (dtype == GF_F64 ? 8 : 4) * (size_t)prob->nlocal;
+  void *du[3] = {nullptr, nullptr, nullptr};
+  const void *dc[3] = {nullptr, nullptr, nullptr};
+  for (int k = 0; k < tr->nstate; k++) {
+    du[k] = gf_work(prob, 90 + k, bytes);
+    if (!du[k]) return gf_fail(ctx, GF_ERR_NOMEM, "staging allocation failed");
+    GF_CUDA(ctx, cudaMemcpyAsync(du[k], u[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (tr->eqn == GF_EQN_ADVECT) {
+    for (int k = 0; k < prob->dim; k++) {
+      void *d = gf_work(prob, 93 + k, bytes);
+      if (!d) return gf_fail(ctx, GF_ERR_NOMEM, "staging allocation failed");
+      GF_CUDA(ctx, cudaMemcpyAsync(d, c[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
+      dc[k] = d;
+    }
+  }
+  rc = gf_rk_advance(prob, dtype, tr, du, dc, t0, dt, nsteps);
+  if (rc) return rc;
+  for (int k = 0; k < tr->nstate; k++)
+    GF_CUDA(ctx, cudaMemcpyAsync(u[k], du[k], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GF_OK;
+}

@@ -1,0 +1,235 @@
+// k_dudt.cuh -- fused right-hand side of GBurgers::dudt_impl
+// (pdes/gburgers.ipp:203-257) and GAdvect::apply (sem/gadvect.ipp:58-100).
+//
+// Per element and per evolved component u_k, one pass computes
+//   adv_k  = M sum_j c_j (dXidX_j D_j u_k)            (GAdvect::apply)
+//   L u_k  = nu sum_j D_j^T (M G_jj D_j u_k)           (GHelmholtz, p = nu)
+//   dudt_k = Minv (-L u_k - adv_k)                     (saxpby + GMass inverse)
+// with c = prescribed velocity (pure advection), c = u (Burgers) or no
+// advection (heat).  The reference gradient D_j u_k is computed once and
+// shared by the advection and the diffusion terms.  Fields are staged in
+// shared memory and contracted line by line as in k_tensor.cuh.
+#pragma once
+#include "k_tensor.cuh"
+
+namespace gfk {
+
+enum { MODE_DUDT = 0, MODE_ADVECT = 1 };
+
+template <int N, int NF> constexpr int epb_dudt3() {
+  return (160 / (N * N)) < 1 ? 1 : (160 / (N * N));
+}
+
+// fields[0..NF): ADVECT: {p, c0, c1, c2}; BURGERS: {u0, u1, u2}; HEAT: {u}.
+// Evolved components: ADVECT/HEAT: field 0; BURGERS: fields 0..2.
+template <typename T, int N, int EPB, int EQN, int MODE>
+__global__ void __launch_bounds__(N *N *EPB)
+    k_dudt3d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T nu,
+             const T *__restrict__ f0, const T *__restrict__ f1, const T *__restrict__ f2,
+             const T *__restrict__ f3, const T *__restrict__ imass, T *__restrict__ o0,
+             T *__restrict__ o1, T *__restrict__ o2) {
+  constexpr int NF = EQN == GF_EQN_ADVECT ? 4 : (EQN == GF_EQN_BURGERS ? 3 : 1);
+  constexpr int NC = EQN == GF_EQN_BURGERS ? 3 : 1;  // evolved components
+  constexpr int P = Pad<N>::P, PLANE = N * P, VOL = N * PLANE, NN = N * N, NNN = N * N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *s = reinterpret_cast<T *>(smem_raw) + threadIdx.y * (NF + 2) * VOL;
+  T *sdx = s + NF * VOL, *sdy = s + (NF + 1) * VOL;
+  const int t = threadIdx.x;
+  const int64_t e = (int64_t)blockIdx.x * EPB + threadIdx.y;
+  const bool active = e < ne;
+  const int a0 = t % N, a1 = t / N;
+  const int64_t base = e * NNN;
+  const T *fin[4] = {f0, f1, f2, f3};
+  T *fout[3] = {o0, o1, o2};
+
+  NodeGeom<T, 3> eg;
+  eg.X[0] = eg.X[1] = eg.X[2] = eg.J = T(0);
+  if (active) elem_geom<T, 3>(g, e, eg);
+
+#pragma unroll
+  for (int f = 0; f < NF; f++) {
+#pragma unroll
+    for (int k = 0; k < N; k++)
+      s[f * VOL + k * PLANE + a1 * P + a0] = active ? fin[f][base + k * NN + t] : T(0);
+  }
+  __syncthreads();
+
+#pragma unroll 1
+  for (int c = 0; c < NC; c++) {
+    const T *su = s + c * VOL;
+    // x-lines (j=a0,k=a1) and y-lines (i=a0,k=a1): reference gradients
+    {
+      T a[N], d[N];
+#pragma unroll
+      for (int m = 0; m < N; m++) a[m] = su[a1 * PLANE + a0 * P + m];
+      line_D<T, N>(B.D, a, d);
+#pragma unroll
+      for (int i = 0; i < N; i++) sdx[a1 * PLANE + a0 * P + i] = d[i];
+#pragma unroll
+      for (int m = 0; m < N; m++) a[m] = su[a1 * PLANE + m * P + a0];
+      line_D<T, N>(B.D, a, d);
+#pragma unroll
+      for (int j = 0; j < N; j++) sdy[a1 * PLANE + j * P + a0] = d[j];
+    }
+    // z-line (i=a0, j=a1)
+    T rz[N], radv[N];
+    {
+      T a[N];
+#pragma unroll
+      for (int m = 0; m < N; m++) a[m] = su[m * PLANE + a1 * P + a0];
+      line_D<T, N>(B.D, a, rz);
+    }
+    __syncthreads();
+    {
+      const int i = a0, j = a1;
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        const int sidx = k * PLANE + j * P + i;
+        NodeGeom<T, 3> ng = eg;
+        if (active) node_geom<T, 3>(g, base + k * NN + j * N + i, ng);
+        const T mass = B.W[k] * B.W[j] * B.W[i] * ng.J;
+        if (EQN != GF_EQN_HEAT) {
+          const int cb = EQN == GF_EQN_ADVECT ? 1 : 0;
+          T po = (sdx[sidx] * ng.X[0]) * s[(cb + 0) * VOL + sidx];
+          po += (sdy[sidx] * ng.X[1]) * s[(cb + 1) * VOL + sidx];
+          po += (rz[k] * ng.X[2]) * s[(cb + 2) * VOL + sidx];
+          radv[k] = po * mass;
+        } else {
+          radv[k] = T(0);
+        }
+        rz[k] = mass * (rz[k] * (ng.X[2] * ng.X[2]));
+      }
+    }
+    if (MODE == MODE_ADVECT) {
+      if (active) {
+#pragma unroll
+        for (int k = 0; k < N; k++) fout[c][base + k * NN + a1 * N + a0] = radv[k];
+      }
+      __syncthreads();
+      continue;
+    }
+    __syncthreads();
+    // x-lines of Dx^T (M G0 dx), in place
+    {
+      const int j = a0, k = a1;
+      T a[N], d[N];
+#pragma unroll
+      for (int m = 0; m < N; m++) {
+        NodeGeom<T, 3> ng = eg;
+        if (active) node_geom<T, 3>(g, base + k * NN + j * N + m, ng);
+        const T mass = B.W[k] * B.W[j] * B.W[m] * ng.J;
+        a[m] = mass * (sdx[k * PLANE + j * P + m] * (ng.X[0] * ng.X[0]));
+      }
+      line_DT<T, N>(B.D, a, d);
+#pragma unroll
+      for (int i = 0; i < N; i++) sdx[k * PLANE + j * P + i] = d[i];
+    }
+    // y-lines of Dy^T (M G1 dy), in place
+    {
+      const int i = a0, k = a1;
+      T a[N], d[N];
+#pragma unroll
+      for (int m = 0; m < N; m++) {
+        NodeGeom<T, 3> ng = eg;
+        if (active) node_geom<T, 3>(g, base + k * NN + m * N + i, ng);
+        const T mass = B.W[k] * B.W[m] * B.W[i] * ng.J;
+        a[m] = mass * (sdy[k * PLANE + m * P + i] * (ng.X[1] * ng.X[1]));
+      }
+      line_DT<T, N>(B.D, a, d);
+#pragma unroll
+      for (int j = 0; j < N; j++) sdy[k * PLANE + j * P + i] = d[j];
+    }
+    __syncthreads();
+    {
+      const int i = a0, j = a1;
+      T d[N];
+      line_DT<T, N>(B.D, rz, d);
+      if (active) {
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          const int sidx = k * PLANE + j * P + i;
+          const int64_t node = base + k * NN + j * N + i;
+          T L = (sdx[sidx] + sdy[sidx]) + d[k];
+          if (nu != T(1)) L *= nu;
+          T rhs = T(-1) * L + T(-1) * radv[k];
+          fout[c][node] = imass[node] * rhs;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// 2-d variant, one thread per node.
+template <typename T, int N, int EPB, int EQN, int MODE>
+__global__ void __launch_bounds__(N *N *EPB)
+    k_dudt2d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T nu,
+             const T *__restrict__ f0, const T *__restrict__ f1, const T *__restrict__ f2,
+             const T *__restrict__ f3, const T *__restrict__ imass, T *__restrict__ o0,
+             T *__restrict__ o1, T *__restrict__ o2) {
+  constexpr int NF = EQN == GF_EQN_ADVECT ? 3 : (EQN == GF_EQN_BURGERS ? 2 : 1);
+  constexpr int NC = EQN == GF_EQN_BURGERS ? 2 : 1;
+  constexpr int P = Pad<N>::P, AREA = N * P, NN = N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *s = reinterpret_cast<T *>(smem_raw) + threadIdx.y * (NF + 2) * AREA;
+  T *sgx = s + NF * AREA, *sgy = s + (NF + 1) * AREA;
+  const int t = threadIdx.x;
+  const int64_t e = (int64_t)blockIdx.x * EPB + threadIdx.y;
+  const bool active = e < ne;
+  const int i = t % N, j = t / N;
+  const int64_t node = e * NN + t;
+  const T *fin[3] = {f0, f1, f2};
+  T *fout[2] = {o0, o1};
+  (void)f3;
+  NodeGeom<T, 2> ng;
+  ng.X[0] = ng.X[1] = ng.J = T(0);
+  if (active) {
+    elem_geom<T, 2>(g, e, ng);
+    node_geom<T, 2>(g, node, ng);
+  }
+#pragma unroll
+  for (int f = 0; f < NF; f++) s[f * AREA + j * P + i] = active ? fin[f][node] : T(0);
+  const T mass = B.W[j] * B.W[i] * ng.J;
+  __syncthreads();
+#pragma unroll 1
+  for (int c = 0; c < NC; c++) {
+    const T *su = s + c * AREA;
+    T dx = B.D[i] * su[j * P];
+    T dy = B.D[j] * su[i];
+#pragma unroll
+    for (int m = 1; m < N; m++) {
+      dx = fma(B.D[i + m * N], su[j * P + m], dx);
+      dy = fma(B.D[j + m * N], su[m * P + i], dy);
+    }
+    T adv = T(0);
+    if (EQN != GF_EQN_HEAT) {
+      const int cb = EQN == GF_EQN_ADVECT ? 1 : 0;
+      T po = (dx * ng.X[0]) * s[(cb + 0) * AREA + j * P + i];
+      po += (dy * ng.X[1]) * s[(cb + 1) * AREA + j * P + i];
+      adv = po * mass;
+    }
+    if (MODE == MODE_ADVECT) {
+      if (active) fout[c][node] = adv;
+      continue;
+    }
+    sgx[j * P + i] = mass * (dx * (ng.X[0] * ng.X[0]));
+    sgy[j * P + i] = mass * (dy * (ng.X[1] * ng.X[1]));
+    __syncthreads();
+    T ox = B.D[i * N] * sgx[j * P];
+    T oy = B.D[j * N] * sgy[i];
+#pragma unroll
+    for (int m = 1; m < N; m++) {
+      ox = fma(B.D[m + i * N], sgx[j * P + m], ox);
+      oy = fma(B.D[m + j * N], sgy[m * P + i], oy);
+    }
+    __syncthreads();
+    if (active) {
+      T L = ox + oy;
+      if (nu != T(1)) L *= nu;
+      T rhs = T(-1) * L + T(-1) * adv;
+      fout[c][node] = imass[node] * rhs;
+    }
+  }
+}
+
+}  // namespace gfk

@@ -1,0 +1,143 @@
+// ops_launch.cuh -- host launchers for the per-order kernel templates,
+// selected at run time by dispatch_n over the GLL point count.
+#pragma once
+#include <unordered_map>
+
+#include "gf_common.cuh"
+#include "k_dudt.cuh"
+#include "k_tensor.cuh"
+
+namespace gfk {
+
+// Raises a kernel's dynamic shared-memory limit once per kernel (several
+// kernels share one function type, so the record is keyed by address).
+template <typename K>
+inline void set_smem(K kern, size_t bytes) {
+  static std::unordered_map<const void *, size_t> done;
+  size_t &have = done[(const void *)kern];
+  if (bytes > have) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    have = bytes;
+  }
+}
+
+template <typename T>
+struct HelmLaunch {
+  template <int N>
+  struct F {
+    static int run(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
+                   const T *u, T *uo, cudaStream_t st, const double *stop) {
+      const Basis<T, N> B = make_basis<T, N>(prob);
+      const Geom<T> g = geom_of<T>(prob);
+      constexpr int P = Pad<N>::P;
+      if (prob->dim == 3) {
+        constexpr int EPB = epb3<N>();
+        const size_t smem = sizeof(T) * 3 * N * N * P * EPB;
+        auto kern = k_helm3d<T, N, EPB>;
+        set_smem(kern, smem);
+        const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+        prob->launches++;
+        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, p, pvec, q, qvec, use_mass, u, uo, stop);
+      } else {
+        constexpr int EPB = epb2<N>();
+        const size_t smem = sizeof(T) * 3 * N * P * EPB;
+        auto kern = k_helm2d<T, N, EPB>;
+        set_smem(kern, smem);
+        const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+        prob->launches++;
+        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, p, pvec, q, qvec, use_mass, u, uo, stop);
+      }
+      return GF_OK;
+    }
+  };
+};
+
+template <typename T>
+struct DerivLaunch {
+  template <int N>
+  struct F {
+    static int run(gf_problem *prob, const T *u, int idir, int dotrans, int phys, int accum, T *du,
+                   cudaStream_t st) {
+      const Basis<T, N> B = make_basis<T, N>(prob);
+      const Geom<T> g = geom_of<T>(prob);
+      if (prob->dim == 3) {
+        const size_t smem = sizeof(T) * N * N * N;
+        auto kern = k_grefderiv<T, N, 3, 1>;
+        set_smem(kern, smem);
+        prob->launches++;
+        kern<<<(unsigned)prob->ne, dim3(N * N, 1), smem, st>>>(B, g, prob->ne, u, idir, dotrans,
+                                                                phys, accum, du);
+      } else {
+        constexpr int EPB = epb2<N>();
+        const size_t smem = sizeof(T) * N * N * EPB;
+        auto kern = k_grefderiv<T, N, 2, EPB>;
+        set_smem(kern, smem);
+        const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+        prob->launches++;
+        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, u, idir, dotrans, phys, accum, du);
+      }
+      return GF_OK;
+    }
+  };
+};
+
+template <typename T, int N, int EQN, int MODE>
+inline void launch_dudt_kernel(gf_problem *prob, T nu, const T *const *f, T *const *o,
+                               const T *imass, cudaStream_t st) {
+  const Basis<T, N> B = make_basis<T, N>(prob);
+  const Geom<T> g = geom_of<T>(prob);
+  constexpr int P = Pad<N>::P;
+  if (prob->dim == 3) {
+    constexpr int NF = EQN == GF_EQN_ADVECT ? 4 : (EQN == GF_EQN_BURGERS ? 3 : 1);
+    constexpr int EPB = epb_dudt3<N, NF>();
+    const size_t smem = sizeof(T) * (NF + 2) * N * N * P * EPB;
+    auto kern = k_dudt3d<T, N, EPB, EQN, MODE>;
+    set_smem(kern, smem);
+    const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+    prob->launches++;
+    kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, nu, f[0], f[1], f[2], f[3], imass,
+                                                o[0], o[1], o[2]);
+  } else {
+    constexpr int NF = EQN == GF_EQN_ADVECT ? 3 : (EQN == GF_EQN_BURGERS ? 2 : 1);
+    constexpr int EPB = epb2<N>();
+    const size_t smem = sizeof(T) * (NF + 2) * N * P * EPB;
+    auto kern = k_dudt2d<T, N, EPB, EQN, MODE>;
+    set_smem(kern, smem);
+    const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+    prob->launches++;
+    kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, nu, f[0], f[1], f[2], f[3], imass,
+                                                o[0], o[1], o[2]);
+  }
+}
+
+template <typename T>
+struct DudtLaunch {
+  template <int N>
+  struct F {
+    static int run(gf_problem *prob, int eqn, int mode, T nu, const T *const *f, T *const *o,
+                   cudaStream_t st) {
+      const T *im = imass_of<T>(prob);
+      if (eqn == GF_EQN_ADVECT && mode == MODE_ADVECT)
+        launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_ADVECT>(prob, nu, f, o, im, st);
+      else if (eqn == GF_EQN_ADVECT)
+        launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_DUDT>(prob, nu, f, o, im, st);
+      else if (eqn == GF_EQN_BURGERS)
+        launch_dudt_kernel<T, N, GF_EQN_BURGERS, MODE_DUDT>(prob, nu, f, o, im, st);
+      else
+        launch_dudt_kernel<T, N, GF_EQN_HEAT, MODE_DUDT>(prob, nu, f, o, im, st);
+      return GF_OK;
+    }
+  };
+};
+
+}  // namespace gfk
+
+// launchers shared across translation units
+template <typename T>
+int launch_helm(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
+                const T *u, T *uo, cudaStream_t st, const double *stop = nullptr);
+template <typename T>
+int launch_dss(gf_problem *prob, int op, T *u, cudaStream_t st);
+template <typename T>
+int launch_dudt(gf_problem *prob, int eqn, int mode, T nu, const T *const *f, T *const *o,
+                cudaStream_t st);

@@ -1,0 +1,327 @@
+"""Host-side mirror of the GeoFLOW interfaces on the hot path, over libgfgpu.
+
+The classes keep the reference's names, argument meaning and error
+behaviour so that code written against the reference reads the same:
+
+  GridBox      grid/ggrid_box.ipp   (host set-up: elements, coordinates,
+                                     regular geometry, Dirichlet mask)
+  GGFX         comm/ggfx.hpp        (doOp with Sum/Smooth/Max/Min,
+                                     get_mult/get_imult)
+  GHelmholtz   sem/ghelmholtz.ipp   (set_Lap_scalar, set_mass_scalar,
+                                     opVec_prod)
+  GMass        sem/gmass.ipp        (opVec_prod; inverse = 1/Smooth(M))
+  GCG          solvers/gcg.ipp      (solve(A, b, x) / solve(A, b, xb, x),
+                                     GCGERR codes, iteration count,
+                                     residual history)
+  GExRKStepper pdes/gexrk_stepper.ipp and GBurgers pdes/gburgers.ipp
+
+Fields are torch CUDA tensors in element-local (E-vector) layout; torch is
+used only for device memory.  Every compute call goes through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+
+
+def _lib():
+    return A.load()
+
+
+def gll_basis(p: int):
+    """GLL nodes, weights and column-major D (GLLBasis, sem/gllbasis.ipp)."""
+    n = p + 1
+    xi, w, D = np.zeros(n), np.zeros(n), np.zeros(n * n)
+    rc = _lib().gf_gll_basis(p, A.ptr(xi), A.ptr(w), A.ptr(D))
+    if rc:
+        raise A.GFError(rc, f"gf_gll_basis({p})")
+    return xi, w, D
+
+
+class Context:
+    """A CUDA device + stream owning libgfgpu state (one per host thread)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+        self.device = device
+        self.torch_device = torch.device("cuda", device)
+        h = C.c_void_p()
+        if stream is None:  # order the work with torch's current stream
+            stream = torch.cuda.current_stream(device).cuda_stream
+        s = C.c_void_p(stream) if stream else None
+        rc = _lib().gf_ctx_create(device, s, C.byref(h))
+        if rc:
+            raise A.GFError(rc, "gf_ctx_create failed (no CUDA device?)")
+        self.handle = h
+
+    def check(self, rc: int, what: str = "") -> int:
+        if rc < 0:
+            msg = _lib().gf_ctx_last_error(self.handle).decode()
+            raise A.GFError(rc, f"{what}: {msg}")
+        return rc
+
+    def synchronize(self):
+        self.check(_lib().gf_ctx_synchronize(self.handle), "synchronize")
+
+    def close(self):
+        if self.handle:
+            _lib().gf_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GridBox:
+    """Regular 2-d/3-d box grid as GGridBox builds it on one rank.
+
+    ne: elements per direction, p: polynomial order, x0/length: box origin
+    and extent, periodic: per-direction flags (else Dirichlet faces).
+    """
+
+    def __init__(self, dim, ne, p, x0=None, length=None, periodic=None):
+        self.dim, self.p, self.n = int(dim), int(p), int(p) + 1
+        self.ne = [int(v) for v in ne][:dim]
+        self.x0 = np.array(x0 if x0 is not None else [0.0] * dim, dtype=np.float64)[:dim]
+        self.length = np.array(length if length is not None else [1.0] * dim, dtype=np.float64)[:dim]
+        self.periodic = [int(bool(v)) for v in (periodic if periodic is not None else [0] * dim)][:dim]
+        self.nelems = int(np.prod(self.ne))
+        self.nn = self.n ** self.dim
+        N = self.nelems * self.nn
+        self.xi, self.W, self.D = gll_basis(self.p)
+        lib = _lib()
+        ne_c = (C.c_int * 3)(*(self.ne + [1] * (3 - dim)))
+        per_c = (C.c_int * 3)(*(self.periodic + [0] * (3 - dim)))
+        self.xyz = [np.zeros(N) for _ in range(dim)]
+        xyz_c = (A.P_double * 3)(*[A.ptr(a) for a in self.xyz])
+        self.elem_geom = np.zeros(self.nelems * (dim + 1))
+        self.mask = np.zeros(N)
+        rc = lib.gf_box_grid(dim, ne_c, self.p, A.ptr(self.x0), A.ptr(self.length), per_c, xyz_c,
+                             A.ptr(self.elem_geom), A.ptr(self.mask))
+        if rc:
+            raise A.GFError(rc, "gf_box_grid")
+        self.node_class = np.zeros(N, dtype=np.int32)
+        self.class_ptr = np.zeros(N + 1, dtype=np.int32)
+        self.members = np.zeros(N, dtype=np.int32)
+        nc = lib.gf_box_classes(dim, ne_c, self.p, per_c, A.ptr(self.node_class),
+                                A.ptr(self.class_ptr), A.ptr(self.members))
+        if nc < 0:
+            raise A.GFError(nc, "gf_box_classes")
+        self.nclass = int(nc)
+        self.class_ptr = self.class_ptr[: nc + 1].copy()
+
+    def ndof(self) -> int:
+        return self.nelems * self.nn
+
+    def xNodes(self):
+        return self.xyz
+
+    def mult(self):
+        cnt = np.diff(self.class_ptr)
+        return cnt[self.node_class].astype(np.float64)
+
+
+class Problem:
+    """Device-resident grid, operators and gather-scatter map (gf_problem)."""
+
+    def __init__(self, ctx: Context, grid: GridBox, dirichlet_mask: bool = True):
+        self.ctx, self.grid = ctx, grid
+        self.dim, self.n, self.nlocal = grid.dim, grid.n, grid.ndof()
+        d = A.ProblemDesc()
+        d.dim, d.ne, d.n = grid.dim, grid.nelems, grid.n
+        self._keep = [grid.D, grid.W, grid.elem_geom, grid.mask, grid.class_ptr, grid.members]
+        d.D, d.W = A.ptr(grid.D), A.ptr(grid.W)
+        d.geom = A.GF_GEOM_AFFINE
+        d.elem_geom = A.ptr(grid.elem_geom)
+        d.node_geom = None
+        d.mask = A.ptr(grid.mask) if dirichlet_mask else None
+        d.nclass = grid.nclass
+        d.class_ptr, d.members = A.ptr(grid.class_ptr), A.ptr(grid.members)
+        h = C.c_void_p()
+        ctx.check(_lib().gf_problem_create(ctx.handle, C.byref(d), C.byref(h)), "gf_problem_create")
+        self.handle = h
+
+    def zeros(self, dtype=None, ncomp=None):
+        import torch
+        dt = dtype or torch.float64
+        if ncomp is None:
+            return torch.zeros(self.nlocal, dtype=dt, device=self.ctx.torch_device)
+        return [torch.zeros(self.nlocal, dtype=dt, device=self.ctx.torch_device) for _ in range(ncomp)]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib().gf_problem_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _dtype_code(t) -> int:
+    import torch
+    if t.dtype == torch.float64:
+        return A.GF_F64
+    if t.dtype == torch.float32:
+        return A.GF_F32
+    raise TypeError(f"unsupported dtype {t.dtype}")
+
+
+def _check_field(prob: Problem, t):
+    if not t.is_cuda or t.numel() != prob.nlocal or not t.is_contiguous():
+        raise ValueError("fields must be contiguous CUDA tensors of N_local elements")
+
+
+class GGFX:
+    """Gather-scatter (GGFX::doOp) over the problem's equivalence classes."""
+    Sum, Smooth, Max, Min = A.GF_DSS_SUM, A.GF_DSS_SMOOTH, A.GF_DSS_MAX, A.GF_DSS_MIN
+
+    def __init__(self, prob: Problem):
+        self.prob = prob
+
+    def doOp(self, u, op) -> bool:
+        _check_field(self.prob, u)
+        self.prob.ctx.check(_lib().gf_dss(self.prob.handle, _dtype_code(u), int(op), A.ptr(u)),
+                            "GGFX::doOp")
+        return True
+
+    def get_mult(self):
+        m = self.prob.zeros()
+        self.prob.ctx.check(_lib().gf_mult(self.prob.handle, 0, A.ptr(m)), "get_mult")
+        return m
+
+    def get_imult(self):
+        m = self.prob.zeros()
+        self.prob.ctx.check(_lib().gf_mult(self.prob.handle, 1, A.ptr(m)), "get_imult")
+        return m
+
+
+class GMass:
+    """Lumped mass W x W (x W) x Jac; inverse=True uses 1/Smooth(M)."""
+
+    def __init__(self, prob: Problem, inverse: bool = False):
+        self.prob, self.inverse = prob, inverse
+
+    def opVec_prod(self, u, utmp, uo):
+        _check_field(self.prob, u)
+        self.prob.ctx.check(_lib().gf_mass_apply(self.prob.handle, _dtype_code(u), int(self.inverse),
+                                                 A.ptr(u), A.ptr(uo)), "GMass::opVec_prod")
+
+
+class GHelmholtz:
+    """H = q M + p L (weak Laplacian L); p defaults to 1, no mass term until
+    set_mass_scalar is called (ghelmholtz.ipp:30-45, 591-625)."""
+
+    def __init__(self, prob: Problem):
+        self.prob = prob
+        self.p, self.q, self.bcompute_helm = 1.0, None, False
+
+    def set_Lap_scalar(self, p):
+        self.p = p
+
+    def set_mass_scalar(self, q):
+        self.q = q
+        self.bcompute_helm = True
+
+    def opVec_prod(self, u, utmp, uo):
+        _check_field(self.prob, u)
+        dt = _dtype_code(u)
+        p_s, p_v = (float(self.p), None) if np.isscalar(self.p) else (1.0, self.p)
+        q = self.q if self.q is not None else 0.0
+        q_s, q_v = (float(q), None) if np.isscalar(q) else (1.0, q)
+        self.prob.ctx.check(_lib().gf_helmholtz_apply(
+            self.prob.handle, dt, p_s, A.ptr(p_v), q_s, A.ptr(q_v), int(self.bcompute_helm),
+            A.ptr(u), A.ptr(uo)), "GHelmholtz::opVec_prod")
+
+
+@dataclass
+class CGTraits:
+    """LinSolverBase::Traits (lin_solver_base.hpp:38-44) plus the B200 options."""
+    maxit: int = 512
+    normtype: int = A.GF_NORM_INF
+    tol: float = 1e-6
+    precond: int = A.GF_PRECOND_NONE
+    precision: int = A.GF_CG_FP64
+    inner_tol: float = 1e-5
+    max_refine: int = 40
+    check_every: int = 16
+    relative: int = 0
+
+    def to_c(self) -> A.CGTraits:
+        t = A.CGTraits()
+        for f in ("maxit", "normtype", "tol", "precond", "precision", "inner_tol", "max_refine",
+                  "check_every", "relative"):
+            setattr(t, f, getattr(self, f))
+        return t
+
+
+class GCG:
+    """Conjugate gradient (GCG::solve_impl): returns GCGERR codes."""
+    GCGERR_NONE, GCGERR_NOCONVERGE, GCGERR_SOLVE, GCGERR_PRECOND, GCGERR_BADITERNUM = 0, 1, 2, 3, 4
+
+    def __init__(self, traits: CGTraits, prob: Problem):
+        self.traits, self.prob = traits, prob
+        self.iter_, self.rnorm_ = 0, 0.0
+        self.residuals_ = np.zeros(max(1, traits.maxit))
+
+    def solve(self, A_op: GHelmholtz, b, *args) -> int:
+        if len(args) == 1:
+            xb, x = None, args[0]
+        elif len(args) == 2:
+            xb, x = args
+        else:
+            raise TypeError("solve(A, b, x) or solve(A, b, xb, x)")
+        for t in (b, x) + ((xb,) if xb is not None else ()):
+            _check_field(self.prob, t)
+        if not np.isscalar(A_op.p) or (A_op.q is not None and not np.isscalar(A_op.q)):
+            raise ValueError("the device CG takes scalar p and q")
+        it, rn = C.c_int(0), C.c_double(0.0)
+        tr = self.traits.to_c()
+        q = float(A_op.q) if A_op.q is not None else 0.0
+        rc = _lib().gf_cg_solve(self.prob.handle, C.byref(tr), float(A_op.p), q,
+                                int(A_op.bcompute_helm), A.ptr(b), A.ptr(xb), A.ptr(x),
+                                C.byref(it), C.byref(rn), A.ptr(self.residuals_))
+        self.prob.ctx.check(rc, "GCG::solve")
+        self.iter_, self.rnorm_ = it.value, rn.value
+        return rc
+
+    def get_iteration_count(self) -> int:
+        return self.iter_
+
+    def get_residuals(self):
+        return self.residuals_[: self.iter_]
+
+
+class GBurgers:
+    """Burgers / advection-diffusion / heat on GExRKStepper (gburgers.ipp)."""
+    ADVECT, BURGERS, HEAT = A.GF_EQN_ADVECT, A.GF_EQN_BURGERS, A.GF_EQN_HEAT
+
+    def __init__(self, prob: Problem, eqn: int, nu: float, scheme: int = A.GF_RK4):
+        self.prob, self.eqn, self.nu, self.scheme = prob, eqn, float(nu), scheme
+        self.nstate = prob.dim if eqn == A.GF_EQN_BURGERS else 1
+
+    def traits(self) -> A.RKTraits:
+        t = A.RKTraits()
+        t.eqn, t.nu, t.nstate, t.scheme = self.eqn, self.nu, self.nstate, self.scheme
+        return t
+
+    def dudt(self, u, c, dudt):
+        lib = _lib()
+        self.prob.ctx.check(lib.gf_dudt(self.prob.handle, _dtype_code(u[0]), self.eqn, self.nu,
+                                        len(u), A.ptr_array(u), A.ptr_array(c or []),
+                                        A.ptr_array(dudt)), "GBurgers::dudt")
+
+    def step(self, u, c=None, dt=1e-4, nsteps=1, t0=0.0):
+        tr = self.traits()
+        self.prob.ctx.check(_lib().gf_rk_advance(self.prob.handle, _dtype_code(u[0]), C.byref(tr),
+                                                 A.ptr_array(u), A.ptr_array(c or []), t0, dt,
+                                                 nsteps), "GBurgers::step")

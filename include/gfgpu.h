@@ -1,0 +1,245 @@
+/*
+ * gfgpu.h -- C ABI of libgfgpu, the B200 (sm_100a) implementation of the
+ * GeoFLOW spectral-element hot path.
+ *
+ * Conventions
+ *  - Every entry point returns int: 0 on success, a positive GCG-style code
+ *    for solver outcomes (GF_CG_NOCONVERGE ...), a negative GF_ERR_* on
+ *    argument or CUDA errors.  The last error message of a context is kept
+ *    (sticky) and read with gf_ctx_last_error().
+ *  - Field arguments are DEVICE pointers in element-local ("E-vector")
+ *    layout: element-major, x fastest inside an element, exactly the
+ *    GTVector layout of the reference (grid/ggrid_box.ipp:394-406).  The
+ *    *_host entry points take host pointers and stage through the device.
+ *  - All work is ordered on the context's CUDA stream; calls that return a
+ *    scalar to the host synchronise that stream.
+ *  - 1-d operators are column-major, D[l + j*n] = dphi_j/dxi(xi_l), as
+ *    GLLBasis::getDerivMatrix(FALSE) (sem/gllbasis.ipp:580-606).
+ *
+ * Reference file citations are relative to NOAA-GSL/GeoFLOW src/cdg/.
+ */
+#ifndef GFGPU_H
+#define GFGPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFGPU_ABI_VERSION 1
+
+/* ---- status codes ---- */
+enum {
+  GF_OK = 0,
+  /* GCG::GCGERR (solvers/gcg.hpp:32), returned by gf_cg_solve */
+  GF_CG_NOCONVERGE = 1,
+  GF_CG_SOLVE = 2,
+  GF_CG_PRECOND = 3,
+  GF_CG_BADITERNUM = 4,
+  /* ABI errors */
+  GF_ERR_ARG = -1,
+  GF_ERR_CUDA = -2,
+  GF_ERR_UNSUPPORTED = -3,
+  GF_ERR_NOMEM = -4,
+  GF_ERR_NONFINITE = -5,
+  GF_ERR_WATCHDOG = -6
+};
+
+/* ---- enumerations ---- */
+enum { GF_F64 = 0, GF_F32 = 1 };                       /* field dtype */
+enum { GF_DSS_SUM = 0, GF_DSS_SMOOTH = 1, GF_DSS_MAX = 2, GF_DSS_MIN = 3 }; /* ggfx.hpp:36-76 */
+enum { GF_NORM_INF = 0, GF_NORM_EUC = 1, GF_NORM_L2 = 2, GF_NORM_L1 = 3 }; /* lin_solver_base.hpp:38 */
+enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1 };
+enum { GF_CG_FP64 = 0, GF_CG_MIXED = 1 };            /* plain FP64 / FP32 apply + FP64 refinement */
+enum { GF_GEOM_AFFINE = 0, GF_GEOM_REGULAR = 1 };     /* see gf_problem_desc */
+enum { GF_EQN_ADVECT = 0, GF_EQN_BURGERS = 1, GF_EQN_HEAT = 2 }; /* GBurgers traits */
+/* GExRKStepper schemes: Butcher orders 1..4 (gbutcherrk.ipp:69-125) and
+ * the SSP schemes (gexrk_stepper.ipp:533-780) */
+enum { GF_RK1 = 1, GF_RK2 = 2, GF_RK3 = 3, GF_RK4 = 4, GF_SSP22 = 22, GF_SSP33 = 33, GF_SSP34 = 34 };
+
+typedef struct gf_context *gf_ctx_t;
+typedef struct gf_problem *gf_problem_t;
+
+/* ---- context ---- */
+/* Creates a context on CUDA device `device`; `stream` is the cudaStream_t
+ * all of the context's work is ordered on (NULL: the legacy default
+ * stream, ordered with every other blocking stream of the process). */
+int gf_ctx_create(int device, void *stream, gf_ctx_t *out);
+int gf_ctx_destroy(gf_ctx_t ctx);
+/* Last error message of the context ("" if none); clears it. */
+const char *gf_ctx_last_error(gf_ctx_t ctx);
+int gf_ctx_synchronize(gf_ctx_t ctx);
+int gf_abi_version(void);
+
+/* ---- host-side set-up helpers (no device work) ---- */
+/* GLL nodes xi[p+1], weights w[p+1] and D[(p+1)^2] in the reference's
+ * long-double construction cast to double.  Replaces GLLBasis::init
+ * (sem/gllbasis.ipp:411-606,715-737). */
+int gf_gll_basis(int p, double *xi, double *w, double *D);
+
+/* Regular box grid of GGridBox (grid/ggrid_box.ipp:24-105,250-463,860-980):
+ * lexicographic element list, node coordinates xyz[dim][N_local], regular
+ * geometry (dXidX = 2/L per element, Jac = prod L / 2^dim), mask[N_local]
+ * (0 on non-periodic boundary nodes, ggrid.ipp:1458-1466).  Any output
+ * pointer may be NULL.  elem_geom[ne*(dim+1)] = {dXidX_0..dim-1, Jac}. */
+int gf_box_grid(int dim, const int *ne, int p, const double *x0,
+                const double *len, const int *periodic, double *const *xyz,
+                double *elem_geom, double *mask);
+
+/* Equivalence classes of a regular box grid (the result of GGFX::init on
+ * periodized coordinates, comm/ggfx.hpp:169-342, ggrid_box.ipp:753-840),
+ * built directly from the lattice: node_class[N_local], class_ptr[nclass+1],
+ * members[N_local] ascending within each class, classes ordered by smallest
+ * member.  Returns nclass (>=0) or a negative error. */
+int64_t gf_box_classes(int dim, const int *ne, int p, const int *periodic,
+                       int32_t *node_class, int32_t *class_ptr,
+                       int32_t *members);
+
+/* Geometry-free matching of GGFX::init (comm/ggfx.hpp:169-342): classes of
+ * nodes whose tolerance boxes intersect, from coordinates xyz[dim][n].
+ * Same outputs as gf_box_classes. */
+int64_t gf_classes_from_coords(int dim, int64_t n, const double *const *xyz,
+                               double tol, int32_t *node_class,
+                               int32_t *class_ptr, int32_t *members);
+
+/* ---- problem (grid + operators + gather-scatter map) ---- */
+typedef struct {
+  int dim;                 /* 2 or 3 */
+  int64_t ne;              /* number of elements */
+  int n;                   /* GLL points per direction (p+1), 2..12 */
+  const double *D;         /* host, n*n column-major 1-d derivative */
+  const double *W;         /* host, n GLL weights */
+  int geom;                /* GF_GEOM_AFFINE or GF_GEOM_REGULAR */
+  /* GF_GEOM_AFFINE: host ne*(dim+1): dXidX_0..dim-1, Jac per element */
+  const double *elem_geom;
+  /* GF_GEOM_REGULAR: host (dim+1)*N_local: dXidX_0..dim-1, Jac per node
+   * (GGrid::dXidX(k,0), GGrid::Jac of reg_geom_init, ggrid.ipp:707-797) */
+  const double *node_geom;
+  const double *mask;      /* host N_local, or NULL (all ones) */
+  /* gather-scatter map (GGFX::recv_map_ as CSR) */
+  int64_t nclass;
+  const int32_t *class_ptr; /* host nclass+1 */
+  const int32_t *members;   /* host N_local, ascending inside each class */
+} gf_problem_desc;
+
+int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *desc, gf_problem_t *out);
+int gf_problem_destroy(gf_problem_t prob);
+int gf_problem_sizes(gf_problem_t prob, int64_t *nlocal, int64_t *nclass);
+/* Number of kernels the library has launched for this problem so far
+ * (instrumentation, in the spirit of the reference's tracer ranges). */
+int gf_problem_stats(gf_problem_t prob, int64_t *kernel_launches);
+
+/* ---- operators (device pointers) ---- */
+/* GHelmholtz::opVec_prod (sem/ghelmholtz.ipp:77-93, reg_prod 309-378):
+ * uo = p L u + q M u with L the weak Laplacian sum_k Dk^T (Gk M) Dk u.
+ * p_vec/q_vec (device, N_local, same dtype) override the scalars when
+ * non-NULL; use_mass=0 drops the mass term (set_mass_scalar never called). */
+int gf_helmholtz_apply(gf_problem_t prob, int dtype, double p, const void *p_vec,
+                       double q, const void *q_vec, int use_mass,
+                       const void *u, void *uo);
+/* Adjoint (transpose) of gf_helmholtz_apply: the operator is symmetric
+ * element by element, so this applies the transposed contractions
+ * explicitly; used by the adjoint path and its dot-product test. */
+int gf_helmholtz_apply_T(gf_problem_t prob, int dtype, double p, double q,
+                         int use_mass, const void *u, void *uo);
+/* GMass::opVec_prod (sem/gmass.ipp:226-233); inverse=1 uses
+ * 1/Smooth(M) (gmass.ipp:65-92). */
+int gf_mass_apply(gf_problem_t prob, int dtype, int inverse, const void *u, void *uo);
+/* GGrid::compute_grefderiv (ggrid.ipp:2046-2265): du = (D_idir or
+ * D_idir^T when dotrans) u, idir = 1..dim. */
+int gf_grefderiv(gf_problem_t prob, int dtype, const void *u, int idir, int dotrans, void *du);
+/* GGrid::compute_grefdiv (ggrid.ipp:1847-1927): divu = sum_k Dk^T u_k
+ * (dotrans=1) or sum_k Dk u_k (dotrans=0). */
+int gf_grefdiv(gf_problem_t prob, int dtype, const void *const *u, int dotrans, void *divu);
+/* GGrid::deriv (ggrid.ipp:1163-1190): physical derivative du/dx_idir. */
+int gf_deriv(gf_problem_t prob, int dtype, const void *u, int idir, void *du);
+/* GAdvect::apply (sem/gadvect.ipp:58-100): po = M sum_j c_j dp/dx_j. */
+int gf_advect_apply(gf_problem_t prob, int dtype, const void *p, int ncomp,
+                    const void *const *c, void *po);
+/* GBurgers::dudt_impl (pdes/gburgers.ipp:203-257), fused per element.
+ * eqn: GF_EQN_ADVECT (nstate=1, c = dim prescribed velocities),
+ * GF_EQN_BURGERS (nstate=dim, c ignored), GF_EQN_HEAT. */
+int gf_dudt(gf_problem_t prob, int dtype, int eqn, double nu, int nstate,
+            const void *const *u, const void *const *c, void *const *dudt);
+/* GGFX::doOp (comm/ggfx.hpp:346-443), bit-exact: each class reduced in
+ * ascending local id order, Sum/Smooth from 0, Max/Min as std::max/min
+ * folds from lowest()/max().  (A NaN produced by Sum/Smooth is the GPU's
+ * canonical NaN, not the input's payload.) */
+int gf_dss(gf_problem_t prob, int dtype, int op, void *u);
+/* GGFX::get_mult / get_imult (comm/ggfx.hpp:453-487), double output. */
+int gf_mult(gf_problem_t prob, int inverse, double *mult);
+/* GGrid::integrate (ggrid.ipp:1077-1147): returns the integral in *result
+ * (host).  Synchronises. */
+int gf_integrate(gf_problem_t prob, int dtype, const void *u, double *result);
+
+/* ---- conjugate gradient (solvers/gcg.ipp:239-429) ---- */
+typedef struct {
+  int maxit;        /* LinSolverBase::Traits::maxit */
+  int normtype;     /* GF_NORM_* */
+  double tol;       /* stop when norm(r) <= (norm(b) < 1 ? tol : tol*norm(b)) */
+  int precond;      /* GF_PRECOND_* (Jacobi has no reference counterpart) */
+  int precision;    /* GF_CG_FP64 or GF_CG_MIXED */
+  double inner_tol; /* MIXED: relative residual drop per FP32 inner solve */
+  int max_refine;   /* MIXED: maximum refinement sweeps */
+  int check_every;  /* iterations between host convergence checks (>=1) */
+  int relative;     /* 1: stop at norm(r) <= tol*norm(b) even when norm(b) < 1 */
+} gf_cg_traits;
+
+/* Solves (p L + q M) x = b on the assembled space (DSS Sum + mask), as
+ * GCG::solve_impl(A,b,xb,x) when xb != NULL or solve_impl(A,b,x) when
+ * xb == NULL.  b, xb, x are device FP64 E-vectors; x holds the initial
+ * guess on entry.  iters/final_norm/residuals (host, maxit) may be NULL.
+ * Returns 0, GF_CG_NOCONVERGE or a negative error. */
+int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *traits, double p, double q,
+                int use_mass, const double *b, const double *xb, double *x,
+                int *iters, double *final_norm, double *residuals);
+/* Same with host buffers: copies b, xb, x to the device, solves, copies x
+ * back.  Synchronises. */
+int gf_cg_solve_host(gf_problem_t prob, const gf_cg_traits *traits, double p, double q,
+                     int use_mass, const double *b, const double *xb, double *x,
+                     int *iters, double *final_norm);
+
+/* ---- explicit RK (pdes/gexrk_stepper.ipp) on the GBurgers RHS ---- */
+typedef struct {
+  int eqn;        /* GF_EQN_* */
+  double nu;      /* dissipation (GBurgers traits nu) */
+  int nstate;     /* evolved components: 1 for ADVECT/HEAT, dim for BURGERS */
+  int scheme;     /* GF_RK1..4, GF_SSP22/33/34 */
+} gf_rk_traits;
+/* Advances u[nstate] (device, dtype) in place by nsteps steps of size dt,
+ * with the DSS Smooth calls where GExRKStepper::step_b / step_ssp* place
+ * them.  c[dim] are prescribed velocities for GF_EQN_ADVECT (else NULL). */
+int gf_rk_advance(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
+                  void *const *u, const void *const *c, double t0, double dt, int nsteps);
+/* Host-buffer variant: copies u and c in, advances, copies u out. */
+int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
+                       void *const *u, const void *const *c, double t0, double dt, int nsteps);
+
+/* ---- adjoint (no reference counterpart) ---- */
+/* Vector-Jacobian product of gf_dudt: given u (and c) and a cotangent
+ * lam[nstate] on dudt, returns ubar[nstate] = (d dudt/du)^T lam. */
+int gf_dudt_vjp(gf_problem_t prob, int dtype, int eqn, double nu, int nstate,
+                const void *const *u, const void *const *c,
+                const void *const *lam, void *const *ubar);
+/* Adjoint of gf_dss (DSS Sum/Smooth are symmetric: each class is reduced
+ * with one weight, so the transpose equals the forward map). */
+int gf_dss_T(gf_problem_t prob, int dtype, int op, void *u);
+/* VJP of one RK step: given the step input u0 and a cotangent lam on the
+ * step output, returns (d step/du0)^T lam in lam (in place). */
+int gf_rk_step_vjp(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
+                   const void *const *u0, const void *const *c, double dt,
+                   void *const *lam);
+/* Gradient of J = 1/2 ||u(T) - u_obs||_M^2 with respect to u(0) through
+ * nsteps RK steps, with a checkpoint every `checkpoint_every` steps and
+ * recomputation.  u0, u_obs, grad: device FP64 [nstate][N_local].
+ * *J receives the misfit (host). */
+int gf_adjoint_gradient(gf_problem_t prob, const gf_rk_traits *traits,
+                        const double *const *u0, const double *const *c,
+                        const double *const *u_obs, double dt, int nsteps,
+                        int checkpoint_every, double *J, double *const *grad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFGPU_H */

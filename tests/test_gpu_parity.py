@@ -1,0 +1,279 @@
+"""GPU parity: every hot-path entry point, called through the C ABI on a
+B200, against the CPU oracle on the same seeded inputs.
+
+Tolerances: bit-exact for the gather-scatter (integer maps, fixed fold
+order); FP64 operator applies within 1e-12 relative (max-norm); FP64
+solves and RK runs within 1e-10 relative; FP32 applies within 1e-5.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from geoflow_b200 import (CGTraits, GBurgers, GCG, GGFX, GHelmholtz, GMass, GridBox, Problem,
+                          _abi as A)
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint64 if a.dtype == np.float64 else np.uint32)
+
+
+def same_bits(a, b):
+    """Bit-identical, except that any NaN matches any NaN: GPU arithmetic
+    returns the canonical NaN where x86 propagates the input payload."""
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.array_equal(na, nb) and np.array_equal(bits(a)[~na], bits(b)[~nb])
+
+
+def dev(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def relerr(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def setup(ctx, dim, ne, p, periodic=None, mask=True):
+    g = GridBox(dim, ne, p, periodic=periodic)
+    o = O.OracleBox(dim, ne, p, periodic=periodic)
+    return g, Problem(ctx, g, dirichlet_mask=mask), o
+
+
+CASES3 = [([2, 2, 2], 2, None), ([3, 2, 2], 4, [1, 0, 1]), ([2, 2, 3], 6, None),
+          ([2, 3, 2], 7, [1, 1, 1]), ([2, 2, 2], 9, None), ([1, 2, 1], 11, None)]
+CASES2 = [([3, 4], 1, None), ([4, 3], 3, [1, 1]), ([3, 3], 4, None), ([2, 5], 6, [0, 1]),
+          ([3, 2], 8, None), ([2, 2], 11, None)]
+
+
+@pytest.mark.parametrize("dim,case", [(3, c) for c in CASES3] + [(2, c) for c in CASES2])
+def test_helmholtz_fp64_matches_oracle(ctx, dim, case):
+    ne, p, per = case
+    g, prob, o = setup(ctx, dim, ne, p, per)
+    rng = np.random.default_rng(7 + p)
+    u = rng.standard_normal(g.ndof())
+    qv = 0.5 + rng.random(g.ndof())
+    for pscal, use_q in ((1.0, False), (0.37, True), (2.5, False)):
+        H = GHelmholtz(prob)
+        H.set_Lap_scalar(pscal)
+        if use_q:
+            H.set_mass_scalar(dev(qv))
+        uo = prob.zeros()
+        H.opVec_prod(dev(u), None, uo)
+        ref = o.helmholtz(u, p=pscal, q_vec=qv if use_q else None)
+        assert relerr(host(uo), ref) < 1e-12
+
+
+def test_helmholtz_pvec_fp64(ctx):
+    g, prob, o = setup(ctx, 3, [2, 2, 2], 5)
+    rng = np.random.default_rng(11)
+    u, pv = rng.standard_normal(g.ndof()), 0.5 + rng.random(g.ndof())
+    H = GHelmholtz(prob)
+    H.set_Lap_scalar(dev(pv))
+    uo = prob.zeros()
+    H.opVec_prod(dev(u), None, uo)
+    assert relerr(host(uo), o.helmholtz(u, p=1.0, p_vec=pv)) < 1e-12
+
+
+@pytest.mark.parametrize("dim,ne,p", [(3, [3, 3, 2], 7), (3, [2, 2, 2], 5), (2, [5, 4], 4)])
+def test_helmholtz_fp32_within_1e5(ctx, dim, ne, p):
+    g, prob, o = setup(ctx, dim, ne, p)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal(g.ndof())
+    H = GHelmholtz(prob)
+    H.set_Lap_scalar(1.0)
+    H.set_mass_scalar(1.0)
+    uo = prob.zeros(torch.float32)
+    H.opVec_prod(dev(u, torch.float32), None, uo)
+    ref = o.helmholtz(u.astype(np.float32).astype(np.float64), p=1.0, q_vec=np.ones(g.ndof()))
+    err = np.linalg.norm(host(uo).astype(np.float64) - ref) / np.linalg.norm(ref)
+    assert err < 1e-5
+
+
+@pytest.mark.parametrize("dim,ne,p,per", [(3, [2, 3, 2], 4, [1, 0, 1]), (2, [3, 3], 5, [1, 1]),
+                                          (3, [2, 2, 2], 7, None), (2, [1, 4], 3, [1, 0])])
+@pytest.mark.parametrize("op", [GGFX.Sum, GGFX.Smooth, GGFX.Max, GGFX.Min])
+def test_dss_bit_exact(ctx, dim, ne, p, per, op):
+    g, prob, o = setup(ctx, dim, ne, p, per)
+    rng = np.random.default_rng(100 + op)
+    u = rng.standard_normal(g.ndof()) * 10.0 ** rng.integers(-3, 4, g.ndof())
+    u[::97] = -0.0
+    u[5] = np.nan
+    u[13] = np.inf
+    for dt in (torch.float64, torch.float32):
+        npdt = np.float64 if dt == torch.float64 else np.float32
+        uh = u.astype(npdt)
+        t = dev(uh, dt)
+        GGFX(prob).doOp(t, op)
+        ref = o.dss(uh.copy(), op)
+        assert same_bits(host(t), ref)
+
+
+def test_mult_and_mass(ctx):
+    g, prob, o = setup(ctx, 3, [2, 3, 2], 4, [1, 0, 0])
+    gg = GGFX(prob)
+    assert np.array_equal(host(gg.get_mult()), o.mult())
+    assert np.array_equal(host(gg.get_imult()), 1.0 / o.mult())
+    u = np.random.default_rng(1).standard_normal(g.ndof())
+    out = prob.zeros()
+    GMass(prob).opVec_prod(dev(u), None, out)
+    assert relerr(host(out), o.mass * u) < 1e-15
+    GMass(prob, inverse=True).opVec_prod(dev(u), None, out)
+    assert relerr(host(out), o.imass * u) < 1e-15
+
+
+@pytest.mark.parametrize("dim,ne,p", [(3, [2, 3, 2], 5), (2, [3, 4], 6)])
+def test_derivatives_match_oracle(ctx, dim, ne, p):
+    g, prob, o = setup(ctx, dim, ne, p)
+    lib = A.load()
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal(g.ndof())
+    du = prob.zeros()
+    for idir in range(1, dim + 1):
+        for dotrans in (0, 1):
+            ctx.check(lib.gf_grefderiv(prob.handle, A.GF_F64, A.ptr(dev(u)), idir, dotrans, A.ptr(du)))
+            assert relerr(host(du), o.grefderiv(u, idir, dotrans)) < 1e-13
+        ctx.check(lib.gf_deriv(prob.handle, A.GF_F64, A.ptr(dev(u)), idir, A.ptr(du)))
+        assert relerr(host(du), o.deriv(u, idir)) < 1e-13
+    us = [rng.standard_normal(g.ndof()) for _ in range(dim)]
+    ts = [dev(a) for a in us]
+    ctx.check(lib.gf_grefdiv(prob.handle, A.GF_F64, A.ptr_array(ts), 1, A.ptr(du)))
+    assert relerr(host(du), o.grefdiv(us, 1)) < 1e-13
+
+
+@pytest.mark.parametrize("dim,ne,p", [(3, [2, 2, 3], 6), (2, [4, 3], 4)])
+def test_advect_and_dudt_match_oracle(ctx, dim, ne, p):
+    g, prob, o = setup(ctx, dim, ne, p, [1] * dim, mask=False)
+    lib = A.load()
+    rng = np.random.default_rng(9)
+    u = [rng.standard_normal(g.ndof()) for _ in range(dim)]
+    c = [rng.standard_normal(g.ndof()) for _ in range(dim)]
+    ut, ct = [dev(a) for a in u], [dev(a) for a in c]
+    po = prob.zeros()
+    ctx.check(lib.gf_advect_apply(prob.handle, A.GF_F64, A.ptr(ut[0]), dim, A.ptr_array(ct), A.ptr(po)))
+    assert relerr(host(po), o.advect(u[0], c)) < 1e-12
+    for kind, nst in ((0, 1), (1, dim), (2, 1)):
+        B = GBurgers(prob, kind, 0.013)
+        out = prob.zeros(ncomp=nst)
+        B.dudt(ut[:nst], ct if kind == 0 else None, out)
+        ref = o.dudt(kind, 0.013, u[:nst], c if kind == 0 else None)
+        for k in range(nst):
+            assert relerr(host(out[k]), ref[k]) < 1e-11
+
+
+def test_integrate(ctx):
+    g, prob, o = setup(ctx, 3, [2, 2, 2], 5)
+    u = np.random.default_rng(2).standard_normal(g.ndof())
+    val = A.C.c_double() if hasattr(A, "C") else None
+    import ctypes as C
+    r = C.c_double()
+    ctx.check(A.load().gf_integrate(prob.handle, A.GF_F64, A.ptr(dev(u)), C.byref(r)))
+    assert abs(r.value - o.integrate(u)) < 1e-12 * max(1.0, abs(o.integrate(np.abs(u))))
+
+
+def test_cdg_cg_poisson_on_gpu(ctx):
+    """cdg_cg.cpp known answer through the device CG (2D, 4x4, p=6)."""
+    g, prob, o = setup(ctx, 2, [4, 4], 6)
+    x, y = g.xyz
+    f = 6.0 * x * y * (1.0 - y) - 2.0 * x ** 3
+    ua = y * (1.0 - y) * x ** 3
+    eps = 100 * np.finfo(float).eps
+    ub = np.zeros(g.ndof())
+    east = np.abs(x - 1.0) <= eps
+    ub[east] = (y * (1.0 - y))[east]
+    b = -(f * o.mass)
+    L = GHelmholtz(prob)
+    cg = GCG(CGTraits(maxit=256, tol=1e-7), prob)
+    u = prob.zeros()
+    rc = cg.solve(L, dev(b), dev(ub), u)
+    assert rc == GCG.GCGERR_NONE
+    uh = host(u)
+    err = o.integrate((uh - ua) ** 2) / o.integrate(np.ones(g.ndof()))
+    assert err < 1e-12
+    # the oracle's restatement stops after the same number of iterations
+    xo = np.zeros(g.ndof())
+    rc_o, it_o, res_o = o.cg_solve(b, xo, xb=ub, maxit=256, tol=1e-7)
+    assert abs(cg.get_iteration_count() - it_o) <= 1
+    # CG amplifies rounding differences between iterate sequences, so the
+    # 1e-10 solution parity is checked with both solves run to 1e-13
+    xo = np.zeros(g.ndof())
+    o.cg_solve(b, xo, xb=ub, maxit=1000, tol=1e-13)
+    u = prob.zeros()
+    GCG(CGTraits(maxit=1000, tol=1e-13), prob).solve(L, dev(b), dev(ub), u)
+    assert relerr(host(u), xo) < 1e-10
+
+
+@pytest.mark.parametrize("precond", [0, 1])
+def test_cg_helmholtz_3d_matches_oracle(ctx, precond):
+    g, prob, o = setup(ctx, 3, [3, 3, 3], 5)
+    rng = np.random.default_rng(4)
+    f = rng.standard_normal(g.ndof())
+    f = f[g.members[g.class_ptr[:-1]]][g.node_class]
+    b = o.mass * f
+    dinv = 1.0 / o.helmholtz_diag(1.0, np.ones(g.ndof())) if precond else None
+    xo = np.zeros(g.ndof())
+    rc_o, it_o, _ = o.cg_solve(b, xo, p=1.0, q_vec=np.ones(g.ndof()), xb=np.zeros(g.ndof()),
+                               maxit=2000, tol=1e-13, dinv=dinv)
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    cg = GCG(CGTraits(maxit=2000, tol=1e-13, precond=precond, check_every=4), prob)
+    x = prob.zeros()
+    rc = cg.solve(H, dev(b), dev(np.zeros(g.ndof())), x)
+    assert rc == 0 and rc_o == 0
+    assert abs(cg.get_iteration_count() - it_o) <= 2
+    assert relerr(host(x), xo) < 1e-10
+
+
+def test_cg_mixed_precision_reaches_fp64_solution(ctx):
+    g, prob, o = setup(ctx, 3, [3, 3, 3], 6)
+    rng = np.random.default_rng(8)
+    f = rng.standard_normal(g.ndof())
+    f = f[g.members[g.class_ptr[:-1]]][g.node_class]
+    b = o.mass * f
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    x64 = prob.zeros()
+    GCG(CGTraits(maxit=5000, tol=1e-12, precond=1), prob).solve(H, dev(b), dev(0 * b), x64)
+    xm = prob.zeros()
+    cgm = GCG(CGTraits(maxit=5000, tol=1e-12, precond=1, precision=A.GF_CG_MIXED), prob)
+    rc = cgm.solve(H, dev(b), dev(0 * b), xm)
+    assert rc == 0
+    assert relerr(host(xm), host(x64)) < 1e-9
+
+
+def test_rk4_advection_2d_matches_oracle(ctx):
+    """Config-1 shape (2D periodic advection-diffusion, RK4), fewer steps."""
+    g, prob, o = setup(ctx, 2, [16, 16], 4, [1, 1], mask=False)
+    x, y = g.xyz
+    rng = np.random.default_rng(20261204)
+    noise = rng.uniform(-1e-3, 1e-3, g.nclass)[g.node_class]
+    u0 = np.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / 0.01)
+    u0 = u0[g.members[g.class_ptr[:-1]]][g.node_class] + noise
+    c = [np.ones(g.ndof()), 0.5 * np.ones(g.ndof())]
+    ut = [dev(u0)]
+    B = GBurgers(prob, GBurgers.ADVECT, 0.01, scheme=A.GF_RK4)
+    B.step(ut, [dev(a) for a in c], dt=1e-4, nsteps=20)
+    uo = [u0.copy()]
+    o.rk_advance(0, 0.01, 4, uo, c=c, dt=1e-4, nsteps=20)
+    assert relerr(host(ut[0]), uo[0]) < 1e-10
+
+
+@pytest.mark.parametrize("scheme", [1, 2, 3, 22, 33, 34])
+def test_rk_schemes_burgers_3d_match_oracle(ctx, scheme):
+    g, prob, o = setup(ctx, 3, [2, 2, 2], 4, [1, 1, 1], mask=False)
+    x, y, z = g.xyz
+    tp = 2 * np.pi
+    u0 = [0.3 * np.sin(tp * x) * np.cos(tp * y), -0.2 * np.cos(tp * z), 0.1 * np.sin(tp * y)]
+    u0 = [a[g.members[g.class_ptr[:-1]]][g.node_class] for a in u0]
+    ut = [dev(a) for a in u0]
+    B = GBurgers(prob, GBurgers.BURGERS, 1e-2, scheme=scheme)
+    B.step(ut, None, dt=2e-3, nsteps=5)
+    uo = [a.copy() for a in u0]
+    o.rk_advance(1, 1e-2, scheme, uo, dt=2e-3, nsteps=5)
+    for k in range(3):
+        assert relerr(host(ut[k]), uo[k]) < 1e-10
