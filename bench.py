@@ -59,7 +59,14 @@ def parse():
     ap.add_argument("--rk-p", type=int, default=5)
     ap.add_argument("--no-rk", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-sample-ne", type=int, default=8)
+    ap.add_argument("--cpu-sample-ne", type=int, default=16)
+    ap.add_argument("--cpu-iters", type=int, default=150)
+    ap.add_argument("--ru", type=int, default=32,
+                    help="FP32 iterations between FP64 residual replacements (mixed solve)")
+    ap.add_argument("--mixed-apply", type=int, default=0,
+                    help="mixed solve: 1 = FP64 arithmetic in the FP32-stored applies")
+    ap.add_argument("--only", choices=["fp64", "mixed", "apply"], default=None,
+                    help="time only one CG path (for profiling runs)")
     return ap.parse_args()
 
 
@@ -317,10 +324,11 @@ def cpu_oracle_iteration_time(sample_ne, p, iters=6):
     dinv = 1.0 / g.helmholtz_diag(1.0, np.ones(g.N))
     q = np.ones(g.N)
     zb = np.zeros(g.N)
+    # a tolerance no residual reaches, so that exactly maxit iterations run
     t0 = time.perf_counter()
-    g.cg_solve(b, np.zeros(g.N), p=1.0, q_vec=q, xb=zb, maxit=1, tol=0.0, dinv=dinv)
+    g.cg_solve(b, np.zeros(g.N), p=1.0, q_vec=q, xb=zb, maxit=1, tol=1e-300, dinv=dinv)
     t1 = time.perf_counter()
-    g.cg_solve(b, np.zeros(g.N), p=1.0, q_vec=q, xb=zb, maxit=1 + iters, tol=0.0, dinv=dinv)
+    g.cg_solve(b, np.zeros(g.N), p=1.0, q_vec=q, xb=zb, maxit=1 + iters, tol=1e-300, dinv=dinv)
     t2 = time.perf_counter()
     per_iter = ((t2 - t1) - (t1 - t0)) / iters
     return per_iter / g.N, g.N, (t2 - t0)
@@ -338,7 +346,7 @@ def run_reference(args, ws, rank):
         cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, iters=2)
     nsample = 0
     for _ in range(args.steps):
-        t, nsample, _w = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, iters=3)
+        t, nsample, _w = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, iters=20)
         per_node.append(t)
     t_iter = statistics.mean(per_node) * n_full
     iters = REF_ITERS_32_P7 if (args.ne, args.p) == (32, 7) and REF_ITERS_32_P7 else None
@@ -383,9 +391,21 @@ def main():
     H.set_Lap_scalar(1.0)
     H.set_mass_scalar(1.0)
     common = dict(maxit=50000, normtype=A.GF_NORM_EUC, tol=args.tol, precond=A.GF_PRECOND_JACOBI,
-                  check_every=32, relative=1)
-    tr_mix = CGTraits(precision=A.GF_CG_MIXED, inner_tol=1e-5, max_refine=60, **common)
-    tr_64 = CGTraits(precision=A.GF_CG_FP64, **common)
+                  relative=1)
+    # mixed: FP64 residual replacement every args.ru FP32 iterations
+    tr_mix = CGTraits(precision=A.GF_CG_MIXED, check_every=args.ru, mixed_apply=args.mixed_apply,
+                      **common)
+    tr_64 = CGTraits(precision=A.GF_CG_FP64, check_every=32, **common)
+    if args.only == "apply":
+        roof = kernel_roofline(ctx, prob, measured_peaks(), reps=args.steps)
+        print(json.dumps({"only": "apply", "helm3d": roof}), flush=True)
+        return
+    if args.only:
+        tr = tr_64 if args.only == "fp64" else tr_mix
+        t, it, rc, _ = time_solves(ctx, prob, H, b, tr, args.steps, args.warmup)
+        print(json.dumps({"only": args.only, "s_per_solve": statistics.mean(t),
+                          "iterations": it[-1], "rc": rc}), flush=True)
+        return
 
     def barrier():
         torch.cuda.synchronize()
@@ -424,7 +444,7 @@ def main():
         rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        t_node, nsample, wall = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p)
+        t_node, nsample, wall = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, args.cpu_iters)
         t_cpu = t_node * prob.nlocal * statistics.mean(it_64)
         cpu = {"value": t_cpu, "unit": "s", "cores": 1, "kind": "port",
                "sample": (f"oracle FP64 Jacobi-PCG iterations on a {args.cpu_sample_ne}^3-element "

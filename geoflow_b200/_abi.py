@@ -37,6 +37,7 @@ class ProblemDesc(C.Structure):
         ("D", P_double), ("W", P_double), ("geom", c_int),
         ("elem_geom", P_double), ("node_geom", P_double), ("mask", P_double),
         ("nclass", c_int64), ("class_ptr", P_int32), ("members", P_int32),
+        ("box_ne", c_int * 3), ("box_periodic", c_int * 3),
     ]
 
 
@@ -44,7 +45,7 @@ class CGTraits(C.Structure):
     _fields_ = [
         ("maxit", c_int), ("normtype", c_int), ("tol", c_double), ("precond", c_int),
         ("precision", c_int), ("inner_tol", c_double), ("max_refine", c_int),
-        ("check_every", c_int), ("relative", c_int),
+        ("check_every", c_int), ("relative", c_int), ("mixed_apply", c_int),
     ]
 
 

@@ -1,20 +1,31 @@
-// api_cg.cu -- conjugate gradient on the assembled Helmholtz operator,
-// following GCG::solve_impl (solvers/gcg.ipp:239-382, the Deville-Fischer-
-// Mund form) with the reference's DSS Sum, Dirichlet mask, multiplicity-
-// weighted dots and norm-based stopping rule, plus a Jacobi preconditioner
-// and a mixed-precision (FP32 inner solve, FP64 residual and refinement)
-// variant, neither of which the reference has.
+// api_cg.cu -- conjugate gradient on the assembled Helmholtz operator.
 //
-// Every iteration is four kernels that never wait on the host:
-//   1. q = A w                         (fused element apply)
-//   2. q = mask * DSS_Sum(q), <w,q>    (class gather-reduce-scatter + dot;
-//      the last block forms alpha = rho / <w,q>)
-//   3. x += alpha w, r -= alpha q, z = P^-1 r, rho' = <r,z>, norm(r)
-//      (the last block forms beta, checks convergence, sets `done`)
-//   4. w = beta w + z
-// Scalars live in a device block; once `done` is set all later kernels of
-// the batch return at once, so batches of iterations can be queued ahead
-// and the host reads the state only every `check_every` iterations.
+// Semantics follow GCG::solve_impl (solvers/gcg.ipp:239-382, the
+// Deville-Fischer-Mund form): r = mask*DSS_Sum(b - A x), dots weighted by
+// 1/multiplicity, the stop rule norm(r) <= (norm(b) < 1 ? tol : tol*norm(b))
+// with norm(b) taken on the element-local b, and the xb lift of
+// solve_impl (2).  Additions the reference lacks: a Jacobi preconditioner,
+// a relative stop option and a mixed-precision solve (FP32 PCG on the
+// correction, FP64 residual and iterative refinement).
+//
+// B200 layout: the iteration vectors live on the unique nodes (one value
+// per GGFX class, 0.68x the element-local size at p = 7) where the
+// reference keeps duplicated element-local copies.  A multiplicity-weighted
+// element-local dot equals the plain unique-node dot, so the algorithm is
+// unchanged.  Per iteration four kernels run back to back with no host
+// round trip:
+//   1. q_E = A_e w   fused element apply, w gathered from the unique nodes
+//                    (box lattice indices computed, or node_class)
+//   2. q = mask * assemble(q_E), <w,q>   one thread per unique node folds
+//                    its element copies in ascending local id; the last
+//                    block forms alpha
+//   3. x += alpha w, r -= alpha q, rho' = <r, Dinv r>, norm(r); the last
+//                    block forms beta and sets `done` at convergence
+//   4. w = beta w + Dinv r
+// Batches of iterations are queued ahead; every kernel returns at once
+// when `done` is set, and the host reads the flag every `check_every`
+// iterations.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -39,20 +50,191 @@ enum {
   S_WQ,
   S_FLAG,   // 1: non-finite scalar (breakdown)
   S_BNORM,
-  S_NTOT,   // number of local nodes (EUC norm)
+  S_NTOT,   // number of element-local nodes (EUC norm)
   S_IVOL,   // 1/volume (L2, L1 norms)
   S_NORMT,  // norm type
-  S_REL,    // 1: rtol = tol * norm(b) always (inner solves)
+  S_REL,    // relative stop rule
+  S_RES,    // norm of the last assembled residual pass
   S_COUNT
 };
 
-struct CGVecs {
-  const double *mask;   // may be null
-  const double *imult;
-  const double *dinv;   // may be null
-  const double *mass;
-  double *hist;         // residual history (maxit)
+// ---- unique-node maps ----
+// rows(f) visits every unique node once, calling f(c, g) with its index c
+// and (box only) lattice coordinates g; each(c, g, f) calls f(m) for the
+// members m of the node in ascending local id; mult(c, g) is the count.
+
+// Box lattice of order N-1.  Blocks walk lattice rows (fixed gy, gz), so a
+// node's coordinates come from the launch shape, and the order being a
+// compile-time constant turns every % and / by p into a multiply-shift.
+template <int N>
+struct MapBox {
+  static constexpr int P = N - 1;
+  int dim, ne[3], per[3], M[3];
+  static MapBox make(const BoxLattice &L) {
+    MapBox m;
+    m.dim = L.dim;
+    m.sorted = 1;
+    for (int d = 0; d < 3; d++) {
+      m.ne[d] = L.ne[d];
+      m.per[d] = L.per[d];
+      m.M[d] = (int)L.M[d];
+      if (d < L.dim && L.per[d] && L.ne[d] == 1) m.sorted = 0;
+    }
+    return m;
+  }
+  template <class F>
+  __device__ __forceinline__ void rows(F f) const {
+    const int nrows = M[1] * M[2];
+    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+      const int g1 = row % M[1], g2 = row / M[1];
+      const int64_t base = (int64_t)row * M[0];
+      for (int g0 = threadIdx.x; g0 < M[0]; g0 += blockDim.x) {
+        const int g[3] = {g0, g1, g2};
+        f(base + g0, g);
+      }
+    }
+  }
+  int sorted;  // 0 when some periodic direction has a single element
+  // (element coordinate, local index) pairs of lattice coordinate g, dir d,
+  // in ascending element coordinate
+  __device__ __forceinline__ int cands(int d, int g, int (&ec)[2], int (&l)[2]) const {
+    const int r = g % P, q = g / P;
+    if (r != 0) {
+      ec[0] = q;
+      l[0] = r;
+      return 1;
+    }
+    if (per[d]) {
+      if (q == 0) {  // wraps: (0, 0) then (ne-1, P)
+        ec[0] = 0;
+        l[0] = 0;
+        ec[1] = ne[d] - 1;
+        l[1] = P;
+      } else {
+        ec[0] = q - 1;
+        l[0] = P;
+        ec[1] = q;
+        l[1] = 0;
+      }
+      return 2;
+    }
+    int k = 0;
+    if (q >= 1) {
+      ec[k] = q - 1;
+      l[k++] = P;
+    }
+    if (q < ne[d]) {
+      ec[k] = q;
+      l[k++] = 0;
+    }
+    return k;
+  }
+  // Members in ascending local id.  With every direction's candidates in
+  // ascending element coordinate, the (z, y, x) nesting already yields
+  // ascending element ids; only a single-element periodic direction (two
+  // members in one element) needs the explicit sort.
+  template <class F>
+  __device__ __forceinline__ void each(int64_t, const int (&g)[3], F f) const {
+    int ec[3][2], l[3][2], cnt[3] = {1, 1, 1};
+    ec[2][0] = ec[2][1] = 0;
+    l[2][0] = l[2][1] = 0;
+    for (int d = 0; d < dim; d++) cnt[d] = cands(d, g[d], ec[d], l[d]);
+    const int nn = dim > 2 ? N * N * N : N * N;
+    if (sorted) {
+#pragma unroll
+      for (int a = 0; a < 2; a++) {
+        if (a >= cnt[2]) break;
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+          if (b >= cnt[1]) break;
+#pragma unroll
+          for (int i = 0; i < 2; i++) {
+            if (i >= cnt[0]) break;
+            const int e = ec[0][i] + ne[0] * (ec[1][b] + ne[1] * ec[2][a]);
+            f((int64_t)(e * nn + (l[0][i] + N * (l[1][b] + N * l[2][a]))));
+          }
+        }
+      }
+      return;
+    }
+    int m[8];
+    int k = 0;
+    for (int a = 0; a < cnt[2]; a++)
+      for (int b = 0; b < cnt[1]; b++)
+        for (int i = 0; i < cnt[0]; i++) {
+          const int e = ec[0][i] + ne[0] * (ec[1][b] + ne[1] * ec[2][a]);
+          m[k++] = e * nn + (l[0][i] + N * (l[1][b] + N * l[2][a]));
+        }
+    for (int i = 1; i < k; i++) {
+      const int v = m[i];
+      int j = i - 1;
+      while (j >= 0 && m[j] > v) {
+        m[j + 1] = m[j];
+        j--;
+      }
+      m[j + 1] = v;
+    }
+    for (int i = 0; i < k; i++) f((int64_t)m[i]);
+  }
+  __device__ __forceinline__ double mult(int64_t, const int (&g)[3]) const {
+    int m = 1;
+    for (int d = 0; d < dim; d++) {
+      int ec[2], l[2];
+      m *= cands(d, g[d], ec, l);
+    }
+    return (double)m;
+  }
+  __device__ __forceinline__ int64_t lof(int64_t i) const {  // E index -> lattice index
+    constexpr int NN = N * N;
+    const int64_t nn = dim > 2 ? (int64_t)NN * N : NN;
+    const int64_t e = i / nn;
+    const int a = (int)(i - e * nn);
+    const int c0 = (int)(e % ne[0]);
+    const int64_t r = e / ne[0];
+    const int c1 = (int)(r % ne[1]), c2 = dim > 2 ? (int)(r / ne[1]) : 0;
+    auto g1 = [&](int d, int ec, int l) {
+      int gi = ec * P + l;
+      return (per[d] && gi == M[d]) ? 0 : gi;
+    };
+    int64_t idx = g1(0, c0, a % N) + (int64_t)M[0] * g1(1, c1, (a / N) % N);
+    if (dim > 2) idx += (int64_t)M[0] * M[1] * g1(2, c2, a / NN);
+    return idx;
+  }
 };
+
+struct MapCsr {
+  const int32_t *ptr, *mem, *ncls;
+  int64_t nL;
+  template <class F>
+  __device__ __forceinline__ void rows(F f) const {
+    const int g[3] = {0, 0, 0};
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nL;
+         c += (int64_t)gridDim.x * blockDim.x)
+      f(c, g);
+  }
+  template <class F>
+  __device__ __forceinline__ void each(int64_t c, const int (&)[3], F f) const {
+    for (int32_t k = ptr[c]; k < ptr[c + 1]; k++) f((int64_t)mem[k]);
+  }
+  __device__ __forceinline__ double mult(int64_t c, const int (&)[3]) const {
+    return (double)(ptr[c + 1] - ptr[c]);
+  }
+  __device__ __forceinline__ int64_t lof(int64_t i) const { return ncls[i]; }
+};
+
+struct Weights {
+  const uint8_t *maskL;  // 1 keep, 0 Dirichlet; null: no mask
+  const double *massL;   // L2/L1 norms
+  const uint8_t *multL;  // multiplicity (EUC norm)
+};
+
+__device__ __forceinline__ double norm_term_L(int normtype, double r, const Weights &wt,
+                                              int64_t c) {
+  if (normtype == GF_NORM_INF) return fabs(r);
+  if (normtype == GF_NORM_EUC) return (double)wt.multL[c] * (r * r);
+  if (normtype == GF_NORM_L2) return wt.massL[c] * (r * r);
+  return wt.massL[c] * fabs(r);
+}
 
 __device__ __forceinline__ double finish_norm(int normtype, double v, const double *scal) {
   if (normtype == GF_NORM_INF) return v;
@@ -61,70 +243,172 @@ __device__ __forceinline__ double finish_norm(int normtype, double v, const doub
   return v * scal[S_IVOL];
 }
 
-// contribution of node i to the norm partial of type normtype
-__device__ __forceinline__ double norm_term(int normtype, double r, const double *mass, int64_t i) {
-  if (normtype == GF_NORM_INF) return fabs(r);
-  if (normtype == GF_NORM_EUC) return r * r;
-  if (normtype == GF_NORM_L2) return mass[i] * (r * r);
-  return mass[i] * fabs(r);
+template <bool MAX>
+__device__ __forceinline__ double acc(double a, double t) {
+  return MAX ? fmax(a, t) : a + t;
 }
 
-// r = b - Ax (in place on ax -> r)
-template <typename T>
-__global__ void k_cg_resid(int64_t n, const T *__restrict__ b, const T *__restrict__ ax,
-                           T *__restrict__ r) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    T v = b[i];
-    v -= ax[i];
-    r[i] = v;
+#define GRID_STRIDE(i, n)                                                        \
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n);     \
+       i += (int64_t)gridDim.x * blockDim.x)
+
+// ---- E <-> L conversions ----
+// out_L[c] = sum of the element copies (ascending local id), FP64
+template <class MAP, typename TI>
+__global__ void k_assemble(int64_t nL, MAP map, const TI *__restrict__ inE, double *__restrict__ outL) {
+  map.rows([&](int64_t c, const int(&g)[3]) {
+    double s = 0.0;
+    map.each(c, g, [&](int64_t m) { s = __dadd_rn(s, (double)inE[m]); });
+    outL[c] = s;
+  });
+}
+
+// x_L[c] = x_E[smallest member]  (x_E is duplicate-consistent)
+template <class MAP>
+__global__ void k_pick(int64_t nL, MAP map, const double *__restrict__ xE, double *__restrict__ xL) {
+  map.rows([&](int64_t c, const int(&g)[3]) {
+    bool first = true;
+    double v = 0.0;
+    map.each(c, g, [&](int64_t m) {
+      if (first) v = xE[m];
+      first = false;
+    });
+    xL[c] = v;
+  });
+}
+
+// x_E = mask_E * x_L[class] + xb_E   (solve_impl (2) epilogue)
+template <class MAP>
+__global__ void k_scatter(int64_t nE, MAP map, const double *__restrict__ xL,
+                          const double *__restrict__ maskE, const double *__restrict__ xbE,
+                          double *__restrict__ xE) {
+  GRID_STRIDE(i, nE) {
+    double v = xL[map.lof(i)];
+    if (maskE) v *= maskE[i];
+    if (xbE) v += xbE[i];
+    xE[i] = v;
   }
 }
 
-// x = mask*x + xb  (solve_impl (2) prologue) or x = mask*x + xb at exit
-template <typename T>
-__global__ void k_cg_lift(int64_t n, const double *__restrict__ mask, const T *__restrict__ xb,
-                          T *__restrict__ x) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    T v = x[i];
-    if (mask) v *= (T)mask[i];
-    if (xb) v += xb[i];
-    x[i] = v;
+// x_E = mask_E * x_E + xb_E   (solve_impl (2) prologue)
+__global__ void k_lift(int64_t nE, const double *__restrict__ maskE, const double *__restrict__ xbE,
+                       double *__restrict__ xE) {
+  GRID_STRIDE(i, nE) {
+    double v = xE[i];
+    if (maskE) v *= maskE[i];
+    if (xbE) v += xbE[i];
+    xE[i] = v;
   }
 }
 
-// DSS Sum + mask over classes; with DOT also accumulates <w,q>_imult and
-// the last block forms alpha = rho / <w,q>.
-template <typename T, bool DOT>
+// norm of the element-local b (the reference measures b as given)
 __global__ void __launch_bounds__(RED_THREADS)
-    k_cg_dss(int64_t nclass, const int32_t *__restrict__ ptr, const int32_t *__restrict__ mem,
-             const double *__restrict__ mask, const double *__restrict__ imult,
-             const T *__restrict__ w, T *__restrict__ q, double *scal, double *partials,
-             unsigned int *counter) {
+    k_norm_E(int64_t n, int normtype, const double *__restrict__ b, const double *__restrict__ mass,
+             double *scal, double *partials, unsigned int *counter) {
+  __shared__ double sh[32];
+  double rn = 0.0;
+  GRID_STRIDE(i, n) {
+    double t;
+    if (normtype == GF_NORM_INF) t = fabs(b[i]);
+    else if (normtype == GF_NORM_EUC) t = b[i] * b[i];
+    else if (normtype == GF_NORM_L2) t = mass[i] * (b[i] * b[i]);
+    else t = mass[i] * fabs(b[i]);
+    rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
+  }
+  rn = normtype == GF_NORM_INF ? block_reduce<true>(rn, sh) : block_reduce<false>(rn, sh);
+  double pv[1] = {rn};
+  if (publish_partials<1>(pv, partials, counter, gridDim.x)) {
+    double t = normtype == GF_NORM_INF ? fold_partials<true>(partials, gridDim.x, sh)
+                                       : fold_partials<false>(partials, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      scal[S_BNORM] = finish_norm(normtype, t, scal);
+      *counter = 0;
+    }
+  }
+}
+
+// Residual pass: r = mask * (b_L - assemble(q_E)) in FP64; also writes the
+// solve-precision copy r_T and rho = <r_T, Dinv r_T>.
+//   mode 0 (start): w_T = Dinv r_T and a fresh CG state: rtol from the
+//     reference rule on norm(b), rnorm = 10 rtol, iter = 0.
+//   mode 2 (reliable update of the mixed solve): the search direction w_T
+//     and the iteration count are kept; rnorm becomes the true residual
+//     norm and `done` is set only if that meets rtol (or maxit is spent).
+template <typename T, class MAP>
+__global__ void __launch_bounds__(RED_THREADS)
+    k_resid(int64_t nL, MAP map, Weights wt, const double *__restrict__ bL,
+            const double *__restrict__ qE, double *__restrict__ rL, T *__restrict__ rT,
+            T *__restrict__ wT, const T *__restrict__ dinv, int mode, double tol, double *scal,
+            double *partials, unsigned int *counter) {
+  __shared__ double sh[32];
+  const int normtype = (int)scal[S_NORMT];
+  double rho = 0.0, rn = 0.0;
+  map.rows([&](int64_t c, const int(&g)[3]) {
+    double s = 0.0;
+    map.each(c, g, [&](int64_t m) { s = __dadd_rn(s, qE[m]); });
+    double r = bL[c] - s;
+    if (wt.maskL && !wt.maskL[c]) r = 0.0;
+    rL[c] = r;
+    const T rt = (T)r;
+    const T zt = dinv ? dinv[c] * rt : rt;
+    if (rT != (T *)rL) rT[c] = rt;
+    if (mode != 2) wT[c] = zt;
+    rho += (double)rt * (double)zt;
+    const double t = norm_term_L(normtype, r, wt, c);
+    rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
+  });
+  rho = block_reduce<false>(rho, sh);
+  rn = normtype == GF_NORM_INF ? block_reduce<true>(rn, sh) : block_reduce<false>(rn, sh);
+  double pv[2] = {rho, rn};
+  if (publish_partials<2>(pv, partials, counter, gridDim.x)) {
+    double rho_t = fold_partials<false>(partials, gridDim.x, sh);
+    double rn_t = normtype == GF_NORM_INF ? fold_partials<true>(partials + gridDim.x, gridDim.x, sh)
+                                          : fold_partials<false>(partials + gridDim.x, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      const double rnorm = finish_norm(normtype, rn_t, scal);
+      scal[S_RES] = rnorm;
+      scal[S_RHO] = rho_t;
+      if (mode == 2) {
+        scal[S_RNORM] = rnorm;
+        const bool bad = !isfinite(rnorm) || !isfinite(rho_t);
+        if (bad) scal[S_FLAG] = 1.0;
+        scal[S_DONE] =
+            (rnorm <= scal[S_RTOL] || scal[S_ITER] >= scal[S_MAXIT] || bad) ? 2.0 : 0.0;
+      } else {
+        const double bnorm = scal[S_BNORM];
+        const double rtol = (scal[S_REL] != 0.0 || bnorm >= 1.0) ? tol * bnorm : tol;
+        scal[S_RTOL] = rtol;
+        scal[S_RNORM] = 10.0 * rtol;
+        scal[S_ITER] = 0.0;
+        scal[S_FLAG] = 0.0;
+        scal[S_DONE] = (scal[S_MAXIT] <= 0.0 || !(10.0 * rtol > rtol)) ? 1.0 : 0.0;
+      }
+      *counter = 0;
+    }
+  }
+}
+
+// 2. q_L = mask * assemble(q_E); <w,q>; alpha
+template <typename T, class MAP>
+__global__ void __launch_bounds__(RED_THREADS)
+    k_asm_dot(int64_t nL, MAP map, Weights wt, const T *__restrict__ qE, const T *__restrict__ w,
+              T *__restrict__ qL, double *scal, double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
   double dot = 0.0;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nclass;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t b = ptr[c], e = ptr[c + 1];
+  map.rows([&](int64_t c, const int(&g)[3]) {
     T s = T(0);
-    for (int32_t k = b; k < e; k++) s = __fadd_rn_t(s, q[mem[k]]);
-    for (int32_t k = b; k < e; k++) {
-      const int32_t m = mem[k];
-      T v = s;
-      if (mask) v *= (T)mask[m];
-      q[m] = v;
-      if (DOT) dot += ((double)w[m] * (double)v) * imult[m];
-    }
-  }
-  if (!DOT) return;
+    map.each(c, g, [&](int64_t m) { s = __fadd_rn_t(s, qE[m]); });
+    if (wt.maskL && !wt.maskL[c]) s = T(0);
+    qL[c] = s;
+    dot += (double)w[c] * (double)s;
+  });
   dot = block_reduce<false>(dot, sh);
   double pv[1] = {dot};
   if (publish_partials<1>(pv, partials, counter, gridDim.x)) {
     double wq = fold_partials<false>(partials, gridDim.x, sh);
     if (threadIdx.x == 0) {
-      double alpha = scal[S_RHO] / wq;
+      const double alpha = scal[S_RHO] / wq;
       scal[S_WQ] = wq;
       scal[S_ALPHA] = alpha;
       if (!isfinite(alpha)) {
@@ -136,64 +420,25 @@ __global__ void __launch_bounds__(RED_THREADS)
   }
 }
 
-// z = P^-1 r; w = z; rho = <r,z>_imult; bnorm partial from b; sets rtol.
-template <typename T>
+// 3. x += alpha w; r -= alpha q; rho' = <r, Dinv r>; norm(r); beta; stop test
+template <typename T, class MAP>
 __global__ void __launch_bounds__(RED_THREADS)
-    k_cg_start(int64_t n, const T *__restrict__ b, const T *__restrict__ r, T *__restrict__ w,
-               CGVecs v, double tol, double *scal, double *partials, unsigned int *counter) {
-  __shared__ double sh[32];
-  const int normtype = (int)scal[S_NORMT];
-  double rho = 0.0, bn = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const T ri = r[i];
-    const T zi = v.dinv ? (T)v.dinv[i] * ri : ri;
-    w[i] = zi;
-    rho += ((double)ri * (double)zi) * v.imult[i];
-    const double t = norm_term(normtype, (double)b[i], v.mass, i);
-    bn = normtype == GF_NORM_INF ? fmax(bn, t) : bn + t;
-  }
-  rho = block_reduce<false>(rho, sh);
-  bn = normtype == GF_NORM_INF ? block_reduce<true>(bn, sh) : block_reduce<false>(bn, sh);
-  double pv[2] = {rho, bn};
-  if (publish_partials<2>(pv, partials, counter, gridDim.x)) {
-    double rho_t = fold_partials<false>(partials, gridDim.x, sh);
-    double bn_t = normtype == GF_NORM_INF ? fold_partials<true>(partials + gridDim.x, gridDim.x, sh)
-                                          : fold_partials<false>(partials + gridDim.x, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      double bnorm = finish_norm(normtype, bn_t, scal);
-      double rtol = (scal[S_REL] != 0.0 || bnorm >= 1.0) ? tol * bnorm : tol;
-      scal[S_RHO] = rho_t;
-      scal[S_BNORM] = bnorm;
-      scal[S_RTOL] = rtol;
-      scal[S_RNORM] = 10.0 * rtol;
-      scal[S_ITER] = 0.0;
-      scal[S_FLAG] = 0.0;
-      scal[S_DONE] = (scal[S_MAXIT] <= 0.0 || !(10.0 * rtol > rtol)) ? 1.0 : 0.0;
-      *counter = 0;
-    }
-  }
-}
-
-// x += alpha w; r -= alpha q; rho' = <r, P^-1 r>; norm(r); beta; stop test.
-template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-    k_cg_update(int64_t n, T *__restrict__ x, const T *__restrict__ w, T *__restrict__ r,
-                const T *__restrict__ q, CGVecs v, double *scal, double *partials,
-                unsigned int *counter) {
+    k_update(int64_t nL, MAP map, Weights wt, T *__restrict__ x, const T *__restrict__ w,
+             T *__restrict__ r, const T *__restrict__ q, const T *__restrict__ dinv,
+             double *__restrict__ hist, double *scal, double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
   const int normtype = (int)scal[S_NORMT];
   const T alpha = (T)scal[S_ALPHA];
   double rho = 0.0, rn = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] = x[i] + alpha * w[i];
-    const T ri = r[i] + (-alpha) * q[i];
-    r[i] = ri;
-    const T zi = v.dinv ? (T)v.dinv[i] * ri : ri;
-    rho += ((double)ri * (double)zi) * v.imult[i];
-    const double t = norm_term(normtype, (double)ri, v.mass, i);
+  // plain streaming over the unique nodes (no lattice information needed)
+  GRID_STRIDE(c, nL) {
+    x[c] = x[c] + alpha * w[c];
+    const T rc = r[c] + (-alpha) * q[c];
+    r[c] = rc;
+    const T zc = dinv ? dinv[c] * rc : rc;
+    rho += (double)rc * (double)zc;
+    const double t = norm_term_L(normtype, (double)rc, wt, c);
     rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
   }
   rho = block_reduce<false>(rho, sh);
@@ -210,43 +455,44 @@ __global__ void __launch_bounds__(RED_THREADS)
       scal[S_RHO] = rho_t;
       scal[S_BETA] = beta;
       scal[S_RNORM] = rnorm;
-      if (v.hist) v.hist[it] = rnorm;
+      if (hist) hist[it] = rnorm;
       scal[S_ITER] = (double)(it + 1);
-      if (!isfinite(rnorm) || !isfinite(beta)) scal[S_FLAG] = 1.0;
-      if (rnorm <= scal[S_RTOL] || it + 1 >= (int)scal[S_MAXIT] || !isfinite(rnorm) ||
-          !isfinite(beta))
-        scal[S_DONE] = 2.0;
+      const bool bad = !isfinite(rnorm) || !isfinite(beta);
+      if (bad) scal[S_FLAG] = 1.0;
+      if (rnorm <= scal[S_RTOL] || it + 1 >= (int)scal[S_MAXIT] || bad) scal[S_DONE] = 2.0;
       *counter = 0;
     }
   }
 }
 
-// w = beta w + z, z = P^-1 r.  Skipped once the solve has stopped.
+// 4. w = beta w + Dinv r
 template <typename T>
-__global__ void k_cg_wupdate(int64_t n, T *__restrict__ w, const T *__restrict__ r,
-                             const double *__restrict__ dinv, const double *scal) {
+__global__ void k_wupdate(int64_t nL, T *__restrict__ w, const T *__restrict__ r,
+                          const T *__restrict__ dinv, const double *scal) {
   if (scal[S_DONE] != 0.0) return;
   const T beta = (T)scal[S_BETA];
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const T ri = r[i];
-    const T zi = dinv ? (T)dinv[i] * ri : ri;
-    w[i] = beta * w[i] + T(1) * zi;
+  GRID_STRIDE(c, nL) {
+    const T rc = r[c];
+    const T zc = dinv ? dinv[c] * rc : rc;
+    w[c] = beta * w[c] + T(1) * zc;
   }
 }
 
-// local diagonal of p L + q M at every node (before DSS Sum)
-template <typename T>
+// x_L += (double) d_L
+__global__ void k_add_correction(int64_t nL, const float *__restrict__ d, double *__restrict__ x) {
+  GRID_STRIDE(c, nL) { x[c] += (double)d[c]; }
+}
+
+// local diagonal of p L + q M at every element-local node
 __global__ void k_helm_diag(int64_t n, int dim, int nb, Basis<double, GF_MAXN> B,
                             const double *__restrict__ egeom, const double *__restrict__ ngeom,
-                            double p, double q, int use_mass, T *__restrict__ diag) {
+                            double p, double q, int use_mass, double *__restrict__ diag) {
   const int nn = dim == 2 ? nb * nb : nb * nb * nb;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  GRID_STRIDE(i, n) {
     const int64_t e = i / nn;
     const int a = (int)(i % nn);
-    int li[3] = {a % nb, (a / nb) % nb, a / (nb * nb)};
-    int stride[3] = {1, nb, nb * nb};
+    const int li[3] = {a % nb, (a / nb) % nb, a / (nb * nb)};
+    const int stride[3] = {1, nb, nb * nb};
     double s = 0.0;
     for (int d = 0; d < dim; d++) {
       for (int m = 0; m < nb; m++) {
@@ -269,143 +515,118 @@ __global__ void k_helm_diag(int64_t n, int dim, int nb, Basis<double, GF_MAXN> B
     s *= p;
     if (use_mass) {
       const double J = egeom ? egeom[e * (dim + 1) + dim] : ngeom[(int64_t)dim * n + i];
-      const double w = dim == 2 ? B.W[li[1]] * B.W[li[0]]
-                                : B.W[li[2]] * B.W[li[1]] * B.W[li[0]];
+      const double w = dim == 2 ? B.W[li[1]] * B.W[li[0]] : B.W[li[2]] * B.W[li[1]] * B.W[li[0]];
       s += q * (w * J);
     }
-    diag[i] = (T)s;
+    diag[i] = s;
   }
 }
 
-__global__ void k_invert(int64_t n, double *__restrict__ d) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    d[i] = 1.0 / d[i];
-}
-
-// rnorm of an FP64 residual into scal[slot] (host reads it)
-__global__ void __launch_bounds__(RED_THREADS)
-    k_norm(int64_t n, int normtype, const double *__restrict__ r, const double *__restrict__ mass,
-           double *scal, int slot, double *partials, unsigned int *counter) {
-  __shared__ double sh[32];
-  double rn = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double t = norm_term(normtype, r[i], mass, i);
-    rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
-  }
-  rn = normtype == GF_NORM_INF ? block_reduce<true>(rn, sh) : block_reduce<false>(rn, sh);
-  double pv[1] = {rn};
-  if (publish_partials<1>(pv, partials, counter, gridDim.x)) {
-    double t = normtype == GF_NORM_INF ? fold_partials<true>(partials, gridDim.x, sh)
-                                       : fold_partials<false>(partials, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      scal[slot] = finish_norm(normtype, t, scal);
-      *counter = 0;
-    }
+__global__ void k_invert(int64_t n, const double *__restrict__ d, double *__restrict__ o64,
+                         float *__restrict__ o32) {
+  GRID_STRIDE(i, n) {
+    const double v = 1.0 / d[i];
+    o64[i] = v;
+    o32[i] = (float)v;
   }
 }
 
+// ---------------------------------------------------------------------
+template <class MAP>
 struct Solver {
   gf_problem *prob;
   gf_context *ctx;
   cudaStream_t st;
-  int64_t n;
-  unsigned gvec, gcls;
+  MAP map;
+  Weights wt;
+  int64_t nE, nL;
+  unsigned gE, gL, gRed;
 
-  explicit Solver(gf_problem *p) : prob(p), ctx(p->ctx), st(p->ctx->stream), n(p->nlocal) {
-    gvec = grid_for(n, RED_THREADS, std::min(p->npartials, ctx->sm_count * 4));
-    gcls = grid_for(p->nclass, RED_THREADS, std::min(p->npartials, ctx->sm_count * 4));
+  Solver(gf_problem *p, MAP m, bool masked)
+      : prob(p), ctx(p->ctx), st(p->ctx->stream), map(m), nE(p->nlocal), nL(p->nclass) {
+    wt.maskL = masked ? p->maskL8 : nullptr;
+    wt.massL = p->massL;
+    wt.multL = p->multL8;
+    gE = grid_for(nE, 256, ctx->sm_count * 8);
+    gL = grid_for(nL, 256, ctx->sm_count * 8);
+    gRed = grid_for(nL, RED_THREADS, std::min(p->npartials, ctx->sm_count * 8));
   }
 
-  // Jacobi inverse diagonal (assembled), FP64, cached in work slot 9
-  double *jacobi(double p, double q, int use_mass) {
-    double *d = (double *)gf_work(prob, 9, sizeof(double) * n);
-    if (!d) return nullptr;
+  void set_scalars(const gf_cg_traits &tr, int maxit, bool relative) {
+    double *h = prob->scal_h;
+    for (int i = 0; i < S_COUNT; i++) h[i] = 0.0;
+    h[S_MAXIT] = (double)maxit;
+    h[S_NTOT] = (double)nE;
+    h[S_NORMT] = (double)tr.normtype;
+    h[S_IVOL] = 1.0 / prob->volume;
+    h[S_REL] = relative ? 1.0 : 0.0;
+  }
+
+  // Jacobi inverse diagonal on unique nodes (FP64 and FP32), slots 8/9/10
+  int jacobi(double p, double q, int use_mass, double **d64, float **d32) {
+    double *dE = (double *)gf_work(prob, 8, sizeof(double) * nE);
+    double *dL = (double *)gf_work(prob, 9, sizeof(double) * nL);
+    float *fL = (float *)gf_work(prob, 10, sizeof(float) * nL);
+    double *iL = (double *)gf_work(prob, 7, sizeof(double) * nL);
+    if (!dE || !dL || !fL || !iL) return GF_ERR_NOMEM;
     Basis<double, GF_MAXN> B;
     for (int i = 0; i < prob->n * prob->n; i++) B.D[i] = prob->D[i];
     for (int i = 0; i < prob->n; i++) B.W[i] = prob->W[i];
-    unsigned g = grid_for(n, 256, ctx->sm_count * 8);
-    prob->launches++;
-    k_helm_diag<double><<<g, 256, 0, st>>>(n, prob->dim, prob->n, B, prob->egeom_d, prob->ngeom_d,
-                                           p, q, use_mass, d);
-    launch_dss<double>(prob, GF_DSS_SUM, d, st);
-    prob->launches++;
-    k_invert<<<g, 256, 0, st>>>(n, d);
-    return d;
+    prob->launches += 3;
+    k_helm_diag<<<gE, 256, 0, st>>>(nE, prob->dim, prob->n, B, prob->egeom_d, prob->ngeom_d, p, q,
+                                    use_mass, dE);
+    k_assemble<MAP, double><<<gL, 256, 0, st>>>(nL, map, dE, dL);
+    k_invert<<<gL, 256, 0, st>>>(nL, dL, iL, fL);
+    *d64 = iL;
+    *d32 = fL;
+    return GF_OK;
   }
 
-  // One CG solve in precision T on device vectors; x holds the initial
-  // guess.  b: right-hand side; xb: boundary lift or null.  Returns the
-  // GCGERR-style code; iterations in *iters.
+  // enqueue k CG iterations in precision T (each returns at once once the
+  // device `done` flag is set)
+  int mixed_apply = 0;  // FP64 arithmetic in the FP32 applies
+
   template <typename T>
-  int solve(const gf_cg_traits &tr, double p, double q, int use_mass, const T *b, const T *xb,
-            T *x, bool bbv, double tol, bool relative, int maxit, const double *dinv, double *hist,
-            int *iters, double *rnorm_out, int slot0) {
-    T *r = (T *)gf_work(prob, slot0 + 0, sizeof(T) * n);
-    T *w = (T *)gf_work(prob, slot0 + 1, sizeof(T) * n);
-    T *qv = (T *)gf_work(prob, slot0 + 2, sizeof(T) * n);
-    if (!r || !w || !qv) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
+  void enqueue(int k, double p, double q, int use_mass, T *x, T *r, T *w, T *qL, T *qE,
+               const T *dinv, double *hist) {
     double *scal = prob->scal_d;
-    const double *mask = bbv ? prob->mask_d : nullptr;
-    CGVecs v{mask, prob->imult_d, dinv, prob->mass_d, hist};
-    // scalars
-    double init[S_COUNT] = {0};
-    init[S_MAXIT] = (double)maxit;
-    init[S_NTOT] = (double)n;
-    init[S_NORMT] = (double)tr.normtype;
-    init[S_IVOL] = 1.0 / prob->volume;
-    init[S_REL] = relative ? 1.0 : 0.0;
-    std::copy(init, init + S_COUNT, prob->scal_h);
-    GF_CUDA(ctx, cudaMemcpyAsync(scal, prob->scal_h, sizeof(double) * S_COUNT,
-                                 cudaMemcpyHostToDevice, st));
-    unsigned gel = grid_for(n, 256, ctx->sm_count * 8);
-    if (bbv && (xb || mask)) {
-      prob->launches++;
-      k_cg_lift<T><<<gel, 256, 0, st>>>(n, mask, xb, x);
+    for (int i = 0; i < k; i++) {
+      if (std::is_same<T, float>::value && mixed_apply && prob->dim == 3)
+        launch_helm_L_f32io(prob, p, q, use_mass, (const float *)w, (float *)qE, st, scal + S_DONE);
+      else
+        launch_helm_L<T>(prob, (T)p, (T)q, use_mass, w, qE, st, scal + S_DONE);
+      k_asm_dot<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, qE, w, qL, scal, prob->partials,
+                                                      prob->counter);
+      k_update<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, x, w, r, qL, dinv, hist, scal,
+                                                     prob->partials, prob->counter);
+      k_wupdate<T><<<gL, 256, 0, st>>>(nL, w, r, dinv, scal);
+      prob->launches += 3;
     }
-    // r = b - A x; DSS Sum; mask
-    int rc = launch_helm<T>(prob, (T)p, nullptr, (T)q, nullptr, use_mass, x, w, st);
-    if (rc) return gf_fail(ctx, rc, "apply failed");
-    prob->launches++;
-    k_cg_resid<T><<<gel, 256, 0, st>>>(n, b, w, r);
-    prob->launches++;
-    k_cg_dss<T, false><<<gcls, RED_THREADS, 0, st>>>(prob->nclass, prob->class_ptr, prob->members,
-                                                      mask, prob->imult_d, w, r, scal,
-                                                      prob->partials, prob->counter);
-    prob->launches++;
-    k_cg_start<T><<<gvec, RED_THREADS, 0, st>>>(n, b, r, w, v, tol, scal, prob->partials,
-                                               prob->counter);
-    GF_CHECK_LAUNCH(ctx);
+  }
+
+  // PCG iterations in precision T on unique-node vectors; the state
+  // (rho, rtol, done) was set up by k_resid.  Returns iterations done.
+  template <typename T>
+  int iterate(const gf_cg_traits &tr, int maxit, double p, double q, int use_mass, T *x, T *r, T *w,
+              T *qL, T *qE, const T *dinv, double *hist, int *iters) {
+    double *scal = prob->scal_d;
     const int every = tr.check_every > 0 ? tr.check_every : 16;
-    int issued = 0;
+    int issued = 0, pending = -1;
+    bool stop = false;
+    double *hbuf = prob->scal_h + 32;
     cudaEvent_t ev[2];
     cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
-    double *hbuf = prob->scal_h + 32;  // two host slots of S_COUNT..: DONE, ITER
-    int pending = -1;
-    bool stop = false;
-    int status = 0;
+    // the state may already be converged (maxit 0 or tol 0)
     while (!stop) {
-      // enqueue a batch
-      for (int k = 0; k < every && issued < maxit; k++, issued++) {
-        launch_helm<T>(prob, (T)p, nullptr, (T)q, nullptr, use_mass, w, qv, st, scal + S_DONE);
-        prob->launches++;
-        k_cg_dss<T, true><<<gcls, RED_THREADS, 0, st>>>(prob->nclass, prob->class_ptr,
-                                                         prob->members, mask, prob->imult_d, w,
-                                                         qv, scal, prob->partials, prob->counter);
-        prob->launches++;
-        k_cg_update<T><<<gvec, RED_THREADS, 0, st>>>(n, x, w, r, qv, v, scal, prob->partials,
-                                                    prob->counter);
-        prob->launches++;
-        k_cg_wupdate<T><<<gel, 256, 0, st>>>(n, w, r, dinv, scal);
-      }
+      const int k = std::min(every, maxit - issued);
+      enqueue<T>(k, p, q, use_mass, x, r, w, qL, qE, dinv, hist);
+      issued += k;
       GF_CHECK_LAUNCH(ctx);
       const int slot = (pending + 1) & 1;
       GF_CUDA(ctx, cudaMemcpyAsync(hbuf + 2 * slot, scal + S_DONE, sizeof(double) * 2,
                                    cudaMemcpyDeviceToHost, st));
       cudaEventRecord(ev[slot], st);
-      // wait for the previous batch's flag while this one runs
       if (pending >= 0) {
         cudaEventSynchronize(ev[pending]);
         if (hbuf[2 * pending] != 0.0) stop = true;
@@ -422,19 +643,130 @@ struct Solver {
     GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h, scal, sizeof(double) * S_COUNT,
                                  cudaMemcpyDeviceToHost, st));
     GF_CUDA(ctx, cudaStreamSynchronize(st));
-    const int it = (int)prob->scal_h[S_ITER];
-    const double rn = prob->scal_h[S_RNORM];
-    if (iters) *iters = it;
-    if (rnorm_out) *rnorm_out = rn;
-    if (prob->scal_h[S_FLAG] != 0.0) status = GF_ERR_NONFINITE;
-    if (bbv) {
-      prob->launches++;
-      k_cg_lift<T><<<gel, 256, 0, st>>>(n, prob->mask_d, xb, x);
-    }
-    GF_CHECK_LAUNCH(ctx);
-    if (status) return gf_fail(ctx, status, "CG breakdown: non-finite scalar at iteration %d", it);
-    if (it >= maxit && rn > tr.tol) return GF_CG_NOCONVERGE;
+    *iters = (int)prob->scal_h[S_ITER];
+    if (prob->scal_h[S_FLAG] != 0.0)
+      return gf_fail(ctx, GF_ERR_NONFINITE, "CG breakdown: non-finite scalar at iteration %d",
+                     *iters);
     return GF_OK;
+  }
+
+  // FP64 residual pass for x_L: r_L = mask (b_L - A x); writes solve-
+  // precision copies rT, wT = Dinv rT and sets up the CG state.
+  template <typename T>
+  int residual(double p, double q, int use_mass, const double *bL, const double *xL, double *qE,
+               double *rL, T *rT, T *wT, const T *dinv, int mode, double tol) {
+    int rc = launch_helm_L<double>(prob, p, q, use_mass, xL, qE, st);
+    if (rc) return rc;
+    prob->launches++;
+    k_resid<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, bL, qE, rL, rT, wT, dinv, mode, tol,
+                                                  prob->scal_d, prob->partials, prob->counter);
+    GF_CHECK_LAUNCH(ctx);
+    return GF_OK;
+  }
+
+  double read_scalar(int slot) {
+    cudaMemcpyAsync(prob->scal_h + slot, prob->scal_d + slot, sizeof(double),
+                    cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return prob->scal_h[slot];
+  }
+
+  int solve(const gf_cg_traits &tr, double p, double q, int use_mass, const double *bE,
+            const double *xbE, double *xE, int *iters_out, double *rn_out, double *hist) {
+    const bool bbv = xbE != nullptr;
+    const double *maskE = bbv ? prob->mask_d : nullptr;
+    double *bL = (double *)gf_work(prob, 0, sizeof(double) * nL);
+    double *xL = (double *)gf_work(prob, 1, sizeof(double) * nL);
+    double *rL = (double *)gf_work(prob, 2, sizeof(double) * nL);
+    double *qE = (double *)gf_work(prob, 3, sizeof(double) * nE);
+    if (!bL || !xL || !rL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
+    double *d64 = nullptr;
+    float *d32 = nullptr;
+    if (tr.precond == GF_PRECOND_JACOBI) {
+      int rc = jacobi(p, q, use_mass, &d64, &d32);
+      if (rc) return gf_fail(ctx, rc, "Jacobi set-up failed");
+    }
+    set_scalars(tr, tr.maxit, tr.relative != 0);
+    GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_d, prob->scal_h, sizeof(double) * S_COUNT,
+                                 cudaMemcpyHostToDevice, st));
+    // prologue: x = mask x + xb; b_L = assemble(b); x_L = x; norm(b)
+    prob->launches += 4;
+    if (bbv) k_lift<<<gE, 256, 0, st>>>(nE, maskE, xbE, xE);
+    k_assemble<MAP, double><<<gL, 256, 0, st>>>(nL, map, bE, bL);
+    k_pick<MAP><<<gL, 256, 0, st>>>(nL, map, xE, xL);
+    k_norm_E<<<grid_for(nE, RED_THREADS, prob->npartials), RED_THREADS, 0, st>>>(
+        nE, tr.normtype, bE, prob->mass_d, prob->scal_d, prob->partials, prob->counter);
+    int rc = GF_OK, total = 0;
+    double rn = 0.0;
+    if (tr.precision == GF_CG_FP64) {
+      double *w = (double *)gf_work(prob, 4, sizeof(double) * nL);
+      double *qL = (double *)gf_work(prob, 5, sizeof(double) * nL);
+      if (!w || !qL) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
+      rc = residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, w, d64, 0, tr.tol);
+      if (rc) return gf_fail(ctx, rc, "residual failed");
+      rc = iterate<double>(tr, tr.maxit, p, q, use_mass, xL, rL, w, qL, qE, d64, hist, &total);
+      if (rc) return rc;
+      rn = prob->scal_h[S_RNORM];
+      rc = (total >= tr.maxit && rn > tr.tol) ? GF_CG_NOCONVERGE : GF_OK;
+    } else {
+      // mixed: FP64 residual -> FP32 PCG correction -> FP64 update
+      float *r32 = (float *)gf_work(prob, 11, sizeof(float) * nL);
+      float *w32 = (float *)gf_work(prob, 12, sizeof(float) * nL);
+      float *x32 = (float *)gf_work(prob, 13, sizeof(float) * nL);
+      float *q32 = (float *)gf_work(prob, 14, sizeof(float) * nL);
+      float *qE32 = (float *)gf_work(prob, 15, sizeof(float) * nE);
+      if (!r32 || !w32 || !x32 || !q32 || !qE32)
+        return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
+      // Reliable updates (Sleijpen & van der Vorst 1996): one FP32 PCG run
+      // on the correction y; every `check_every` iterations y is folded
+      // into the FP64 x and the FP32 residual is replaced by the true FP64
+      // residual b - A x, keeping the search direction, so the Krylov space
+      // is never restarted.  The solve stops only on the true residual.
+      const int every = tr.check_every > 0 ? tr.check_every : 32;
+      mixed_apply = tr.mixed_apply;
+      int r2 = residual<float>(p, q, use_mass, bL, xL, qE, rL, r32, w32, d32, 0, tr.tol);
+      if (r2) return gf_fail(ctx, r2, "residual failed");
+      GF_CUDA(ctx, cudaMemsetAsync(x32, 0, sizeof(float) * nL, st));
+      rc = GF_CG_NOCONVERGE;
+      for (;;) {
+        enqueue<float>(every, p, q, use_mass, x32, r32, w32, q32, qE32, d32, nullptr);
+        prob->launches += 1;
+        k_add_correction<<<gL, 256, 0, st>>>(nL, x32, xL);
+        GF_CUDA(ctx, cudaMemsetAsync(x32, 0, sizeof(float) * nL, st));
+        r2 = residual<float>(p, q, use_mass, bL, xL, qE, rL, r32, w32, d32, 2, tr.tol);
+        if (r2) return gf_fail(ctx, r2, "residual failed");
+        GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h, prob->scal_d, sizeof(double) * S_COUNT,
+                                     cudaMemcpyDeviceToHost, st));
+        GF_CUDA(ctx, cudaStreamSynchronize(st));
+        const double *h = prob->scal_h;
+        total = (int)h[S_ITER];
+        rn = h[S_RES];
+        if (h[S_FLAG] != 0.0)
+          return gf_fail(ctx, GF_ERR_NONFINITE, "CG breakdown at iteration %d", total);
+        if (rn <= h[S_RTOL]) {
+          rc = GF_OK;
+          break;
+        }
+        if (total >= tr.maxit) break;
+      }
+    }
+    // epilogue: x_E = mask x_L + xb
+    prob->launches++;
+    k_scatter<MAP><<<gE, 256, 0, st>>>(nE, map, xL, maskE, bbv ? xbE : nullptr, xE);
+    GF_CHECK_LAUNCH(ctx);
+    *iters_out = total;
+    *rn_out = rn;
+    return rc;
+  }
+};
+
+template <int N>
+struct BoxSolve {
+  static int run(gf_problem *prob, const gf_cg_traits *tr, double p, double q, int use_mass,
+                 const double *b, const double *xb, double *x, int *it, double *rn, double *hist,
+                 bool masked) {
+    Solver<MapBox<N>> S(prob, MapBox<N>::make(prob->box), masked);
+    return S.solve(*tr, p, q, use_mass, b, xb, x, it, rn, hist);
   }
 };
 
@@ -449,115 +781,33 @@ extern "C" int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *tr, double p, 
   GF_REQUIRE(ctx, tr->maxit >= 0, "maxit must be >= 0");
   GF_REQUIRE(ctx, tr->normtype >= GF_NORM_INF && tr->normtype <= GF_NORM_L1, "bad norm type");
   GF_REQUIRE(ctx, tr->precision == GF_CG_FP64 || tr->precision == GF_CG_MIXED, "bad precision");
+  GF_REQUIRE(ctx, tr->precond == GF_PRECOND_NONE || tr->precond == GF_PRECOND_JACOBI,
+             "bad preconditioner");
   GF_CUDA(ctx, cudaSetDevice(ctx->device));
-  Solver S(prob);
-  const int64_t n = prob->nlocal;
-  const bool bbv = xb != nullptr;
-  double *dinv = nullptr;
-  if (tr->precond == GF_PRECOND_JACOBI) {
-    dinv = S.jacobi(p, q, use_mass);
-    if (!dinv) return gf_fail(ctx, GF_ERR_NOMEM, "Jacobi diagonal allocation failed");
-  }
   double *hist = nullptr;
   if (residuals && tr->maxit > 0) {
-    hist = (double *)gf_work(prob, 11, sizeof(double) * tr->maxit);
+    hist = (double *)gf_work(prob, 16, sizeof(double) * tr->maxit);
+    if (!hist) return gf_fail(ctx, GF_ERR_NOMEM, "history allocation failed");
     cudaMemsetAsync(hist, 0, sizeof(double) * tr->maxit, ctx->stream);
   }
-  int rc;
-  int it = 0;
+  int it = 0, rc;
   double rn = 0.0;
-  if (tr->precision == GF_CG_FP64) {
-    rc = S.solve<double>(*tr, p, q, use_mass, b, xb, x, bbv, tr->tol, tr->relative != 0, tr->maxit, dinv, hist,
-                         &it, &rn, 0);
+  const bool masked = xb != nullptr && prob->maskL8 != nullptr;
+  if (prob->has_box) {
+    rc = dispatch_n<BoxSolve>(prob->n, prob, tr, p, q, use_mass, b, xb, x, &it, &rn, hist, masked);
   } else {
-    // Mixed precision: FP64 residual r = b - A x (assembled, masked),
-    // FP32 PCG for the correction, FP64 update of x, repeated.
-    cudaStream_t st = ctx->stream;
-    double *r64 = (double *)gf_work(prob, 3, sizeof(double) * n);
-    double *ax = (double *)gf_work(prob, 4, sizeof(double) * n);
-    float *r32 = (float *)gf_work(prob, 5, sizeof(float) * n);
-    float *d32 = (float *)gf_work(prob, 6, sizeof(float) * n);
-    if (!r64 || !ax || !r32 || !d32) return gf_fail(ctx, GF_ERR_NOMEM, "work allocation failed");
-    const unsigned gel = grid_for(n, 256, ctx->sm_count * 8);
-    const double *mask = bbv ? prob->mask_d : nullptr;
-    if (bbv) {
-      prob->launches++;
-      k_cg_lift<double><<<gel, 256, 0, st>>>(n, mask, xb, x);
-    }
-    // b norm and rtol as the reference (gcg.ipp:290-293)
-    prob->scal_h[S_NORMT] = tr->normtype;
-    prob->scal_h[S_NTOT] = (double)n;
-    prob->scal_h[S_IVOL] = 1.0 / prob->volume;
-    GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_d + S_NTOT, prob->scal_h + S_NTOT, sizeof(double) * 3,
-                                 cudaMemcpyHostToDevice, st));
-    prob->launches++;
-    k_norm<<<S.gvec, RED_THREADS, 0, st>>>(n, tr->normtype, b, prob->mass_d, prob->scal_d, 40,
-                                           prob->partials, prob->counter);
-    GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h + 40, prob->scal_d + 40, sizeof(double),
-                                 cudaMemcpyDeviceToHost, st));
-    GF_CUDA(ctx, cudaStreamSynchronize(st));
-    const double bnorm = prob->scal_h[40];
-    const double rtol = (tr->relative || bnorm >= 1.0) ? tr->tol * bnorm : tr->tol;
-    const int sweeps = tr->max_refine > 0 ? tr->max_refine : 20;
-    const double itol = tr->inner_tol > 0 ? tr->inner_tol : 1e-5;
-    rc = GF_CG_NOCONVERGE;
-    int total = 0;
-    for (int sweep = 0; sweep <= sweeps; sweep++) {
-      // FP64 residual
-      int rr = launch_helm<double>(prob, p, nullptr, q, nullptr, use_mass, x, ax, st);
-      if (rr) return gf_fail(ctx, rr, "apply failed");
-      prob->launches++;
-      k_cg_resid<double><<<gel, 256, 0, st>>>(n, b, ax, r64);
-      prob->launches++;
-      k_cg_dss<double, false><<<S.gcls, RED_THREADS, 0, st>>>(
-          prob->nclass, prob->class_ptr, prob->members, mask, prob->imult_d, ax, r64,
-          prob->scal_d, prob->partials, prob->counter);
-      prob->launches++;
-      k_norm<<<S.gvec, RED_THREADS, 0, st>>>(n, tr->normtype, r64, prob->mass_d, prob->scal_d, 41,
-                                             prob->partials, prob->counter);
-      GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h + 41, prob->scal_d + 41, sizeof(double),
-                                   cudaMemcpyDeviceToHost, st));
-      GF_CUDA(ctx, cudaStreamSynchronize(st));
-      rn = prob->scal_h[41];
-      if (rn <= rtol) {
-        rc = GF_OK;
-        break;
-      }
-      if (sweep == sweeps || total >= tr->maxit) break;
-      // FP32 correction: A d = r, d0 = 0, to a relative drop itol
-      prob->launches++;
-      k_convert<float, double><<<gel, 256, 0, st>>>(n, r64, r32);
-      cudaMemsetAsync(d32, 0, sizeof(float) * n, st);
-      int in_it = 0;
-      double in_rn = 0.0;
-      // relative drop itol, but no deeper than needed to reach rtol
-      const double rel = std::max(itol, 0.5 * rtol / rn);
-      // the correction obeys the same Dirichlet mask (zero lift)
-      int irc = S.solve<float>(*tr, p, q, use_mass, r32, nullptr, d32, bbv, rel, true,
-                               tr->maxit - total, dinv, nullptr, &in_it, &in_rn, 13);
-      if (irc < 0) return irc;
-      total += in_it;
-      // x += d
-      prob->launches++;
-      k_convert<double, float><<<gel, 256, 0, st>>>(n, d32, ax);
-      prob->launches++;
-      k_axpby<double><<<gel, 256, 0, st>>>(n, 1.0, ax, 1.0, x);
-    }
-    if (bbv) {
-      prob->launches++;
-      k_cg_lift<double><<<gel, 256, 0, st>>>(n, prob->mask_d, xb, x);
-    }
-    GF_CHECK_LAUNCH(ctx);
-    it = total;
-    if (rc == GF_CG_NOCONVERGE && rn <= tr->tol) rc = GF_OK;
+    Solver<MapCsr> S(prob, MapCsr{prob->class_ptr, prob->members, prob->node_class, prob->nclass},
+                     masked);
+    rc = S.solve(*tr, p, q, use_mass, b, xb, x, &it, &rn, hist);
   }
+  if (rc < 0) return rc;
   if (iters) *iters = it;
   if (final_norm) *final_norm = rn;
-  if (residuals && hist && tr->maxit > 0) {
+  if (residuals && hist && it > 0 && tr->precision == GF_CG_FP64) {
     GF_CUDA(ctx, cudaMemcpyAsync(residuals, hist, sizeof(double) * std::min(it, tr->maxit),
                                  cudaMemcpyDeviceToHost, ctx->stream));
-    GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return rc;
 }
 

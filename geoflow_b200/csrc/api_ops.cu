@@ -15,13 +15,41 @@ using namespace gfk;
 template <typename T>
 int launch_helm(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
                 const T *u, T *uo, cudaStream_t st, const double *stop) {
-  return dispatch_n<HelmLaunch<T>::template F>(prob->n, prob, p, pvec, q, qvec, use_mass, u, uo, st,
-                                               stop);
+  return dispatch_n<HelmLaunch<T, LoadE<T>>::template F>(prob->n, prob, p, pvec, q, qvec, use_mass,
+                                                         LoadE<T>{u}, uo, st, stop);
 }
 template int launch_helm<double>(gf_problem *, double, const double *, double, const double *, int,
                                  const double *, double *, cudaStream_t, const double *);
 template int launch_helm<float>(gf_problem *, float, const float *, float, const float *, int,
                                 const float *, float *, cudaStream_t, const double *);
+
+template <typename T>
+int launch_helm_L(gf_problem *prob, T p, T q, int use_mass, const T *wL, T *uo, cudaStream_t st,
+                  const double *stop) {
+  if (prob->has_box)
+    return dispatch_n<HelmLaunch<T, LoadBox<T>>::template F>(
+        prob->n, prob, p, (const T *)nullptr, q, (const T *)nullptr, use_mass,
+        LoadBox<T>{wL, prob->box}, uo, st, stop);
+  return dispatch_n<HelmLaunch<T, LoadCsr<T>>::template F>(
+      prob->n, prob, p, (const T *)nullptr, q, (const T *)nullptr, use_mass,
+      LoadCsr<T>{wL, prob->node_class}, uo, st, stop);
+}
+template int launch_helm_L<double>(gf_problem *, double, double, int, const double *, double *,
+                                   cudaStream_t, const double *);
+
+int launch_helm_L_f32io(gf_problem *prob, double p, double q, int use_mass, const float *wL,
+                        float *uo, cudaStream_t st, const double *stop) {
+  if (prob->dim != 3) return GF_ERR_UNSUPPORTED;
+  if (prob->has_box)
+    return dispatch_n<HelmLaunch<double, LoadBox<float>, float>::template F>(
+        prob->n, prob, p, (const double *)nullptr, q, (const double *)nullptr, use_mass,
+        LoadBox<float>{wL, prob->box}, uo, st, stop);
+  return dispatch_n<HelmLaunch<double, LoadCsr<float>, float>::template F>(
+      prob->n, prob, p, (const double *)nullptr, q, (const double *)nullptr, use_mass,
+      LoadCsr<float>{wL, prob->node_class}, uo, st, stop);
+}
+template int launch_helm_L<float>(gf_problem *, float, float, int, const float *, float *,
+                                  cudaStream_t, const double *);
 
 extern "C" int gf_helmholtz_apply(gf_problem_t prob, int dtype, double p, const void *p_vec,
                                   double q, const void *q_vec, int use_mass, const void *u,

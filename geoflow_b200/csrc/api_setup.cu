@@ -407,7 +407,8 @@ extern "C" int gf_problem_destroy(gf_problem_t prob) {
   void *ptrs[] = {prob->egeom_d, prob->egeom_f, prob->ngeom_d, prob->ngeom_f, prob->mask_d,
                   prob->mask_f, prob->imass_d, prob->imass_f, prob->mass_d, prob->imult_d,
                   prob->imult_f, prob->class_ptr, prob->members, prob->node_class, prob->sh_ptr,
-                  prob->sh_members, prob->scal_d, prob->partials, prob->counter};
+                  prob->sh_members, prob->scal_d, prob->partials, prob->counter,
+                  prob->massL, prob->maskL8, prob->multL8};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (prob->scal_h) cudaFreeHost(prob->scal_h);
@@ -521,6 +522,60 @@ extern "C" int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *d, gf_prob
     shp[nshared] = (int32_t)pos;
   }
   p->nshared = nshared;
+  // Unique-node indexing.  For a regular box the unique nodes are the
+  // lattice points; the CSR must then be exactly the lattice classes.
+  std::vector<int64_t> lofc(d->nclass);  // unique-node index of each class
+  for (int64_t c = 0; c < d->nclass; c++) lofc[c] = c;
+  if (d->box_ne[0] > 0) {
+    gfk::BoxLattice L{};
+    L.dim = dim;
+    L.p = n - 1;
+    int64_t nel = 1;
+    for (int k = 0; k < 3; k++) {
+      L.ne[k] = k < dim ? d->box_ne[k] : 1;
+      L.per[k] = k < dim ? (d->box_periodic[k] != 0) : 0;
+      L.M[k] = k < dim ? (int64_t)L.ne[k] * L.p + (L.per[k] ? 0 : 1) : 1;
+      if (k < dim) nel *= L.ne[k];
+    }
+    if (nel != d->ne || L.size() != d->nclass) {
+      gf_problem_destroy(p);
+      return gf_fail(ctx, GF_ERR_ARG, "box description does not match the element or class count");
+    }
+    // every class must be one lattice point
+    for (int64_t c = 0; c < d->nclass; c++) {
+      int64_t key = -1;
+      for (int32_t k = d->class_ptr[c]; k < d->class_ptr[c + 1]; k++) {
+        const int64_t i = d->members[k], e = i / nn;
+        const int a = (int)(i % nn);
+        int ec[3];
+        L.elem_coords(e, ec);
+        int64_t g = L.g1(0, ec[0], a % n) + L.M[0] * L.g1(1, ec[1], (a / n) % n);
+        if (dim > 2) g += L.M[0] * L.M[1] * L.g1(2, ec[2], a / (n * n));
+        if (key >= 0 && g != key) {
+          gf_problem_destroy(p);
+          return gf_fail(ctx, GF_ERR_ARG, "gather-scatter classes are not the box lattice classes");
+        }
+        key = g;
+      }
+      lofc[c] = key;
+    }
+    p->box = L;
+    p->has_box = true;
+  }
+  {
+    std::vector<double> massL(d->nclass, 0.0);
+    std::vector<uint8_t> maskL(d->nclass, 1), multL(d->nclass, 1);
+    for (int64_t c = 0; c < d->nclass; c++) {
+      double s = 0.0;
+      for (int32_t k = d->class_ptr[c]; k < d->class_ptr[c + 1]; k++) s += mass[d->members[k]];
+      massL[lofc[c]] = s;
+      multL[lofc[c]] = (uint8_t)std::min<int32_t>(255, d->class_ptr[c + 1] - d->class_ptr[c]);
+      if (d->mask) maskL[lofc[c]] = d->mask[d->members[d->class_ptr[c]]] != 0.0;
+    }
+    p->massL = upload(massL);
+    p->multL8 = upload(multL);
+    if (d->mask) p->maskL8 = upload(maskL);
+  }
   p->mass_d = upload(mass);
   p->imass_d = upload(imass);
   p->imass_f = upload(to_f32(imass));
@@ -536,7 +591,7 @@ extern "C" int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *d, gf_prob
   p->node_class = upload(ncls);
   p->sh_ptr = upload(shp);
   if (nshm) p->sh_members = upload(shm);
-  p->npartials = 1024;
+  p->npartials = 2048;
   cudaMalloc(&p->partials, sizeof(double) * 4 * p->npartials);
   cudaMalloc(&p->counter, sizeof(unsigned int) * 8);
   cudaMemsetAsync(p->counter, 0, sizeof(unsigned int) * 8, ctx->stream);

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/gfgpu.h"
+#include "lattice.cuh"
 
 #define GF_MAXN 12  // largest GLL point count compiled (p = 11)
 
@@ -57,6 +58,13 @@ struct gf_problem {
   int32_t *class_ptr = nullptr;  // nclass+1
   int32_t *members = nullptr;    // nlocal
   int32_t *node_class = nullptr; // nlocal
+  // regular box lattice (GGridBox): unique nodes indexed by lattice point
+  bool has_box = false;
+  gfk::BoxLattice box{};
+  // unique-node (L) vectors, indexed by lattice point (box) or class (CSR)
+  double *massL = nullptr;      // assembled mass (L2/L1 norms)
+  uint8_t *multL8 = nullptr;    // multiplicity per unique node (EUC norm)
+  uint8_t *maskL8 = nullptr;    // Dirichlet mask per unique node: 1 keep, 0 masked
   // classes with more than one member (shared nodes) and the singletons
   int64_t nshared = 0;
   int32_t *sh_ptr = nullptr;

@@ -14,6 +14,7 @@
 // sum_k D_k^T gdu_k, times a scalar p, plus q M u.
 #pragma once
 #include "gf_common.cuh"
+#include "k_maps.cuh"
 
 namespace gfk {
 
@@ -79,11 +80,16 @@ __device__ __forceinline__ void node_geom(const Geom<T> &g, int64_t node, NodeGe
 // ---------------------------------------------------------------------
 // 3-d Helmholtz apply: uo = p * sum_k Dk^T M Gk Dk u + q M u
 // ---------------------------------------------------------------------
-template <typename T, int N, int EPB>
+// LD is the input loader (k_maps.cuh): the element-local vector itself, or
+// a unique-node vector gathered through the box lattice or node_class.
+// T is the arithmetic type; the input is stored as LD::value_type and the
+// output as TO (FP32 storage with FP64 arithmetic keeps the apply's
+// rounding at the storage level, which the mixed-precision CG relies on).
+template <typename T, int N, int EPB, class LD, typename TO = T>
 __global__ void __launch_bounds__(N *N *EPB)
     k_helm3d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T p,
              const T *__restrict__ pvec, T q, const T *__restrict__ qvec, int use_mass,
-             const T *__restrict__ u, T *__restrict__ uo, const double *__restrict__ stop) {
+             const LD ld, TO *__restrict__ uo, const double *__restrict__ stop) {
   if (stop && stop[0] != 0.0) return;
   constexpr int P = Pad<N>::P, PLANE = N * P, VOL = N * PLANE, NN = N * N, NNN = N * N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -101,11 +107,17 @@ __global__ void __launch_bounds__(N *N *EPB)
 
   // stage 0: load z-line (i=a0, j=a1) into registers and shared memory
   T ru[N];
+  if (active) {
+    typename LD::value_type lv[N];
+    ld.template zline<N>(e, a0, a1, lv);
 #pragma unroll
-  for (int k = 0; k < N; k++) {
-    ru[k] = active ? u[base + k * NN + t] : T(0);
-    su[k * PLANE + a1 * P + a0] = ru[k];
+    for (int k = 0; k < N; k++) ru[k] = (T)lv[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k++) ru[k] = T(0);
   }
+#pragma unroll
+  for (int k = 0; k < N; k++) su[k * PLANE + a1 * P + a0] = ru[k];
   __syncthreads();
 
   // stage 1: x-line (j=a0, k=a1)
@@ -201,7 +213,7 @@ __global__ void __launch_bounds__(N *N *EPB)
           mu *= qvec ? qvec[node] : q;
           o += mu;
         }
-        uo[node] = o;
+        uo[node] = (TO)o;
       }
     }
   }
@@ -210,11 +222,11 @@ __global__ void __launch_bounds__(N *N *EPB)
 // ---------------------------------------------------------------------
 // 2-d Helmholtz apply (one thread per node)
 // ---------------------------------------------------------------------
-template <typename T, int N, int EPB>
+template <typename T, int N, int EPB, class LD>
 __global__ void __launch_bounds__(N *N *EPB)
     k_helm2d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T p,
              const T *__restrict__ pvec, T q, const T *__restrict__ qvec, int use_mass,
-             const T *__restrict__ u, T *__restrict__ uo, const double *__restrict__ stop) {
+             const LD ld, T *__restrict__ uo, const double *__restrict__ stop) {
   if (stop && stop[0] != 0.0) return;
   constexpr int P = Pad<N>::P, AREA = N * P, NN = N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -231,7 +243,7 @@ __global__ void __launch_bounds__(N *N *EPB)
   if (active) {
     elem_geom<T, 2>(g, e, ng);
     node_geom<T, 2>(g, node, ng);
-    uv = u[node];
+    uv = ld.template point2<N>(e, i, j);
     if (pvec) pv = pvec[node];
   }
   su[j * P + i] = uv;

@@ -1,6 +1,7 @@
 // ops_launch.cuh -- host launchers for the per-order kernel templates,
 // selected at run time by dispatch_n over the GLL point count.
 #pragma once
+#include <type_traits>
 #include <unordered_map>
 
 #include "gf_common.cuh"
@@ -21,31 +22,35 @@ inline void set_smem(K kern, size_t bytes) {
   }
 }
 
-template <typename T>
+template <typename T, class LD, typename TO = T>
 struct HelmLaunch {
   template <int N>
   struct F {
     static int run(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
-                   const T *u, T *uo, cudaStream_t st, const double *stop) {
+                   LD ld, TO *uo, cudaStream_t st, const double *stop) {
       const Basis<T, N> B = make_basis<T, N>(prob);
       const Geom<T> g = geom_of<T>(prob);
       constexpr int P = Pad<N>::P;
       if (prob->dim == 3) {
         constexpr int EPB = epb3<N>();
         const size_t smem = sizeof(T) * 3 * N * N * P * EPB;
-        auto kern = k_helm3d<T, N, EPB>;
+        auto kern = k_helm3d<T, N, EPB, LD, TO>;
         set_smem(kern, smem);
         const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
         prob->launches++;
-        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, p, pvec, q, qvec, use_mass, u, uo, stop);
+        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, p, pvec, q, qvec, use_mass, ld,
+                                                    uo, stop);
+      } else if constexpr (!std::is_same<T, TO>::value) {
+        return GF_ERR_UNSUPPORTED;  // mixed storage/arithmetic is 3-d only
       } else {
         constexpr int EPB = epb2<N>();
         const size_t smem = sizeof(T) * 3 * N * P * EPB;
-        auto kern = k_helm2d<T, N, EPB>;
+        auto kern = k_helm2d<T, N, EPB, LD>;
         set_smem(kern, smem);
         const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
         prob->launches++;
-        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, p, pvec, q, qvec, use_mass, u, uo, stop);
+        kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, p, pvec, q, qvec, use_mass, ld,
+                                                    uo, stop);
       }
       return GF_OK;
     }
@@ -136,6 +141,14 @@ struct DudtLaunch {
 template <typename T>
 int launch_helm(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
                 const T *u, T *uo, cudaStream_t st, const double *stop = nullptr);
+// same operator on a unique-node input wL (gathered per element), writing
+// the element-local result uo
+template <typename T>
+int launch_helm_L(gf_problem *prob, T p, T q, int use_mass, const T *wL, T *uo, cudaStream_t st,
+                  const double *stop = nullptr);
+// FP32-stored input and output, FP64 arithmetic (3-d)
+int launch_helm_L_f32io(gf_problem *prob, double p, double q, int use_mass, const float *wL,
+                        float *uo, cudaStream_t st, const double *stop);
 template <typename T>
 int launch_dss(gf_problem *prob, int op, T *u, cudaStream_t st);
 template <typename T>

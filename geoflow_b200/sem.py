@@ -131,7 +131,8 @@ class GridBox:
 class Problem:
     """Device-resident grid, operators and gather-scatter map (gf_problem)."""
 
-    def __init__(self, ctx: Context, grid: GridBox, dirichlet_mask: bool = True):
+    def __init__(self, ctx: Context, grid: GridBox, dirichlet_mask: bool = True,
+                 structured: bool = True):
         self.ctx, self.grid = ctx, grid
         self.dim, self.n, self.nlocal = grid.dim, grid.n, grid.ndof()
         d = A.ProblemDesc()
@@ -144,6 +145,10 @@ class Problem:
         d.mask = A.ptr(grid.mask) if dirichlet_mask else None
         d.nclass = grid.nclass
         d.class_ptr, d.members = A.ptr(grid.class_ptr), A.ptr(grid.members)
+        if structured:  # unique nodes indexed by lattice point (no index arrays)
+            for k in range(grid.dim):
+                d.box_ne[k] = grid.ne[k]
+                d.box_periodic[k] = grid.periodic[k]
         h = C.c_void_p()
         ctx.check(_lib().gf_problem_create(ctx.handle, C.byref(d), C.byref(h)), "gf_problem_create")
         self.handle = h
@@ -255,11 +260,12 @@ class CGTraits:
     max_refine: int = 40
     check_every: int = 16
     relative: int = 0
+    mixed_apply: int = 0
 
     def to_c(self) -> A.CGTraits:
         t = A.CGTraits()
         for f in ("maxit", "normtype", "tol", "precond", "precision", "inner_tol", "max_refine",
-                  "check_every", "relative"):
+                  "check_every", "relative", "mixed_apply"):
             setattr(t, f, getattr(self, f))
         return t
 

@@ -121,6 +121,13 @@ typedef struct {
   int64_t nclass;
   const int32_t *class_ptr; /* host nclass+1 */
   const int32_t *members;   /* host N_local, ascending inside each class */
+  /* optional: the grid is a regular box of box_ne[d] elements per direction
+   * in lexicographic order (GGridBox), periodic where box_periodic[d] != 0.
+   * When box_ne[0] > 0 the library checks that the CSR equals the lattice
+   * classes and then indexes unique nodes by lattice point, reading no
+   * index arrays in the solver. */
+  int box_ne[3];
+  int box_periodic[3];
 } gf_problem_desc;
 
 int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *desc, gf_problem_t *out);
@@ -184,6 +191,8 @@ typedef struct {
   int max_refine;   /* MIXED: maximum refinement sweeps */
   int check_every;  /* iterations between host convergence checks (>=1) */
   int relative;     /* 1: stop at norm(r) <= tol*norm(b) even when norm(b) < 1 */
+  int mixed_apply;  /* MIXED, 3-d: 0 FP32 arithmetic in the FP32 solve's applies,
+                       1 FP64 arithmetic on the FP32-stored vectors */
 } gf_cg_traits;
 
 /* Solves (p L + q M) x = b on the assembled space (DSS Sum + mask), as

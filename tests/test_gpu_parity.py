@@ -39,10 +39,10 @@ def relerr(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-def setup(ctx, dim, ne, p, periodic=None, mask=True):
+def setup(ctx, dim, ne, p, periodic=None, mask=True, structured=True):
     g = GridBox(dim, ne, p, periodic=periodic)
     o = O.OracleBox(dim, ne, p, periodic=periodic)
-    return g, Problem(ctx, g, dirichlet_mask=mask), o
+    return g, Problem(ctx, g, dirichlet_mask=mask, structured=structured), o
 
 
 CASES3 = [([2, 2, 2], 2, None), ([3, 2, 2], 4, [1, 0, 1]), ([2, 2, 3], 6, None),
@@ -176,9 +176,10 @@ def test_integrate(ctx):
     assert abs(r.value - o.integrate(u)) < 1e-12 * max(1.0, abs(o.integrate(np.abs(u))))
 
 
-def test_cdg_cg_poisson_on_gpu(ctx):
+@pytest.mark.parametrize("structured", [True, False])
+def test_cdg_cg_poisson_on_gpu(ctx, structured):
     """cdg_cg.cpp known answer through the device CG (2D, 4x4, p=6)."""
-    g, prob, o = setup(ctx, 2, [4, 4], 6)
+    g, prob, o = setup(ctx, 2, [4, 4], 6, structured=structured)
     x, y = g.xyz
     f = 6.0 * x * y * (1.0 - y) - 2.0 * x ** 3
     ua = y * (1.0 - y) * x ** 3
@@ -208,9 +209,10 @@ def test_cdg_cg_poisson_on_gpu(ctx):
     assert relerr(host(u), xo) < 1e-10
 
 
+@pytest.mark.parametrize("structured", [True, False])
 @pytest.mark.parametrize("precond", [0, 1])
-def test_cg_helmholtz_3d_matches_oracle(ctx, precond):
-    g, prob, o = setup(ctx, 3, [3, 3, 3], 5)
+def test_cg_helmholtz_3d_matches_oracle(ctx, precond, structured):
+    g, prob, o = setup(ctx, 3, [3, 3, 3], 5, structured=structured)
     rng = np.random.default_rng(4)
     f = rng.standard_normal(g.ndof())
     f = f[g.members[g.class_ptr[:-1]]][g.node_class]
@@ -229,8 +231,9 @@ def test_cg_helmholtz_3d_matches_oracle(ctx, precond):
     assert relerr(host(x), xo) < 1e-10
 
 
-def test_cg_mixed_precision_reaches_fp64_solution(ctx):
-    g, prob, o = setup(ctx, 3, [3, 3, 3], 6)
+@pytest.mark.parametrize("structured", [True, False])
+def test_cg_mixed_precision_reaches_fp64_solution(ctx, structured):
+    g, prob, o = setup(ctx, 3, [3, 3, 3], 6, structured=structured)
     rng = np.random.default_rng(8)
     f = rng.standard_normal(g.ndof())
     f = f[g.members[g.class_ptr[:-1]]][g.node_class]
@@ -238,12 +241,17 @@ def test_cg_mixed_precision_reaches_fp64_solution(ctx):
     H = GHelmholtz(prob)
     H.set_mass_scalar(1.0)
     x64 = prob.zeros()
-    GCG(CGTraits(maxit=5000, tol=1e-12, precond=1), prob).solve(H, dev(b), dev(0 * b), x64)
+    common = dict(maxit=5000, tol=1e-12, precond=1, normtype=A.GF_NORM_EUC, relative=1)
+    cg64 = GCG(CGTraits(**common), prob)
+    assert cg64.solve(H, dev(b), dev(0 * b), x64) == 0
     xm = prob.zeros()
-    cgm = GCG(CGTraits(maxit=5000, tol=1e-12, precond=1, precision=A.GF_CG_MIXED), prob)
+    cgm = GCG(CGTraits(precision=A.GF_CG_MIXED, check_every=16, **common), prob)
     rc = cgm.solve(H, dev(b), dev(0 * b), xm)
     assert rc == 0
+    # both meet a 1e-12 relative residual; the solutions agree to ~kappa * 1e-12
     assert relerr(host(xm), host(x64)) < 1e-9
+    # the FP32 Krylov run is never restarted: about the FP64 iteration count
+    assert cgm.get_iteration_count() <= 1.5 * cg64.get_iteration_count() + 32
 
 
 def test_rk4_advection_2d_matches_oracle(ctx):
@@ -277,3 +285,35 @@ def test_rk_schemes_burgers_3d_match_oracle(ctx, scheme):
     o.rk_advance(1, 1e-2, scheme, uo, dt=2e-3, nsteps=5)
     for k in range(3):
         assert relerr(host(ut[k]), uo[k]) < 1e-10
+
+
+@pytest.mark.parametrize("structured", [True, False])
+@pytest.mark.parametrize("normtype", [A.GF_NORM_EUC, A.GF_NORM_L2, A.GF_NORM_L1])
+def test_cg_norm_types_periodic_unmasked(ctx, structured, normtype):
+    """solve_impl (1) (no boundary lift, no mask) with every norm type on a
+    periodic box: same iteration count and solution as the oracle."""
+    g, prob, o = setup(ctx, 3, [2, 3, 2], 4, [1, 1, 1], mask=False, structured=structured)
+    rng = np.random.default_rng(12)
+    f = rng.standard_normal(g.ndof())
+    f = f[g.members[g.class_ptr[:-1]]][g.node_class]
+    b = o.mass * f
+    q = np.ones(g.ndof())
+    xo = np.zeros(g.ndof())
+    rc_o, it_o, _ = o.cg_solve(b, xo, p=1.0, q_vec=q, maxit=500, normtype=normtype, tol=1e-12,
+                               use_mask=False)
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    cg = GCG(CGTraits(maxit=500, tol=1e-12, normtype=normtype, check_every=3), prob)
+    x = prob.zeros()
+    rc = cg.solve(H, dev(b), x)
+    assert rc == rc_o == 0
+    assert abs(cg.get_iteration_count() - it_o) <= 1
+    assert relerr(host(x), xo) < 1e-9
+
+
+def test_box_description_must_match_classes(ctx):
+    """A box description whose lattice disagrees with the CSR is refused."""
+    g = GridBox(3, [2, 2, 2], 3)
+    g.ne = [4, 2, 1]  # same element count, different lattice
+    with pytest.raises(A.GFError):
+        Problem(ctx, g)
