@@ -29,6 +29,9 @@ GF_CG_FP64, GF_CG_MIXED = 0, 1
 GF_GEOM_AFFINE, GF_GEOM_REGULAR = 0, 1
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
 GF_RK1, GF_RK2, GF_RK3, GF_RK4, GF_SSP22, GF_SSP33, GF_SSP34 = 1, 2, 3, 4, 22, 33, 34
+# gf_integrate_noalloc: fixed scratch of GF_NOALLOC_MAX_BLOCKS blocks of GF_NOALLOC_CHUNK
+GF_NOALLOC_CHUNK, GF_NOALLOC_MAX_BLOCKS = 4096, 32768
+GF_NOALLOC_MAX_N = GF_NOALLOC_CHUNK * GF_NOALLOC_MAX_BLOCKS
 
 
 class ProblemDesc(C.Structure):
@@ -91,6 +94,7 @@ SIGNATURES = {
                               c_double, c_int]),
     "gf_rk_advance_host": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
                                    c_double, c_int]),
+    "gf_integrate_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gf_dudt_vjp": (c_int, [c_void_p, c_int, c_int, c_double, c_int, P_void, P_void, P_void,
                             P_void]),
     "gf_dss_T": (c_int, [c_void_p, c_int, c_int, c_void_p]),

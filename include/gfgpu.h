@@ -225,6 +225,24 @@ int gf_rk_advance(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
 int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
                        void *const *u, const void *const *c, double t0, double dt, int nsteps);
 
+/* ---- allocation-free integral (no counterpart in the reference) ----
+ * sum_i mass[i]*u[i] over n nodes into *result, all three device pointers;
+ * with mass = the local mass W (x) W (x) W Jac this is GGrid::integrate.
+ * For callers that cannot call cudaMalloc where they integrate (a host
+ * framework owning device memory through its own pool, a loop that must
+ * not stall on an allocation, a deployment that forbids allocation after
+ * start-up): nothing is allocated, the scratch is a fixed 256 KB array in
+ * the library (held by every GPU that loads it until exit), so n may be at
+ * most GF_NOALLOC_MAX_BLOCKS * GF_NOALLOC_CHUNK (134,217,728); larger n is
+ * rejected with GF_ERR_ARG.  The first call on a device looks up the
+ * array's device address; make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race, so order them on one
+ * stream.  `stream` is a cudaStream_t (NULL: legacy default stream). */
+#define GF_NOALLOC_CHUNK 4096
+#define GF_NOALLOC_MAX_BLOCKS 32768
+int gf_integrate_noalloc(int64_t n, const double *mass, const double *u, double *result,
+                         void *stream);
+
 /* ---- adjoint (no reference counterpart) ---- */
 /* Vector-Jacobian product of gf_dudt: given u (and c) and a cotangent
  * lam[nstate] on dudt, returns ubar[nstate] = (d dudt/du)^T lam. */
