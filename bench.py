@@ -43,7 +43,7 @@ L2_BYTES = 126 * 2 ** 20
 # iterations the reference's FP64 Jacobi-PCG (the algorithm of GCG::solve_impl,
 # preconditioned) needs on the headline problem, as measured by the device
 # FP64 path of the same algorithm; used to project the CPU time to solution
-REF_ITERS_32_P7 = None
+REF_ITERS_32_P7 = 220
 
 
 def parse():
@@ -312,6 +312,60 @@ def rk_stage_bench(ctx, ne, p, steps=3, warmup=2):
 
 
 # ---------------------------------------------------------------------------
+def adjoint_bench(ctx, ne=16, p=6, nsteps=50, ck=10, reps=3):
+    """Adjoint workload: gradient of J = 1/2 ||u(T) - u_obs||_M^2 with
+    respect to u(0) through 50 RK4 steps of 3d Burgers (16^3 elements,
+    p = 6, FP64), checkpoint every 10 steps, against the forward run alone."""
+    import torch
+    from geoflow_b200 import GBurgers, GridBox, Problem
+    from geoflow_b200 import _abi as A
+    g = GridBox(3, [ne] * 3, p, periodic=[1, 1, 1])
+    prob = Problem(ctx, g, dirichlet_mask=False)
+    dev = ctx.torch_device
+    rng = np.random.default_rng(SEED + 4)
+    first = g.members[g.class_ptr[:-1]][g.node_class]
+
+    def fourier(amp):
+        u = np.zeros(g.ndof())
+        for _ in range(8):
+            k = rng.integers(-4, 5, 3)
+            u += rng.standard_normal() * np.cos(2 * np.pi * (k[0] * g.xyz[0] + k[1] * g.xyz[1]
+                                                             + k[2] * g.xyz[2])
+                                                + rng.uniform(0, 2 * np.pi))
+        u = u[first]
+        return torch.from_numpy(amp * u / np.abs(u).max()).to(dev)
+
+    dt, nu = 1e-3, 1e-3
+    B = GBurgers(prob, GBurgers.BURGERS, nu, scheme=A.GF_RK4)
+    u0 = [fourier(0.5) for _ in range(3)]
+    obs = [a + fourier(0.1) for a in u0]
+    B.step(obs, None, dt=dt, nsteps=nsteps)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()  # warm-up (allocates the work buffers once)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e) / 1e3)
+        return statistics.median(ts)
+
+    u = [a.clone() for a in u0]
+    launches0 = C_stats(prob)
+    t_fwd = timed(lambda: B.step(u, None, dt=dt, nsteps=nsteps))
+    t_adj = timed(lambda: B.adjoint_gradient(u0, None, obs, dt, nsteps, ck))
+    prob.close()
+    return {"workload": (f"3d Burgers, periodic {ne}^3 elements p={p}, RK4, {nsteps} steps, "
+                         f"nu={nu:g}, dt={dt:g}, FP64, checkpoint every {ck}"),
+            "n_local": prob.nlocal, "forward_s": t_fwd, "gradient_s": t_adj,
+            "gradient_over_forward": t_adj / t_fwd}
+
+
+# ---------------------------------------------------------------------------
 def cpu_oracle_iteration_time(sample_ne, p, iters=6):
     """Seconds per FP64 Jacobi-PCG iteration of the CPU oracle (a plain-C
     restatement of GCG::solve_impl + GHelmholtz::reg_prod + GGFX::doOp) on a
@@ -439,9 +493,10 @@ def main():
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    rk = None
+    rk = adj = None
     if not args.no_rk:
         rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p)
+        adj = adjoint_bench(ctx)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         t_node, nsample, wall = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, args.cpu_iters)
@@ -473,6 +528,7 @@ def main():
                      "traffic": None},
         "kernels": {"helm3d": roof, "dss_sum": dss},
         "rk_stage": rk,
+        "adjoint": adj,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": per_step_launches * args.steps,

@@ -141,7 +141,7 @@ bool Stepper<T>::alloc() {
 
 // One step uin -> uout (uout may not alias uin).
 template <typename T>
-int Stepper<T>::step(T *const *uin, T *const *uout, T dt) {
+int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
   const unsigned g = grid_for(n, 256, prob->ctx->sm_count * 8);
   int rc;
   if (scheme >= 1 && scheme <= 4) {
@@ -149,33 +149,37 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt) {
     butcher(scheme, alpha, beta, cc);
     const int ns = scheme;
     const T h = dt;
+    // stage inputs go to the tape when one is given
+    auto stage_in = [&](int m) { return tape ? tape + 3 * m : (T *const *)utmp; };
     for (int k = 0; k < nstate; k++)
       cudaMemcpyAsync(uout[k], uin[k], sizeof(T) * n, cudaMemcpyDeviceToDevice, st);
     for (int m = 0; m < ns - 1; m++) {
+      T *const *um = stage_in(m);
       for (int k = 0; k < nstate; k++) {
         prob->launches++;
         k_stage_sum<T><<<g, 256, 0, st>>>(n, uin[k], m, K[0][k], K[1][k], K[2][k],
                                           (T)beta[m][0] * h, (T)beta[m][1] * h,
-                                          (T)beta[m][2] * h, utmp[k]);
+                                          (T)beta[m][2] * h, um[k]);
       }
-      if ((rc = rhs(utmp, K[m]))) return rc;
+      if ((rc = rhs(um, K[m]))) return rc;
       for (int k = 0; k < nstate; k++) {
         smooth(K[m][k]);
         prob->launches++;
         k_accum<T><<<g, 256, 0, st>>>(n, K[m][k], (T)cc[m] * h, uout[k]);
       }
     }
+    T *const *uf = stage_in(ns - 1);
     for (int k = 0; k < nstate; k++) {
       prob->launches++;
       k_stage_sum<T><<<g, 256, 0, st>>>(n, uin[k], ns - 1, K[0][k], K[1][k], K[2][k],
                                         (T)beta[ns - 1][0] * h, (T)beta[ns - 1][1] * h,
-                                        (T)beta[ns - 1][2] * h, utmp[k]);
-      smooth(utmp[k]);
+                                        (T)beta[ns - 1][2] * h, uf[k]);
+      smooth(uf[k]);
     }
     // the final stage result goes to the last K slot (K[0] in the
     // reference, whose earlier content is no longer needed)
     T *const *Kf = K[0];
-    if ((rc = rhs(utmp, Kf))) return rc;
+    if ((rc = rhs(uf, Kf))) return rc;
     for (int k = 0; k < nstate; k++) smooth(Kf[k]);
     for (int k = 0; k < nstate; k++) {
       prob->launches++;
@@ -184,6 +188,23 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt) {
     }
     return GF_OK;
   }
+  // SSP stage inputs are uin and the substep results left in K[0..ns-2]
+  if (tape) {
+    if ((rc = step_ssp(uin, uout, dt))) return rc;
+    for (int k = 0; k < nstate; k++) {
+      cudaMemcpyAsync(tape[k], uin[k], sizeof(T) * n, cudaMemcpyDeviceToDevice, st);
+      for (int m = 1; m < stages(); m++)
+        cudaMemcpyAsync(tape[3 * m + k], K[m - 1][k], sizeof(T) * n, cudaMemcpyDeviceToDevice, st);
+    }
+    return GF_OK;
+  }
+  return step_ssp(uin, uout, dt);
+}
+
+template <typename T>
+int Stepper<T>::step_ssp(T *const *uin, T *const *uout, T dt) {
+  const unsigned g = grid_for(n, 256, prob->ctx->sm_count * 8);
+  int rc;
   const T one = T(1);
   if (scheme == GF_SSP22) {
     if ((rc = rhs(uin, K[0]))) return rc;

@@ -30,7 +30,12 @@ struct Stepper {
   bool alloc();
   int rhs(T *const *u, T *const *Kout);
   void smooth(T *v);
-  int step(T *const *uin, T *const *uout, T dt);
+  // One step uin -> uout.  With a tape (pointers tape[3*m + k], m = 0 ..
+  // stages-1), stage m's input state (the argument of its RHS call) is left
+  // in tape[3*m + k] for the adjoint sweep.
+  int step(T *const *uin, T *const *uout, T dt, T *const *tape = nullptr);
+  int step_ssp(T *const *uin, T *const *uout, T dt);
+  int stages() const { return scheme <= 4 ? scheme : (scheme == GF_SSP22 ? 2 : (scheme == GF_SSP33 ? 3 : 4)); }
 };
 
 }  // namespace gfrk

@@ -132,16 +132,31 @@ class Problem:
     """Device-resident grid, operators and gather-scatter map (gf_problem)."""
 
     def __init__(self, ctx: Context, grid: GridBox, dirichlet_mask: bool = True,
-                 structured: bool = True):
+                 structured: bool = True, geometry: str = "affine"):
+        """geometry: "affine" passes one (dXi/dX, Jac) set per element;
+        "regular" passes the same factors per node (the GGrid per-node
+        planes dXidX, Jac of a deformed grid)."""
         self.ctx, self.grid = ctx, grid
         self.dim, self.n, self.nlocal = grid.dim, grid.n, grid.ndof()
         d = A.ProblemDesc()
         d.dim, d.ne, d.n = grid.dim, grid.nelems, grid.n
         self._keep = [grid.D, grid.W, grid.elem_geom, grid.mask, grid.class_ptr, grid.members]
         d.D, d.W = A.ptr(grid.D), A.ptr(grid.W)
-        d.geom = A.GF_GEOM_AFFINE
-        d.elem_geom = A.ptr(grid.elem_geom)
-        d.node_geom = None
+        if geometry == "affine":
+            d.geom = A.GF_GEOM_AFFINE
+            d.elem_geom = A.ptr(grid.elem_geom)
+            d.node_geom = None
+        elif geometry == "regular":
+            npe = grid.n ** grid.dim
+            eg = grid.elem_geom.reshape(grid.nelems, grid.dim + 1)
+            ng = np.ascontiguousarray(np.concatenate(
+                [np.repeat(eg[:, k], npe) for k in range(grid.dim + 1)]))
+            self._keep.append(ng)
+            d.geom = A.GF_GEOM_REGULAR
+            d.elem_geom = None
+            d.node_geom = A.ptr(ng)
+        else:
+            raise ValueError(f"unknown geometry {geometry!r}")
         d.mask = A.ptr(grid.mask) if dirichlet_mask else None
         d.nclass = grid.nclass
         d.class_ptr, d.members = A.ptr(grid.class_ptr), A.ptr(grid.members)
@@ -331,3 +346,33 @@ class GBurgers:
         self.prob.ctx.check(_lib().gf_rk_advance(self.prob.handle, _dtype_code(u[0]), C.byref(tr),
                                                  A.ptr_array(u), A.ptr_array(c or []), t0, dt,
                                                  nsteps), "GBurgers::step")
+
+    # ---- adjoint (no reference counterpart; FP64 only) ----
+    def dudt_vjp(self, u, c, lam, ubar):
+        """ubar = (d dudt/du)^T lam at state u (velocity c for advection)."""
+        self.prob.ctx.check(_lib().gf_dudt_vjp(self.prob.handle, _dtype_code(lam[0]), self.eqn,
+                                               self.nu, len(lam), A.ptr_array(u or []),
+                                               A.ptr_array(c or []), A.ptr_array(lam),
+                                               A.ptr_array(ubar)), "GBurgers::dudt_vjp")
+
+    def step_vjp(self, u0, c, dt, lam):
+        """lam <- (d step/d u0)^T lam for one step from u0 (in place)."""
+        tr = self.traits()
+        self.prob.ctx.check(_lib().gf_rk_step_vjp(self.prob.handle, _dtype_code(lam[0]),
+                                                  C.byref(tr), A.ptr_array(u0),
+                                                  A.ptr_array(c or []), dt, A.ptr_array(lam)),
+                            "GBurgers::step_vjp")
+
+    def adjoint_gradient(self, u0, c, u_obs, dt, nsteps, checkpoint_every=10):
+        """(J, grad): J = 1/2 sum_k ||u_k(T) - obs_k||_M^2 after nsteps steps
+        from u0, and dJ/du0, with a checkpoint every `checkpoint_every`
+        steps and recomputation."""
+        import torch
+        tr = self.traits()
+        grad = [torch.empty_like(a) for a in u0]
+        J = C.c_double(0.0)
+        self.prob.ctx.check(_lib().gf_adjoint_gradient(
+            self.prob.handle, C.byref(tr), A.ptr_array(u0), A.ptr_array(c or []),
+            A.ptr_array(u_obs), dt, nsteps, checkpoint_every, C.byref(J), A.ptr_array(grad)),
+            "GBurgers::adjoint_gradient")
+        return J.value, grad
