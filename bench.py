@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample-ne", type=int, default=16)
     ap.add_argument("--cpu-iters", type=int, default=150)
+    ap.add_argument("--inner", type=float, default=None,
+                    help="mixed: relative drop per restarted FP32 run (0: reliable updates)")
     ap.add_argument("--ru", type=int, default=32,
                     help="FP32 iterations between FP64 residual replacements (mixed solve)")
     ap.add_argument("--mixed-apply", type=int, default=0,
@@ -447,8 +449,9 @@ def main():
     common = dict(maxit=50000, normtype=A.GF_NORM_EUC, tol=args.tol, precond=A.GF_PRECOND_JACOBI,
                   relative=1)
     # mixed: FP64 residual replacement every args.ru FP32 iterations
+    mix_kw = {} if args.inner is None else {"inner_tol": args.inner}
     tr_mix = CGTraits(precision=A.GF_CG_MIXED, check_every=args.ru, mixed_apply=args.mixed_apply,
-                      **common)
+                      **mix_kw, **common)
     tr_64 = CGTraits(precision=A.GF_CG_FP64, check_every=32, **common)
     if args.only == "apply":
         roof = kernel_roofline(ctx, prob, measured_peaks(), reps=args.steps)

@@ -16,8 +16,9 @@
 // round trip:
 //   1. q_E = A_e w   fused element apply, w gathered from the unique nodes
 //                    (box lattice indices computed, or node_class)
-//   2. q = mask * assemble(q_E), <w,q>   one thread per unique node folds
-//                    its element copies in ascending local id; the last
+//   2. q = mask * assemble(q_E), <w,q>   each unique node's element copies
+//                    are folded in ascending local id (box: by the element
+//                    owning the node; CSR: one thread per class); the last
 //                    block forms alpha
 //   3. x += alpha w, r -= alpha q, rho' = <r, Dinv r>, norm(r); the last
 //                    block forms beta and sets `done` at convergence
@@ -55,6 +56,8 @@ enum {
   S_NORMT,  // norm type
   S_REL,    // relative stop rule
   S_RES,    // norm of the last assembled residual pass
+  S_OTOL,   // stop threshold of the whole solve (S_RTOL: of the current run)
+  S_INNER,  // restarted mixed solve: relative tolerance of each FP32 run
   S_COUNT
 };
 
@@ -176,6 +179,85 @@ struct MapBox {
     }
     for (int i = 0; i < k; i++) f((int64_t)m[i]);
   }
+  // f(c, s) for every lattice point c, s = sum of its element copies in
+  // ascending local id (added in TS).  Walked by element: every lattice
+  // point is owned by one element, the one holding it at local index < P in
+  // every direction (or P on a non-periodic upper boundary), and the
+  // element's N^2 threads each take one (l0, l1) column of its owned
+  // points.  The other members sit at index P of the lower neighbours, so
+  // each element-local value is read exactly once, by whole element
+  // planes, with all index arithmetic fixed per thread.  Needs blockDim.x
+  // = RED_THREADS.
+  template <typename TS, typename TV, class F>
+  __device__ __forceinline__ void rows_sum(const TV *__restrict__ inE, F f) const {
+    if (!sorted) {
+      rows([&](int64_t c, const int(&g)[3]) {
+        TS s = TS(0);
+        each(c, g, [&](int64_t m) { s = __fadd_rn_t(s, (TS)inE[m]); });
+        f(c, s);
+      });
+      return;
+    }
+    constexpr int NN = N * N, EPB = (RED_THREADS / NN) < 1 ? 1 : RED_THREADS / NN;
+    const int slot = threadIdx.x / NN, t = threadIdx.x % NN;
+    if (slot >= EPB) return;
+    const int l0 = t % N, l1 = t / N;
+    const bool d3 = dim > 2;
+    const int64_t nn = d3 ? (int64_t)NN * N : NN;
+    const int64_t nel = (int64_t)ne[0] * ne[1] * (d3 ? ne[2] : 1);
+    const int64_t sy = ne[0], sz = (int64_t)ne[0] * ne[1];
+    for (int64_t e = (int64_t)blockIdx.x * EPB + slot; e < nel; e += (int64_t)gridDim.x * EPB) {
+      const int ec0 = (int)(e % ne[0]);
+      const int64_t rr = e / ne[0];
+      const int ec1 = (int)(rr % ne[1]), ec2 = d3 ? (int)(rr / ne[1]) : 0;
+      if (l0 == P && (per[0] || ec0 != ne[0] - 1)) continue;  // owned by the x-neighbour
+      if (l1 == P && (per[1] || ec1 != ne[1] - 1)) continue;
+      // members per direction as (element offset, local index), ascending
+      int64_t dx[2] = {0, 0}, dy[2] = {0, 0};
+      int lx[2] = {l0, l0}, ly[2] = {l1, l1};
+      int nx = 1, ny = 1;
+      if (l0 == 0 && (per[0] || ec0 > 0)) {
+        nx = 2;
+        if (ec0 > 0) { dx[0] = -1; lx[0] = P; }
+        else { dx[1] = ne[0] - 1; lx[1] = P; }
+      }
+      if (l1 == 0 && (per[1] || ec1 > 0)) {
+        ny = 2;
+        if (ec1 > 0) { dy[0] = -sy; ly[0] = P; }
+        else { dy[1] = (ne[1] - 1) * sy; ly[1] = P; }
+      }
+      const int64_t cxy = (int64_t)ec0 * P + l0 + (int64_t)M[0] * ((int64_t)ec1 * P + l1);
+      const int64_t plane = (int64_t)M[0] * M[1];
+#pragma unroll
+      for (int l2 = 0; l2 < (d3 ? N : 1); l2++) {
+        if (d3 && l2 == P && (per[2] || ec2 != ne[2] - 1)) continue;
+        int64_t dz[2] = {0, 0};
+        int lz[2] = {l2, l2}, nz = 1;
+        if (d3 && l2 == 0 && (per[2] || ec2 > 0)) {
+          nz = 2;
+          if (ec2 > 0) { dz[0] = -sz; lz[0] = P; }
+          else { dz[1] = (ne[2] - 1) * sz; lz[1] = P; }
+        }
+        TS s = TS(0);
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+          if (a >= nz) break;
+#pragma unroll
+          for (int b = 0; b < 2; b++) {
+            if (b >= ny) break;
+            const int64_t eb = e + dz[a] + dy[b];
+            const int off = NN * lz[a] + N * ly[b];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+              if (i >= nx) break;
+              s = __fadd_rn_t(s, (TS)inE[(eb + dx[i]) * nn + off + lx[i]]);
+            }
+          }
+        }
+        f(cxy + (d3 ? plane * ((int64_t)ec2 * P + l2) : 0), s);
+      }
+    }
+  }
   __device__ __forceinline__ double mult(int64_t, const int (&g)[3]) const {
     int m = 1;
     for (int d = 0; d < dim; d++) {
@@ -219,6 +301,15 @@ struct MapCsr {
   __device__ __forceinline__ double mult(int64_t c, const int (&)[3]) const {
     return (double)(ptr[c + 1] - ptr[c]);
   }
+  template <typename TS, typename TV, class F>
+  __device__ __forceinline__ void rows_sum(const TV *__restrict__ inE, F f) const {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nL;
+         c += (int64_t)gridDim.x * blockDim.x) {
+      TS s = TS(0);
+      for (int32_t k = ptr[c]; k < ptr[c + 1]; k++) s = __fadd_rn_t(s, (TS)inE[mem[k]]);
+      f(c, s);
+    }
+  }
   __device__ __forceinline__ int64_t lof(int64_t i) const { return ncls[i]; }
 };
 
@@ -256,11 +347,7 @@ __device__ __forceinline__ double acc(double a, double t) {
 // out_L[c] = sum of the element copies (ascending local id), FP64
 template <class MAP, typename TI>
 __global__ void k_assemble(int64_t nL, MAP map, const TI *__restrict__ inE, double *__restrict__ outL) {
-  map.rows([&](int64_t c, const int(&g)[3]) {
-    double s = 0.0;
-    map.each(c, g, [&](int64_t m) { s = __dadd_rn(s, (double)inE[m]); });
-    outL[c] = s;
-  });
+  map.template rows_sum<double>(inE, [&](int64_t c, double s) { outL[c] = s; });
 }
 
 // x_L[c] = x_E[smallest member]  (x_E is duplicate-consistent)
@@ -331,6 +418,10 @@ __global__ void __launch_bounds__(RED_THREADS)
 // solve-precision copy r_T and rho = <r_T, Dinv r_T>.
 //   mode 0 (start): w_T = Dinv r_T and a fresh CG state: rtol from the
 //     reference rule on norm(b), rnorm = 10 rtol, iter = 0.
+//   mode 1 (restart of the mixed solve after a correction): a fresh CG
+//     state on the new residual; the iteration count is kept; `done` = 2
+//     when the true residual meets the solve's threshold, else the next
+//     FP32 run stops at max(inner * norm(r), threshold).
 //   mode 2 (reliable update of the mixed solve): the search direction w_T
 //     and the iteration count are kept; rnorm becomes the true residual
 //     norm and `done` is set only if that meets rtol (or maxit is spent).
@@ -343,9 +434,7 @@ __global__ void __launch_bounds__(RED_THREADS)
   __shared__ double sh[32];
   const int normtype = (int)scal[S_NORMT];
   double rho = 0.0, rn = 0.0;
-  map.rows([&](int64_t c, const int(&g)[3]) {
-    double s = 0.0;
-    map.each(c, g, [&](int64_t m) { s = __dadd_rn(s, qE[m]); });
+  map.template rows_sum<double>(qE, [&](int64_t c, double s) {
     double r = bL[c] - s;
     if (wt.maskL && !wt.maskL[c]) r = 0.0;
     rL[c] = r;
@@ -374,11 +463,19 @@ __global__ void __launch_bounds__(RED_THREADS)
         if (bad) scal[S_FLAG] = 1.0;
         scal[S_DONE] =
             (rnorm <= scal[S_RTOL] || scal[S_ITER] >= scal[S_MAXIT] || bad) ? 2.0 : 0.0;
+      } else if (mode == 1) {
+        const double otol = scal[S_OTOL];
+        scal[S_RNORM] = rnorm;
+        const bool bad = !isfinite(rnorm) || !isfinite(rho_t);
+        if (bad) scal[S_FLAG] = 1.0;
+        scal[S_DONE] = (rnorm <= otol || scal[S_ITER] >= scal[S_MAXIT] || bad) ? 2.0 : 0.0;
+        scal[S_RTOL] = fmax(scal[S_INNER] * rnorm, otol);
       } else {
         const double bnorm = scal[S_BNORM];
         const double rtol = (scal[S_REL] != 0.0 || bnorm >= 1.0) ? tol * bnorm : tol;
-        scal[S_RTOL] = rtol;
-        scal[S_RNORM] = 10.0 * rtol;
+        scal[S_OTOL] = rtol;
+        scal[S_RTOL] = scal[S_INNER] > 0.0 ? fmax(scal[S_INNER] * rnorm, rtol) : rtol;
+        scal[S_RNORM] = 10.0 * scal[S_RTOL];
         scal[S_ITER] = 0.0;
         scal[S_FLAG] = 0.0;
         scal[S_DONE] = (scal[S_MAXIT] <= 0.0 || !(10.0 * rtol > rtol)) ? 1.0 : 0.0;
@@ -396,9 +493,7 @@ __global__ void __launch_bounds__(RED_THREADS)
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
   double dot = 0.0;
-  map.rows([&](int64_t c, const int(&g)[3]) {
-    T s = T(0);
-    map.each(c, g, [&](int64_t m) { s = __fadd_rn_t(s, qE[m]); });
+  map.template rows_sum<T>(qE, [&](int64_t c, T s) {
     if (wt.maskL && !wt.maskL[c]) s = T(0);
     qL[c] = s;
     dot += (double)w[c] * (double)s;
@@ -560,6 +655,7 @@ struct Solver {
     h[S_NORMT] = (double)tr.normtype;
     h[S_IVOL] = 1.0 / prob->volume;
     h[S_REL] = relative ? 1.0 : 0.0;
+    h[S_INNER] = (tr.precision == GF_CG_MIXED && tr.inner_tol > 0.0) ? tr.inner_tol : 0.0;
   }
 
   // Jacobi inverse diagonal on unique nodes (FP64 and FP32), slots 8/9/10
@@ -728,7 +824,35 @@ struct Solver {
       if (r2) return gf_fail(ctx, r2, "residual failed");
       GF_CUDA(ctx, cudaMemsetAsync(x32, 0, sizeof(float) * nL, st));
       rc = GF_CG_NOCONVERGE;
-      for (;;) {
+      // Restarted refinement (inner_tol > 0): each FP32 PCG run solves
+      // A y = r from y = 0 to inner_tol * norm(r); x += y in FP64 and the
+      // next run starts on the true FP64 residual.
+      for (int refine = 0; tr.inner_tol > 0.0; refine++) {
+        int its = 0;
+        const int left = std::max(1, tr.maxit - total);
+        if ((r2 = iterate<float>(tr, left, p, q, use_mass, x32, r32, w32, q32, qE32, d32, nullptr,
+                                 &its)))
+          return r2;
+        prob->launches += 1;
+        k_add_correction<<<gL, 256, 0, st>>>(nL, x32, xL);
+        GF_CUDA(ctx, cudaMemsetAsync(x32, 0, sizeof(float) * nL, st));
+        r2 = residual<float>(p, q, use_mass, bL, xL, qE, rL, r32, w32, d32, 1, tr.tol);
+        if (r2) return gf_fail(ctx, r2, "residual failed");
+        GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h, prob->scal_d, sizeof(double) * S_COUNT,
+                                     cudaMemcpyDeviceToHost, st));
+        GF_CUDA(ctx, cudaStreamSynchronize(st));
+        const double *h = prob->scal_h;
+        total = (int)h[S_ITER];
+        rn = h[S_RES];
+        if (h[S_FLAG] != 0.0)
+          return gf_fail(ctx, GF_ERR_NONFINITE, "CG breakdown at iteration %d", total);
+        if (rn <= h[S_OTOL]) {
+          rc = GF_OK;
+          break;
+        }
+        if (total >= tr.maxit || (tr.max_refine > 0 && refine + 1 >= tr.max_refine)) break;
+      }
+      for (; !(tr.inner_tol > 0.0);) {
         enqueue<float>(every, p, q, use_mass, x32, r32, w32, q32, qE32, d32, nullptr);
         prob->launches += 1;
         k_add_correction<<<gL, 256, 0, st>>>(nL, x32, xL);

@@ -23,6 +23,25 @@ int gf_fail(gf_context *ctx, int code, const char *fmt, ...) {
   return code;
 }
 
+namespace gfk {
+// K1(l,m) = sum_i D(i,l) W_i D(i,m), D(i,m) = D[i + m*n], accumulated in
+// long double, then averaged with its centro-reflection K1(n-1-l, n-1-m)
+// (equal in exact arithmetic) so that the even-odd form is exact.
+void gf_k1_matrix(int n, const double *D, const double *W, double *K1) {
+  std::vector<long double> K((size_t)n * n);
+  for (int l = 0; l < n; l++)
+    for (int m = 0; m < n; m++) {
+      long double s = 0.0L;
+      for (int i = 0; i < n; i++)
+        s += ((long double)D[i + l * n] * (long double)D[i + m * n]) * (long double)W[i];
+      K[l + m * n] = s;
+    }
+  for (int l = 0; l < n; l++)
+    for (int m = 0; m < n; m++)
+      K1[l + m * n] = (double)(0.5L * (K[l + m * n] + K[(n - 1 - l) + (n - 1 - m) * n]));
+}
+}  // namespace gfk
+
 void *gf_work(gf_problem *prob, int slot, size_t bytes) {
   if ((int)prob->work.size() <= slot) prob->work.resize(slot + 1);
   gf_buffer &b = prob->work[slot];
@@ -467,6 +486,7 @@ extern "C" int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *d, gf_prob
   p->geom = d->geom;
   std::memcpy(p->D, d->D, sizeof(double) * n * n);
   std::memcpy(p->W, d->W, sizeof(double) * n);
+  gfk::gf_k1_matrix(n, p->D, p->W, p->K1);
 
   // geometry
   std::vector<double> jac(N), X0(N);

@@ -42,6 +42,7 @@ struct gf_problem {
   double volume = 0.0;  // sum of the local mass (integral of 1)
   double D[GF_MAXN * GF_MAXN];
   double W[GF_MAXN];
+  double K1[GF_MAXN * GF_MAXN];  // D^T diag(W) D (affine-element apply)
   // device geometry (both precisions)
   double *egeom_d = nullptr;  // ne*(dim+1) (AFFINE)
   float *egeom_f = nullptr;
@@ -100,6 +101,12 @@ int gf_fail(gf_context *ctx, int code, const char *fmt, ...);
 // Returns a device buffer of at least `bytes` from slot `slot` of the
 // problem's scratch list (allocated once, reused).
 void *gf_work(gf_problem *prob, int slot, size_t bytes);
+
+namespace gfk {
+// K1 = D^T diag(W) D of a GLL basis (n points), exactly symmetric and
+// centro-symmetric; column-major like D.
+void gf_k1_matrix(int n, const double *D, const double *W, double *K1);
+}  // namespace gfk
 
 // ---- per-order constants passed by value to kernels ----
 // D is stored column-major: D(l,j) = D[l + j*N].

@@ -6,6 +6,7 @@
 
 #include "gf_common.cuh"
 #include "k_dudt.cuh"
+#include "k_helm_k1.cuh"
 #include "k_tensor.cuh"
 
 namespace gfk {
@@ -28,9 +29,22 @@ struct HelmLaunch {
   struct F {
     static int run(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
                    LD ld, TO *uo, cudaStream_t st, const double *stop) {
-      const Basis<T, N> B = make_basis<T, N>(prob);
       const Geom<T> g = geom_of<T>(prob);
       constexpr int P = Pad<N>::P;
+      if (prob->dim == 3 && g.egeom && !pvec) {
+        // affine elements, scalar p: one K1 contraction per direction
+        constexpr int EPB = epb_k1<N>();
+        const K1Basis<T, N> KB = make_k1basis<T, N>(prob);
+        const size_t smem = sizeof(T) * 2 * N * N * P * EPB;
+        auto kern = k_helm3d_k1<T, N, EPB, LD, TO>;
+        set_smem(kern, smem);
+        const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+        prob->launches++;
+        kern<<<grid, dim3(N * N, EPB), smem, st>>>(KB, g.egeom, prob->ne, p, q, qvec, use_mass, ld,
+                                                    uo, stop);
+        return GF_OK;
+      }
+      const Basis<T, N> B = make_basis<T, N>(prob);
       if (prob->dim == 3) {
         constexpr int EPB = epb3<N>();
         const size_t smem = sizeof(T) * 3 * N * N * P * EPB;

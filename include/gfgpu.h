@@ -187,8 +187,10 @@ typedef struct {
   double tol;       /* stop when norm(r) <= (norm(b) < 1 ? tol : tol*norm(b)) */
   int precond;      /* GF_PRECOND_* (Jacobi has no reference counterpart) */
   int precision;    /* GF_CG_FP64 or GF_CG_MIXED */
-  double inner_tol; /* MIXED: relative residual drop per FP32 inner solve */
-  int max_refine;   /* MIXED: maximum refinement sweeps */
+  double inner_tol; /* MIXED: > 0 restarted refinement, each FP32 PCG run
+                       reduces the true residual by this factor; 0 one FP32
+                       PCG run with reliable updates every check_every its */
+  int max_refine;   /* MIXED, restarted: maximum refinement sweeps (0: no cap) */
   int check_every;  /* iterations between host convergence checks (>=1) */
   int relative;     /* 1: stop at norm(r) <= tol*norm(b) even when norm(b) < 1 */
   int mixed_apply;  /* MIXED, 3-d: 0 FP32 arithmetic in the FP32 solve's applies,

@@ -231,8 +231,11 @@ def test_cg_helmholtz_3d_matches_oracle(ctx, precond, structured):
     assert relerr(host(x), xo) < 1e-10
 
 
+@pytest.mark.parametrize("inner", [0.0, 1e-4])
 @pytest.mark.parametrize("structured", [True, False])
-def test_cg_mixed_precision_reaches_fp64_solution(ctx, structured):
+def test_cg_mixed_precision_reaches_fp64_solution(ctx, structured, inner):
+    """inner = 0: one FP32 PCG run with reliable updates; inner > 0:
+    restarted refinement, each FP32 run reducing the residual by `inner`."""
     g, prob, o = setup(ctx, 3, [3, 3, 3], 6, structured=structured)
     rng = np.random.default_rng(8)
     f = rng.standard_normal(g.ndof())
@@ -245,13 +248,15 @@ def test_cg_mixed_precision_reaches_fp64_solution(ctx, structured):
     cg64 = GCG(CGTraits(**common), prob)
     assert cg64.solve(H, dev(b), dev(0 * b), x64) == 0
     xm = prob.zeros()
-    cgm = GCG(CGTraits(precision=A.GF_CG_MIXED, check_every=16, **common), prob)
+    cgm = GCG(CGTraits(precision=A.GF_CG_MIXED, check_every=16, inner_tol=inner, **common), prob)
     rc = cgm.solve(H, dev(b), dev(0 * b), xm)
     assert rc == 0
     # both meet a 1e-12 relative residual; the solutions agree to ~kappa * 1e-12
     assert relerr(host(xm), host(x64)) < 1e-9
-    # the FP32 Krylov run is never restarted: about the FP64 iteration count
-    assert cgm.get_iteration_count() <= 1.5 * cg64.get_iteration_count() + 32
+    # reliable updates never restart the FP32 Krylov run: about the FP64
+    # count; restarts rebuild the Krylov space once per refinement sweep
+    bound = 1.5 if inner == 0.0 else 3.0
+    assert cgm.get_iteration_count() <= bound * cg64.get_iteration_count() + 32
 
 
 def test_rk4_advection_2d_matches_oracle(ctx):
