@@ -67,7 +67,11 @@ def parse():
                     help="FP32 iterations between FP64 residual replacements (mixed solve)")
     ap.add_argument("--mixed-apply", type=int, default=0,
                     help="mixed solve: 1 = FP64 arithmetic in the FP32-stored applies")
-    ap.add_argument("--only", choices=["fp64", "mixed", "apply"], default=None,
+    ap.add_argument("--poly", type=int, default=2,
+                    help="FP32 applies per Chebyshev preconditioner application")
+    ap.add_argument("--poly-ratio", type=float, default=0.0,
+                    help="b/a of the Chebyshev interval (0: library default)")
+    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply"], default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
 
@@ -453,15 +457,23 @@ def main():
     tr_mix = CGTraits(precision=A.GF_CG_MIXED, check_every=args.ru, mixed_apply=args.mixed_apply,
                       **mix_kw, **common)
     tr_64 = CGTraits(precision=A.GF_CG_FP64, check_every=32, **common)
+    # FP64 flexible CG with the FP32 Chebyshev polynomial preconditioner
+    tr_cheb = CGTraits(precision=A.GF_CG_MIXED, check_every=4, poly_degree=args.poly,
+                       poly_ratio=args.poly_ratio,
+                       **dict(common, precond=A.GF_PRECOND_CHEBYSHEV))
     if args.only == "apply":
         roof = kernel_roofline(ctx, prob, measured_peaks(), reps=args.steps)
         print(json.dumps({"only": "apply", "helm3d": roof}), flush=True)
         return
     if args.only:
-        tr = tr_64 if args.only == "fp64" else tr_mix
-        t, it, rc, _ = time_solves(ctx, prob, H, b, tr, args.steps, args.warmup)
-        print(json.dumps({"only": args.only, "s_per_solve": statistics.mean(t),
-                          "iterations": it[-1], "rc": rc}), flush=True)
+        tr = {"fp64": tr_64, "mixed": tr_mix, "cheb": tr_cheb}[args.only]
+        t, it, rc, x = time_solves(ctx, prob, H, b, tr, args.steps, args.warmup)
+        out = {"only": args.only, "s_per_solve": statistics.mean(t), "iterations": it[-1],
+               "rc": rc}
+        if args.only != "fp64":
+            _, _, _, x64 = time_solves(ctx, prob, H, b, tr_64, 1, 0)
+            out["rel_diff_vs_fp64"] = float((x - x64).abs().max() / x64.abs().max())
+        print(json.dumps(out), flush=True)
         return
 
     def barrier():

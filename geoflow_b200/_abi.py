@@ -24,7 +24,7 @@ GF_ERR_NONFINITE, GF_ERR_WATCHDOG = -5, -6
 GF_F64, GF_F32 = 0, 1
 GF_DSS_SUM, GF_DSS_SMOOTH, GF_DSS_MAX, GF_DSS_MIN = 0, 1, 2, 3
 GF_NORM_INF, GF_NORM_EUC, GF_NORM_L2, GF_NORM_L1 = 0, 1, 2, 3
-GF_PRECOND_NONE, GF_PRECOND_JACOBI = 0, 1
+GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV = 0, 1, 2
 GF_CG_FP64, GF_CG_MIXED = 0, 1
 GF_GEOM_AFFINE, GF_GEOM_REGULAR = 0, 1
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
@@ -49,6 +49,7 @@ class CGTraits(C.Structure):
         ("maxit", c_int), ("normtype", c_int), ("tol", c_double), ("precond", c_int),
         ("precision", c_int), ("inner_tol", c_double), ("max_refine", c_int),
         ("check_every", c_int), ("relative", c_int), ("mixed_apply", c_int),
+        ("poly_degree", c_int), ("poly_ratio", c_double),
     ]
 
 

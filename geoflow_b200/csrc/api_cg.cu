@@ -58,6 +58,8 @@ enum {
   S_RES,    // norm of the last assembled residual pass
   S_OTOL,   // stop threshold of the whole solve (S_RTOL: of the current run)
   S_INNER,  // restarted mixed solve: relative tolerance of each FP32 run
+  S_ZR,     // polynomial-preconditioned solve: <r, z> of the last step
+  S_FIRST,  // polynomial-preconditioned solve: 1 before its first step
   S_COUNT
 };
 
@@ -520,7 +522,8 @@ template <typename T, class MAP>
 __global__ void __launch_bounds__(RED_THREADS)
     k_update(int64_t nL, MAP map, Weights wt, T *__restrict__ x, const T *__restrict__ w,
              T *__restrict__ r, const T *__restrict__ q, const T *__restrict__ dinv,
-             double *__restrict__ hist, double *scal, double *partials, unsigned int *counter) {
+             double *__restrict__ hist, double *__restrict__ ab, int nab, double *scal,
+             double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
   const int normtype = (int)scal[S_NORMT];
@@ -551,6 +554,10 @@ __global__ void __launch_bounds__(RED_THREADS)
       scal[S_BETA] = beta;
       scal[S_RNORM] = rnorm;
       if (hist) hist[it] = rnorm;
+      if (ab && it < nab) {  // Lanczos coefficients of the preconditioned operator
+        ab[2 * it] = scal[S_ALPHA];
+        ab[2 * it + 1] = beta;
+      }
       scal[S_ITER] = (double)(it + 1);
       const bool bad = !isfinite(rnorm) || !isfinite(beta);
       if (bad) scal[S_FLAG] = 1.0;
@@ -576,6 +583,108 @@ __global__ void k_wupdate(int64_t nL, T *__restrict__ w, const T *__restrict__ r
 // x_L += (double) d_L
 __global__ void k_add_correction(int64_t nL, const float *__restrict__ d, double *__restrict__ x) {
   GRID_STRIDE(c, nL) { x[c] += (double)d[c]; }
+}
+
+// ---- FP32 Chebyshev polynomial preconditioner z = P(r) ----
+// The Chebyshev iteration for D^-1 A z = D^-1 r on the eigenvalue interval
+// [a, b] (Saad, Iterative Methods for Sparse Linear Systems, 2nd ed.,
+// Algorithm 12.1), run for a fixed number of steps from z = 0:
+//   res_0 = r, d_0 = D^-1 res_0 / theta, z_1 = d_0,
+//   res_j = res_{j-1} - A d_{j-1},  d_j = c1_j d_{j-1} + c2_j D^-1 res_j,
+//   z_{j+1} = z_j + d_j,
+// theta = (a+b)/2.  With fixed coefficients z is a fixed polynomial in
+// D^-1 A applied to D^-1 r: symmetric, and positive definite when b bounds
+// the spectrum.  The pass that produces the final z also reduces
+// <r, z> and <z, q> for the flexible CG step (fcg_finish).
+__device__ __forceinline__ void fcg_finish(double rz, double zq, double *scal, double *partials,
+                                           unsigned int *counter, double *sh) {
+  double pv[2] = {rz, zq};
+  if (publish_partials<2>(pv, partials, counter, gridDim.x)) {
+    const double rz_t = fold_partials<false>(partials, gridDim.x, sh);
+    const double zq_t = fold_partials<false>(partials + gridDim.x, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      // Polak-Ribiere beta = <z, r - r_old> / <z_old, r_old>, with
+      // r - r_old = -alpha q: robust to a preconditioner that is not
+      // exactly linear (FP32 rounding)
+      const double beta = scal[S_FIRST] != 0.0 ? 0.0 : -scal[S_ALPHA] * zq_t / scal[S_ZR];
+      scal[S_BETA] = beta;
+      scal[S_ZR] = rz_t;
+      scal[S_RHO] = rz_t;
+      scal[S_FIRST] = 0.0;
+      if (!isfinite(beta) || !isfinite(rz_t) || !(rz_t > 0.0)) {
+        scal[S_FLAG] = 1.0;
+        scal[S_DONE] = 2.0;
+      }
+      *counter = 0;
+    }
+  }
+}
+
+// res = (float) r, d = z = dinv res / theta  (last: also the FCG scalars)
+__global__ void __launch_bounds__(RED_THREADS)
+    k_cheb_init(int64_t nL, const double *__restrict__ r, const float *__restrict__ dinv, float c0,
+                float *__restrict__ res, float *__restrict__ d, float *__restrict__ z, int last,
+                const double *__restrict__ q, double *scal, double *partials,
+                unsigned int *counter) {
+  __shared__ double sh[32];
+  if (scal[S_DONE] != 0.0) return;
+  double rz = 0.0, zq = 0.0;
+  GRID_STRIDE(c, nL) {
+    const double r64 = r[c];
+    const float rc = (float)r64;
+    const float dc = c0 * (dinv[c] * rc);
+    z[c] = dc;
+    if (last) {
+      rz += r64 * (double)dc;
+      zq += (double)dc * q[c];
+    } else {
+      res[c] = rc;
+      d[c] = dc;
+    }
+  }
+  if (!last) return;
+  rz = block_reduce<false>(rz, sh);
+  zq = block_reduce<false>(zq, sh);
+  fcg_finish(rz, zq, scal, partials, counter, sh);
+}
+
+// res -= mask assemble(qE) (= A d), d = c1 d + c2 dinv res, z += d
+template <class MAP>
+__global__ void __launch_bounds__(RED_THREADS)
+    k_cheb_step(int64_t nL, MAP map, Weights wt, const float *__restrict__ qE,
+                const float *__restrict__ dinv, float c1, float c2, float *__restrict__ res,
+                float *__restrict__ d, float *__restrict__ z, int last,
+                const double *__restrict__ r, const double *__restrict__ q, double *scal,
+                double *partials, unsigned int *counter) {
+  __shared__ double sh[32];
+  if (scal[S_DONE] != 0.0) return;
+  double rz = 0.0, zq = 0.0;
+  map.template rows_sum<float>(qE, [&](int64_t c, float s) {
+    if (wt.maskL && !wt.maskL[c]) s = 0.0f;
+    const float rc = res[c] - s;
+    const float dc = c1 * d[c] + c2 * (dinv[c] * rc);
+    const float zc = z[c] + dc;
+    z[c] = zc;
+    if (last) {
+      rz += r[c] * (double)zc;
+      zq += (double)zc * q[c];
+    } else {
+      res[c] = rc;
+      d[c] = dc;
+    }
+  });
+  if (!last) return;
+  rz = block_reduce<false>(rz, sh);
+  zq = block_reduce<false>(zq, sh);
+  fcg_finish(rz, zq, scal, partials, counter, sh);
+}
+
+// w = z + beta w  (FP64 search direction, FP32 preconditioned residual)
+__global__ void k_fcg_w(int64_t nL, double *__restrict__ w, const float *__restrict__ z,
+                        const double *scal) {
+  if (scal[S_DONE] != 0.0) return;
+  const double beta = scal[S_BETA];
+  GRID_STRIDE(c, nL) { w[c] = fma(beta, w[c], (double)z[c]); }
 }
 
 // local diagonal of p L + q M at every element-local node
@@ -627,6 +736,42 @@ __global__ void k_invert(int64_t n, const double *__restrict__ d, double *__rest
 }
 
 // ---------------------------------------------------------------------
+// Largest eigenvalue of the Lanczos tridiagonal built from n PCG steps
+// (alpha_j, beta_j = rho_{j+1}/rho_j): T_jj = 1/alpha_j + beta_{j-1}/alpha_{j-1},
+// T_j,j+1 = sqrt(beta_j)/alpha_j.  Its eigenvalues are Ritz values of the
+// preconditioned operator, the largest converging fast from below.
+// Bisection on the Sturm count; returns 0 when the coefficients are unusable.
+double lanczos_max(const double *ab, int n) {
+  std::vector<double> dg(n), off(n > 1 ? n - 1 : 1, 0.0);
+  for (int j = 0; j < n; j++) {
+    const double a = ab[2 * j], b = ab[2 * j + 1];
+    if (!(a > 0.0) || !std::isfinite(a) || !(b >= 0.0) || !std::isfinite(b)) return 0.0;
+    dg[j] = 1.0 / a + (j > 0 ? ab[2 * j - 1] / ab[2 * (j - 1)] : 0.0);
+    if (j < n - 1) off[j] = std::sqrt(b) / a;
+  }
+  double lo = 0.0, hi = 0.0;
+  for (int j = 0; j < n; j++) {
+    const double r = (j > 0 ? std::fabs(off[j - 1]) : 0.0) + (j < n - 1 ? std::fabs(off[j]) : 0.0);
+    hi = std::max(hi, dg[j] + r);
+  }
+  auto below = [&](double x) {  // eigenvalues < x
+    int cnt = 0;
+    double qv = 1.0;
+    for (int j = 0; j < n; j++) {
+      qv = dg[j] - x - (j > 0 ? off[j - 1] * off[j - 1] / qv : 0.0);
+      if (qv == 0.0) qv = -1e-300;
+      if (qv < 0.0) cnt++;
+    }
+    return cnt;
+  };
+  for (int it = 0; it < 200; it++) {
+    const double mid = 0.5 * (lo + hi);
+    if (below(mid) >= n) hi = mid;
+    else lo = mid;
+  }
+  return hi;
+}
+
 template <class MAP>
 struct Solver {
   gf_problem *prob;
@@ -636,6 +781,8 @@ struct Solver {
   Weights wt;
   int64_t nE, nL;
   unsigned gE, gL, gRed;
+  double *ab = nullptr;  // alpha, beta of the first nab iterations (Lanczos)
+  int nab = 0;
 
   Solver(gf_problem *p, MAP m, bool masked)
       : prob(p), ctx(p->ctx), st(p->ctx->stream), map(m), nE(p->nlocal), nL(p->nclass) {
@@ -693,11 +840,118 @@ struct Solver {
         launch_helm_L<T>(prob, (T)p, (T)q, use_mass, w, qE, st, scal + S_DONE);
       k_asm_dot<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, qE, w, qL, scal, prob->partials,
                                                       prob->counter);
-      k_update<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, x, w, r, qL, dinv, hist, scal,
-                                                     prob->partials, prob->counter);
+      k_update<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, x, w, r, qL, dinv, hist, ab,
+                                                     nab, scal, prob->partials, prob->counter);
       k_wupdate<T><<<gL, 256, 0, st>>>(nL, w, r, dinv, scal);
       prob->launches += 3;
     }
+  }
+
+  // Polynomial-preconditioned FP64 CG: per iteration the FP64 apply,
+  // assembly with <w,q>, x/r update and stop test, then z = P(r) in FP32
+  // (poly_degree FP32 applies) and w = z + beta w.
+  struct Poly {
+    int m = 0;            // FP32 applies per preconditioner application
+    float c0 = 0.0f;      // 1/theta
+    std::vector<float> c1, c2;  // step coefficients, index 1..m
+    double *w = nullptr, *qL = nullptr;
+    float *res = nullptr, *d = nullptr, *z = nullptr, *qE32 = nullptr;
+    const float *dinv = nullptr;
+  };
+
+  void precondition(const Poly &P, double p, double q, int use_mass, const double *rL) {
+    double *scal = prob->scal_d;
+    prob->launches += 1 + P.m;  // the applies count themselves
+    k_cheb_init<<<gRed, RED_THREADS, 0, st>>>(nL, rL, P.dinv, P.c0, P.res, P.d, P.z, P.m == 0,
+                                              P.qL, scal, prob->partials, prob->counter);
+    for (int j = 1; j <= P.m; j++) {
+      launch_helm_L<float>(prob, (float)p, (float)q, use_mass, P.d, P.qE32, st, scal + S_DONE);
+      k_cheb_step<MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, P.qE32, P.dinv, P.c1[j], P.c2[j],
+                                                     P.res, P.d, P.z, j == P.m, rL, P.qL, scal,
+                                                     prob->partials, prob->counter);
+    }
+  }
+
+  void enqueue_poly(int k, const Poly &P, double p, double q, int use_mass, double *x, double *r,
+                    double *qE, double *hist) {
+    double *scal = prob->scal_d;
+    for (int i = 0; i < k; i++) {
+      launch_helm_L<double>(prob, p, q, use_mass, P.w, qE, st, scal + S_DONE);
+      k_asm_dot<double, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, qE, P.w, P.qL, scal,
+                                                           prob->partials, prob->counter);
+      k_update<double, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, x, P.w, r, P.qL, nullptr,
+                                                          hist, nullptr, 0, scal, prob->partials,
+                                                          prob->counter);
+      precondition(P, p, q, use_mass, r);
+      k_fcg_w<<<gL, 256, 0, st>>>(nL, P.w, P.z, scal);
+      prob->launches += 3;
+    }
+  }
+
+  // FP64 flexible CG with the FP32 Chebyshev preconditioner.  The first
+  // LANCZOS iterations are plain Jacobi PCG; their alpha/beta give the
+  // largest eigenvalue of D^-1 A (Lanczos Ritz value, times a safety
+  // factor), which fixes the polynomial's interval [b/ratio, b].  The
+  // direction is then restarted with w = P(r) and CG continues with the
+  // polynomial preconditioner.  Iterations count FP64 outer steps.
+  static constexpr int LANCZOS = 12;
+  int solve_poly(const gf_cg_traits &tr, double p, double q, int use_mass, const double *bL,
+                 double *xL, double *rL, double *qE, const double *d64, const float *d32,
+                 double *hist, int *total, double *rn) {
+    Poly P;
+    P.m = std::max(0, tr.poly_degree);
+    P.dinv = d32;
+    P.w = (double *)gf_work(prob, 4, sizeof(double) * nL);
+    P.qL = (double *)gf_work(prob, 5, sizeof(double) * nL);
+    P.res = (float *)gf_work(prob, 11, sizeof(float) * nL);
+    P.d = (float *)gf_work(prob, 12, sizeof(float) * nL);
+    P.z = (float *)gf_work(prob, 13, sizeof(float) * nL);
+    P.qE32 = (float *)gf_work(prob, 15, sizeof(float) * nE);
+    double *abd = (double *)gf_work(prob, 17, sizeof(double) * 2 * LANCZOS);
+    if (!P.w || !P.qL || !P.res || !P.d || !P.z || !P.qE32 || !abd)
+      return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
+    int rc = residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, P.w, d64, 0, tr.tol);
+    if (rc) return gf_fail(ctx, rc, "residual failed");
+    const int n0 = std::min(tr.maxit, LANCZOS);
+    ab = abd;
+    nab = n0;
+    rc = iterate<double>(tr, n0, p, q, use_mass, xL, rL, P.w, P.qL, qE, d64, hist, total);
+    ab = nullptr;
+    nab = 0;
+    if (rc) return rc;
+    const double *h = prob->scal_h;
+    if (h[S_DONE] == 0.0 && *total < tr.maxit) {
+      double abh[2 * LANCZOS];
+      GF_CUDA(ctx, cudaMemcpy(abh, abd, sizeof(double) * 2 * *total, cudaMemcpyDeviceToHost));
+      const double lmax = lanczos_max(abh, *total);
+      if (!(lmax > 0.0)) return gf_fail(ctx, GF_ERR_NONFINITE, "eigenvalue estimate failed");
+      const double ratio = tr.poly_ratio > 1.0 ? tr.poly_ratio : std::max(4.0, 2.0 * P.m * P.m);
+      const double b = 1.1 * lmax, a = b / ratio;
+      const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+      P.c0 = (float)(1.0 / theta);
+      P.c1.assign(P.m + 1, 0.0f);
+      P.c2.assign(P.m + 1, 0.0f);
+      double rho = 1.0 / sigma;
+      for (int j = 1; j <= P.m; j++) {
+        const double rn1 = 1.0 / (2.0 * sigma - rho);
+        P.c1[j] = (float)(rn1 * rho);
+        P.c2[j] = (float)(2.0 * rn1 / delta);
+        rho = rn1;
+      }
+      // restart the direction: w = P(r)
+      prob->scal_h[S_FIRST] = 1.0;
+      GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_d + S_FIRST, prob->scal_h + S_FIRST, sizeof(double),
+                                   cudaMemcpyHostToDevice, st));
+      precondition(P, p, q, use_mass, rL);
+      prob->launches++;
+      k_fcg_w<<<gL, 256, 0, st>>>(nL, P.w, P.z, prob->scal_d);
+      rc = batches(tr, tr.maxit - *total, total, [&](int k) {
+        enqueue_poly(k, P, p, q, use_mass, xL, rL, qE, hist);
+      });
+      if (rc) return rc;
+    }
+    *rn = prob->scal_h[S_RNORM];
+    return (*total >= tr.maxit && *rn > prob->scal_h[S_RTOL]) ? GF_CG_NOCONVERGE : GF_OK;
   }
 
   // PCG iterations in precision T on unique-node vectors; the state
@@ -705,6 +959,16 @@ struct Solver {
   template <typename T>
   int iterate(const gf_cg_traits &tr, int maxit, double p, double q, int use_mass, T *x, T *r, T *w,
               T *qL, T *qE, const T *dinv, double *hist, int *iters) {
+    return batches(tr, maxit, iters, [&](int k) {
+      enqueue<T>(k, p, q, use_mass, x, r, w, qL, qE, dinv, hist);
+    });
+  }
+
+  // Queues iterations in batches of check_every (enq(k) queues k of them)
+  // and reads the device `done` flag one batch behind, so the GPU never
+  // waits for the host; stops at `done` or after maxit iterations.
+  template <class ENQ>
+  int batches(const gf_cg_traits &tr, int maxit, int *iters, ENQ enq) {
     double *scal = prob->scal_d;
     const int every = tr.check_every > 0 ? tr.check_every : 16;
     int issued = 0, pending = -1;
@@ -716,7 +980,7 @@ struct Solver {
     // the state may already be converged (maxit 0 or tol 0)
     while (!stop) {
       const int k = std::min(every, maxit - issued);
-      enqueue<T>(k, p, q, use_mass, x, r, w, qL, qE, dinv, hist);
+      enq(k);
       issued += k;
       GF_CHECK_LAUNCH(ctx);
       const int slot = (pending + 1) & 1;
@@ -778,7 +1042,7 @@ struct Solver {
     if (!bL || !xL || !rL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
     double *d64 = nullptr;
     float *d32 = nullptr;
-    if (tr.precond == GF_PRECOND_JACOBI) {
+    if (tr.precond != GF_PRECOND_NONE) {
       int rc = jacobi(p, q, use_mass, &d64, &d32);
       if (rc) return gf_fail(ctx, rc, "Jacobi set-up failed");
     }
@@ -794,7 +1058,10 @@ struct Solver {
         nE, tr.normtype, bE, prob->mass_d, prob->scal_d, prob->partials, prob->counter);
     int rc = GF_OK, total = 0;
     double rn = 0.0;
-    if (tr.precision == GF_CG_FP64) {
+    if (tr.precond == GF_PRECOND_CHEBYSHEV) {
+      rc = solve_poly(tr, p, q, use_mass, bL, xL, rL, qE, d64, d32, hist, &total, &rn);
+      if (rc < 0) return rc;
+    } else if (tr.precision == GF_CG_FP64) {
       double *w = (double *)gf_work(prob, 4, sizeof(double) * nL);
       double *qL = (double *)gf_work(prob, 5, sizeof(double) * nL);
       if (!w || !qL) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
@@ -905,8 +1172,12 @@ extern "C" int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *tr, double p, 
   GF_REQUIRE(ctx, tr->maxit >= 0, "maxit must be >= 0");
   GF_REQUIRE(ctx, tr->normtype >= GF_NORM_INF && tr->normtype <= GF_NORM_L1, "bad norm type");
   GF_REQUIRE(ctx, tr->precision == GF_CG_FP64 || tr->precision == GF_CG_MIXED, "bad precision");
-  GF_REQUIRE(ctx, tr->precond == GF_PRECOND_NONE || tr->precond == GF_PRECOND_JACOBI,
+  GF_REQUIRE(ctx, tr->precond == GF_PRECOND_NONE || tr->precond == GF_PRECOND_JACOBI ||
+                      tr->precond == GF_PRECOND_CHEBYSHEV,
              "bad preconditioner");
+  GF_REQUIRE(ctx, tr->precond != GF_PRECOND_CHEBYSHEV || (tr->poly_degree >= 0 &&
+                                                         tr->poly_degree <= 64),
+             "poly_degree must be 0..64");
   GF_CUDA(ctx, cudaSetDevice(ctx->device));
   double *hist = nullptr;
   if (residuals && tr->maxit > 0) {

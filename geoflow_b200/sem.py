@@ -271,16 +271,18 @@ class CGTraits:
     tol: float = 1e-6
     precond: int = A.GF_PRECOND_NONE
     precision: int = A.GF_CG_FP64
-    inner_tol: float = 1e-5
+    inner_tol: float = 0.0
     max_refine: int = 40
     check_every: int = 16
     relative: int = 0
     mixed_apply: int = 0
+    poly_degree: int = 2
+    poly_ratio: float = 0.0
 
     def to_c(self) -> A.CGTraits:
         t = A.CGTraits()
         for f in ("maxit", "normtype", "tol", "precond", "precision", "inner_tol", "max_refine",
-                  "check_every", "relative", "mixed_apply"):
+                  "check_every", "relative", "mixed_apply", "poly_degree", "poly_ratio"):
             setattr(t, f, getattr(self, f))
         return t
 

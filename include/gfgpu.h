@@ -50,7 +50,10 @@ enum {
 enum { GF_F64 = 0, GF_F32 = 1 };                       /* field dtype */
 enum { GF_DSS_SUM = 0, GF_DSS_SMOOTH = 1, GF_DSS_MAX = 2, GF_DSS_MIN = 3 }; /* ggfx.hpp:36-76 */
 enum { GF_NORM_INF = 0, GF_NORM_EUC = 1, GF_NORM_L2 = 2, GF_NORM_L1 = 3 }; /* lin_solver_base.hpp:38 */
-enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1 };
+/* CHEBYSHEV: FP64 flexible CG whose preconditioner is a Chebyshev
+ * polynomial in D^-1 A applied in FP32 (poly_degree FP32 applies per step);
+ * no reference counterpart */
+enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1, GF_PRECOND_CHEBYSHEV = 2 };
 enum { GF_CG_FP64 = 0, GF_CG_MIXED = 1 };            /* plain FP64 / FP32 apply + FP64 refinement */
 enum { GF_GEOM_AFFINE = 0, GF_GEOM_REGULAR = 1 };     /* see gf_problem_desc */
 enum { GF_EQN_ADVECT = 0, GF_EQN_BURGERS = 1, GF_EQN_HEAT = 2 }; /* GBurgers traits */
@@ -195,6 +198,10 @@ typedef struct {
   int relative;     /* 1: stop at norm(r) <= tol*norm(b) even when norm(b) < 1 */
   int mixed_apply;  /* MIXED, 3-d: 0 FP32 arithmetic in the FP32 solve's applies,
                        1 FP64 arithmetic on the FP32-stored vectors */
+  int poly_degree;  /* CHEBYSHEV: FP32 applies per preconditioner application */
+  double poly_ratio;/* CHEBYSHEV: b/a of the polynomial's interval [a, b], b from
+                       a Lanczos estimate of the largest eigenvalue of D^-1 A
+                       (<= 1: max(4, 2 poly_degree^2)) */
 } gf_cg_traits;
 
 /* Solves (p L + q M) x = b on the assembled space (DSS Sum + mask), as

@@ -5,6 +5,8 @@ Tolerances: bit-exact for the gather-scatter (integer maps, fixed fold
 order); FP64 operator applies within 1e-12 relative (max-norm); FP64
 solves and RK runs within 1e-10 relative; FP32 applies within 1e-5.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 import torch
@@ -257,6 +259,43 @@ def test_cg_mixed_precision_reaches_fp64_solution(ctx, structured, inner):
     # count; restarts rebuild the Krylov space once per refinement sweep
     bound = 1.5 if inner == 0.0 else 3.0
     assert cgm.get_iteration_count() <= bound * cg64.get_iteration_count() + 32
+
+
+@pytest.mark.parametrize("degree", [0, 3, 8])
+@pytest.mark.parametrize("structured,p", [(True, 6), (False, 5)])
+def test_cg_chebyshev_preconditioned_reaches_fp64_solution(ctx, structured, p, degree):
+    """FP64 flexible CG with the FP32 Chebyshev polynomial preconditioner
+    meets the same 1e-12 relative residual as plain FP64 Jacobi-PCG; the
+    solutions agree to ~kappa * 1e-12, in fewer FP64 iterations."""
+    g, prob, o = setup(ctx, 3, [3, 3, 3], p, structured=structured)
+    rng = np.random.default_rng(9)
+    f = rng.standard_normal(g.ndof())
+    f = f[g.members[g.class_ptr[:-1]]][g.node_class]
+    b = o.mass * f
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    common = dict(maxit=5000, tol=1e-12, normtype=A.GF_NORM_EUC, relative=1)
+    x64 = prob.zeros()
+    cg64 = GCG(CGTraits(precond=A.GF_PRECOND_JACOBI, **common), prob)
+    assert cg64.solve(H, dev(b), dev(0 * b), x64) == 0
+    xc = prob.zeros()
+    cgc = GCG(CGTraits(precond=A.GF_PRECOND_CHEBYSHEV, poly_degree=degree, **common), prob)
+    assert cgc.solve(H, dev(b), dev(0 * b), xc) == 0
+    assert relerr(host(xc), host(x64)) < 1e-9
+    if degree >= 3:
+        assert cgc.get_iteration_count() < cg64.get_iteration_count()
+
+
+def test_cg_chebyshev_rejects_bad_degree(ctx):
+    g, prob, o = setup(ctx, 3, [2, 2, 2], 4)
+    lib = A.load()
+    tr = CGTraits(precond=A.GF_PRECOND_CHEBYSHEV, poly_degree=65).to_c()
+    b = prob.zeros()
+    x = prob.zeros()
+    it = C.c_int()
+    rn = C.c_double()
+    assert lib.gf_cg_solve(prob.handle, C.byref(tr), 1.0, 1.0, 1, A.ptr(b), None, A.ptr(x),
+                           C.byref(it), C.byref(rn), None) == A.GF_ERR_ARG
 
 
 def test_rk4_advection_2d_matches_oracle(ctx):
