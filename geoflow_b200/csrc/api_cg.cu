@@ -28,6 +28,7 @@
 // iterations.
 #include <algorithm>
 #include <cmath>
+#include <unordered_map>
 #include <vector>
 
 #include "gf_common.cuh"
@@ -431,7 +432,7 @@ template <typename T, class MAP>
 __global__ void __launch_bounds__(RED_THREADS)
     k_resid(int64_t nL, MAP map, Weights wt, const double *__restrict__ bL,
             const double *__restrict__ qE, double *__restrict__ rL, T *__restrict__ rT,
-            T *__restrict__ wT, const T *__restrict__ dinv, int mode, double tol, double *scal,
+            T *__restrict__ wT, const float *__restrict__ dinv, int mode, double tol, double *scal,
             double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   const int normtype = (int)scal[S_NORMT];
@@ -441,7 +442,7 @@ __global__ void __launch_bounds__(RED_THREADS)
     if (wt.maskL && !wt.maskL[c]) r = 0.0;
     rL[c] = r;
     const T rt = (T)r;
-    const T zt = dinv ? dinv[c] * rt : rt;
+    const T zt = dinv ? (T)dinv[c] * rt : rt;
     if (rT != (T *)rL) rT[c] = rt;
     if (mode != 2) wT[c] = zt;
     rho += (double)rt * (double)zt;
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(RED_THREADS)
 template <typename T, class MAP>
 __global__ void __launch_bounds__(RED_THREADS)
     k_update(int64_t nL, MAP map, Weights wt, T *__restrict__ x, const T *__restrict__ w,
-             T *__restrict__ r, const T *__restrict__ q, const T *__restrict__ dinv,
+             T *__restrict__ r, const T *__restrict__ q, const float *__restrict__ dinv,
              double *__restrict__ hist, double *__restrict__ ab, int nab, double *scal,
              double *partials, unsigned int *counter) {
   __shared__ double sh[32];
@@ -534,7 +535,7 @@ __global__ void __launch_bounds__(RED_THREADS)
     x[c] = x[c] + alpha * w[c];
     const T rc = r[c] + (-alpha) * q[c];
     r[c] = rc;
-    const T zc = dinv ? dinv[c] * rc : rc;
+    const T zc = dinv ? (T)dinv[c] * rc : rc;
     rho += (double)rc * (double)zc;
     const double t = norm_term_L(normtype, (double)rc, wt, c);
     rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
@@ -570,12 +571,12 @@ __global__ void __launch_bounds__(RED_THREADS)
 // 4. w = beta w + Dinv r
 template <typename T>
 __global__ void k_wupdate(int64_t nL, T *__restrict__ w, const T *__restrict__ r,
-                          const T *__restrict__ dinv, const double *scal) {
+                          const float *__restrict__ dinv, const double *scal) {
   if (scal[S_DONE] != 0.0) return;
   const T beta = (T)scal[S_BETA];
   GRID_STRIDE(c, nL) {
     const T rc = r[c];
-    const T zc = dinv ? dinv[c] * rc : rc;
+    const T zc = dinv ? (T)dinv[c] * rc : rc;
     w[c] = beta * w[c] + T(1) * zc;
   }
 }
@@ -784,6 +785,24 @@ struct Solver {
   double *ab = nullptr;  // alpha, beta of the first nab iterations (Lanczos)
   int nab = 0;
 
+  // Grid of a grid-stride reduction kernel: the blocks that are resident at
+  // once (occupancy x SMs, cached per kernel), so every block runs in the
+  // first wave; capped by gRed (work and partial-sum slots).
+  template <class K>
+  unsigned rgrid(K kern) {
+    static std::unordered_map<const void *, int> occ;
+    auto it = occ.find((const void *)kern);
+    int nb = 0;
+    if (it == occ.end()) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, RED_THREADS, 0) != cudaSuccess)
+        nb = 1;
+      occ[(const void *)kern] = nb;
+    } else {
+      nb = it->second;
+    }
+    return std::max(1u, std::min(gRed, (unsigned)(std::max(nb, 1) * ctx->sm_count)));
+  }
+
   Solver(gf_problem *p, MAP m, bool masked)
       : prob(p), ctx(p->ctx), st(p->ctx->stream), map(m), nE(p->nlocal), nL(p->nclass) {
     wt.maskL = masked ? p->maskL8 : nullptr;
@@ -831,16 +850,16 @@ struct Solver {
 
   template <typename T>
   void enqueue(int k, double p, double q, int use_mass, T *x, T *r, T *w, T *qL, T *qE,
-               const T *dinv, double *hist) {
+               const float *dinv, double *hist) {
     double *scal = prob->scal_d;
     for (int i = 0; i < k; i++) {
       if (std::is_same<T, float>::value && mixed_apply && prob->dim == 3)
         launch_helm_L_f32io(prob, p, q, use_mass, (const float *)w, (float *)qE, st, scal + S_DONE);
       else
         launch_helm_L<T>(prob, (T)p, (T)q, use_mass, w, qE, st, scal + S_DONE);
-      k_asm_dot<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, qE, w, qL, scal, prob->partials,
+      k_asm_dot<T, MAP><<<rgrid(k_asm_dot<T, MAP>), RED_THREADS, 0, st>>>(nL, map, wt, qE, w, qL, scal, prob->partials,
                                                       prob->counter);
-      k_update<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, x, w, r, qL, dinv, hist, ab,
+      k_update<T, MAP><<<rgrid(k_update<T, MAP>), RED_THREADS, 0, st>>>(nL, map, wt, x, w, r, qL, dinv, hist, ab,
                                                      nab, scal, prob->partials, prob->counter);
       k_wupdate<T><<<gL, 256, 0, st>>>(nL, w, r, dinv, scal);
       prob->launches += 3;
@@ -862,11 +881,11 @@ struct Solver {
   void precondition(const Poly &P, double p, double q, int use_mass, const double *rL) {
     double *scal = prob->scal_d;
     prob->launches += 1 + P.m;  // the applies count themselves
-    k_cheb_init<<<gRed, RED_THREADS, 0, st>>>(nL, rL, P.dinv, P.c0, P.res, P.d, P.z, P.m == 0,
+    k_cheb_init<<<rgrid(k_cheb_init), RED_THREADS, 0, st>>>(nL, rL, P.dinv, P.c0, P.res, P.d, P.z, P.m == 0,
                                               P.qL, scal, prob->partials, prob->counter);
     for (int j = 1; j <= P.m; j++) {
       launch_helm_L<float>(prob, (float)p, (float)q, use_mass, P.d, P.qE32, st, scal + S_DONE);
-      k_cheb_step<MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, P.qE32, P.dinv, P.c1[j], P.c2[j],
+      k_cheb_step<MAP><<<rgrid(k_cheb_step<MAP>), RED_THREADS, 0, st>>>(nL, map, wt, P.qE32, P.dinv, P.c1[j], P.c2[j],
                                                      P.res, P.d, P.z, j == P.m, rL, P.qL, scal,
                                                      prob->partials, prob->counter);
     }
@@ -877,9 +896,9 @@ struct Solver {
     double *scal = prob->scal_d;
     for (int i = 0; i < k; i++) {
       launch_helm_L<double>(prob, p, q, use_mass, P.w, qE, st, scal + S_DONE);
-      k_asm_dot<double, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, qE, P.w, P.qL, scal,
+      k_asm_dot<double, MAP><<<rgrid(k_asm_dot<double, MAP>), RED_THREADS, 0, st>>>(nL, map, wt, qE, P.w, P.qL, scal,
                                                            prob->partials, prob->counter);
-      k_update<double, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, x, P.w, r, P.qL, nullptr,
+      k_update<double, MAP><<<rgrid(k_update<double, MAP>), RED_THREADS, 0, st>>>(nL, map, wt, x, P.w, r, P.qL, nullptr,
                                                           hist, nullptr, 0, scal, prob->partials,
                                                           prob->counter);
       precondition(P, p, q, use_mass, r);
@@ -910,12 +929,12 @@ struct Solver {
     double *abd = (double *)gf_work(prob, 17, sizeof(double) * 2 * LANCZOS);
     if (!P.w || !P.qL || !P.res || !P.d || !P.z || !P.qE32 || !abd)
       return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
-    int rc = residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, P.w, d64, 0, tr.tol);
+    int rc = residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, P.w, d32, 0, tr.tol);
     if (rc) return gf_fail(ctx, rc, "residual failed");
     const int n0 = std::min(tr.maxit, LANCZOS);
     ab = abd;
     nab = n0;
-    rc = iterate<double>(tr, n0, p, q, use_mass, xL, rL, P.w, P.qL, qE, d64, hist, total);
+    rc = iterate<double>(tr, n0, p, q, use_mass, xL, rL, P.w, P.qL, qE, d32, hist, total);
     ab = nullptr;
     nab = 0;
     if (rc) return rc;
@@ -958,7 +977,7 @@ struct Solver {
   // (rho, rtol, done) was set up by k_resid.  Returns iterations done.
   template <typename T>
   int iterate(const gf_cg_traits &tr, int maxit, double p, double q, int use_mass, T *x, T *r, T *w,
-              T *qL, T *qE, const T *dinv, double *hist, int *iters) {
+              T *qL, T *qE, const float *dinv, double *hist, int *iters) {
     return batches(tr, maxit, iters, [&](int k) {
       enqueue<T>(k, p, q, use_mass, x, r, w, qL, qE, dinv, hist);
     });
@@ -1014,11 +1033,11 @@ struct Solver {
   // precision copies rT, wT = Dinv rT and sets up the CG state.
   template <typename T>
   int residual(double p, double q, int use_mass, const double *bL, const double *xL, double *qE,
-               double *rL, T *rT, T *wT, const T *dinv, int mode, double tol) {
+               double *rL, T *rT, T *wT, const float *dinv, int mode, double tol) {
     int rc = launch_helm_L<double>(prob, p, q, use_mass, xL, qE, st);
     if (rc) return rc;
     prob->launches++;
-    k_resid<T, MAP><<<gRed, RED_THREADS, 0, st>>>(nL, map, wt, bL, qE, rL, rT, wT, dinv, mode, tol,
+    k_resid<T, MAP><<<rgrid(k_resid<T, MAP>), RED_THREADS, 0, st>>>(nL, map, wt, bL, qE, rL, rT, wT, dinv, mode, tol,
                                                   prob->scal_d, prob->partials, prob->counter);
     GF_CHECK_LAUNCH(ctx);
     return GF_OK;
@@ -1065,9 +1084,9 @@ struct Solver {
       double *w = (double *)gf_work(prob, 4, sizeof(double) * nL);
       double *qL = (double *)gf_work(prob, 5, sizeof(double) * nL);
       if (!w || !qL) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
-      rc = residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, w, d64, 0, tr.tol);
+      rc = residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, w, d32, 0, tr.tol);
       if (rc) return gf_fail(ctx, rc, "residual failed");
-      rc = iterate<double>(tr, tr.maxit, p, q, use_mass, xL, rL, w, qL, qE, d64, hist, &total);
+      rc = iterate<double>(tr, tr.maxit, p, q, use_mass, xL, rL, w, qL, qE, d32, hist, &total);
       if (rc) return rc;
       rn = prob->scal_h[S_RNORM];
       rc = (total >= tr.maxit && rn > tr.tol) ? GF_CG_NOCONVERGE : GF_OK;
