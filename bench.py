@@ -75,7 +75,7 @@ def parse():
                     help="FP32 applies per Chebyshev preconditioner application")
     ap.add_argument("--poly-ratio", type=float, default=0.0,
                     help="b/a of the Chebyshev interval (0: library default)")
-    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply"], default=None,
+    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply", "adjoint"], default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
 
@@ -465,6 +465,9 @@ def main():
     tr_cheb = CGTraits(precision=A.GF_CG_MIXED, check_every=4, poly_degree=args.poly,
                        poly_ratio=args.poly_ratio,
                        **dict(common, precond=A.GF_PRECOND_CHEBYSHEV))
+    if args.only == "adjoint":
+        print(json.dumps({"only": "adjoint", "adjoint": adjoint_bench(ctx)}), flush=True)
+        return
     if args.only == "apply":
         roof = kernel_roofline(ctx, prob, measured_peaks(), reps=args.steps)
         print(json.dumps({"only": "apply", "helm3d": roof}), flush=True)

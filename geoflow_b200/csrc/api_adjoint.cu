@@ -121,11 +121,147 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// 3-d VJP, line-based like k_dudt3d: EPB elements per block, thread
+// (a0, a1) of an element owns the x-line (j=a0, k=a1), the y-line
+// (i=a0, k=a1) and the z-line (i=a0, j=a1).  Per evolved component m the
+// x/y owners contract their lines (D, flux, D^T) into shared memory, the
+// z-owner keeps its line in registers and sums the three.  The Burgers
+// term of component m, X_m M sum_k (D_m u_k) mu_k, is formed by the owners
+// of direction-m lines.
+template <int N> constexpr int epb_vjp3() { return (160 / (N * N)) < 1 ? 1 : 160 / (N * N); }
+
+template <int N, int EPB, int EQN>
+__global__ void __launch_bounds__(N *N *EPB)
+    k_dudt_vjp3d(const __grid_constant__ Basis<double, N> B, const Geom<double> g, int64_t ne,
+                 double nu, const double *__restrict__ c0, const double *__restrict__ c1,
+                 const double *__restrict__ c2, const double *__restrict__ l0,
+                 const double *__restrict__ l1, const double *__restrict__ l2,
+                 const double *__restrict__ imass, double *__restrict__ o0,
+                 double *__restrict__ o1, double *__restrict__ o2) {
+  constexpr int NC = EQN == GF_EQN_BURGERS ? 3 : 1;  // evolved components
+  constexpr int NV = EQN == GF_EQN_HEAT ? 0 : 3;     // advecting velocities
+  constexpr int P = Pad<N>::P, PLANE = N * P, VOL = N * PLANE, NN = N * N, NNN = NN * N;
+  constexpr int NF = NV + NC + 2;
+  extern __shared__ __align__(16) double smv[];
+  double *sc = smv + threadIdx.y * NF * VOL;  // NV velocity fields
+  double *smu = sc + NV * VOL;                // NC fields mu = Minv lam
+  double *sx = smu + NC * VOL, *sy = sx + VOL;
+  const int t = threadIdx.x;
+  const int64_t e = (int64_t)blockIdx.x * EPB + threadIdx.y;
+  const bool active = e < ne;
+  const int a0 = t % N, a1 = t / N;
+  const int64_t base = e * NNN;
+  const double *cin[3] = {c0, c1, c2};
+  const double *lin[3] = {l0, l1, l2};
+  double *outp[3] = {o0, o1, o2};
+  NodeGeom<double, 3> eg;
+  eg.X[0] = eg.X[1] = eg.X[2] = eg.J = 0.0;
+  if (active) elem_geom<double, 3>(g, e, eg);
+  // geometry and mass at local node (i, j, k)
+  auto geo = [&](int i, int j, int k, NodeGeom<double, 3> &ng) {
+    ng = eg;
+    if (active) node_geom<double, 3>(g, base + k * NN + j * N + i, ng);
+    return B.W[k] * B.W[j] * B.W[i] * ng.J;
+  };
+#pragma unroll 1
+  for (int k = 0; k < N; k++) {
+    const int64_t node = base + k * NN + a1 * N + a0;
+    const int si = k * PLANE + a1 * P + a0;
+    for (int v = 0; v < NV; v++) sc[v * VOL + si] = active ? cin[v][node] : 0.0;
+    const double im = active ? imass[node] : 0.0;
+    for (int m = 0; m < NC; m++) smu[m * VOL + si] = active ? im * lin[m][node] : 0.0;
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int m = 0; m < NC; m++) {
+    const double *mu = smu + m * VOL;
+    // the direction-dd line starting at shared offset base_s (node stride
+    // `stride`, local index ijk[slot] running along it): D, flux, D^T, plus
+    // the Burgers term when dd == m; written to dst (x/y) or kept in res
+    auto line = [&](int dd, int base_s, int stride, int (&ijk)[3], int slot, double *dst,
+                    double (&res)[N]) {
+      double a[N], d[N], s[N];
+#pragma unroll
+      for (int q = 0; q < N; q++) a[q] = mu[base_s + q * stride];
+      line_D<double, N>(B.D, a, d);
+      double bt[N];
+#pragma unroll
+      for (int q = 0; q < N; q++) bt[q] = 0.0;
+      if (EQN == GF_EQN_BURGERS && dd == m) {
+        // sum_k (D_dd u_k) mu_k along the line
+#pragma unroll 1
+        for (int kk = 0; kk < 3; kk++) {
+          double uu[N], du[N];
+#pragma unroll
+          for (int q = 0; q < N; q++) uu[q] = sc[kk * VOL + base_s + q * stride];
+          line_D<double, N>(B.D, uu, du);
+#pragma unroll
+          for (int q = 0; q < N; q++) bt[q] = fma(du[q], smu[kk * VOL + base_s + q * stride], bt[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < N; q++) {
+        ijk[slot] = q;
+        NodeGeom<double, 3> ng;
+        const double M = geo(ijk[0], ijk[1], ijk[2], ng);
+        const double X = ng.X[dd];
+        double sv = nu * (M * ((X * X) * d[q]));
+        if (NV) sv += X * sc[dd * VOL + base_s + q * stride] * M * a[q];
+        s[q] = sv;
+        bt[q] *= X * M;
+      }
+      line_DT<double, N>(B.D, s, res);
+#pragma unroll
+      for (int q = 0; q < N; q++) res[q] += bt[q];
+      if (dst) {
+#pragma unroll
+        for (int q = 0; q < N; q++) dst[base_s + q * stride] = res[q];
+      }
+    };
+    {
+      int ijk[3] = {0, a0, a1}, slot = 0;  // x-line (j=a0, k=a1)
+      double r[N];
+      line(0, a1 * PLANE + a0 * P, 1, ijk, slot, sx, r);
+    }
+    {
+      int ijk[3] = {a0, 0, a1}, slot = 1;  // y-line (i=a0, k=a1)
+      double r[N];
+      line(1, a1 * PLANE + a0, P, ijk, slot, sy, r);
+    }
+    double rz[N];
+    {
+      int ijk[3] = {a0, a1, 0}, slot = 2;  // z-line (i=a0, j=a1), registers
+      line(2, a1 * P + a0, PLANE, ijk, slot, nullptr, rz);
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        const int si = k * PLANE + a1 * P + a0;
+        outp[m][base + k * NN + a1 * N + a0] = -((sx[si] + sy[si]) + rz[k]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int N, int DIM, int EQN>
 int launch_vjp_n(gf_problem *prob, double nu, const double *const *c, const double *const *lam,
                  double *const *out, cudaStream_t st) {
   const Basis<double, N> B = make_basis<double, N>(prob);
   const Geom<double> g = geom_of<double>(prob);
+  if (DIM == 3) {
+    constexpr int EPB = epb_vjp3<N>();
+    constexpr int NF = (EQN == GF_EQN_HEAT ? 0 : 3) + (EQN == GF_EQN_BURGERS ? 3 : 1) + 2;
+    const size_t smem = sizeof(double) * NF * N * N * Pad<N>::P * EPB;
+    auto kern = k_dudt_vjp3d<N, EPB, EQN>;
+    set_smem(kern, smem);
+    prob->launches++;
+    kern<<<(unsigned)((prob->ne + EPB - 1) / EPB), dim3(N * N, EPB), smem, st>>>(
+        B, g, prob->ne, nu, c[0], c[1], c[2], lam[0], lam[1], lam[2], prob->imass_d, out[0],
+        out[1], out[2]);
+    return cudaPeekAtLastError() == cudaSuccess ? GF_OK : GF_ERR_CUDA;
+  }
   constexpr int NE = DIM == 3 ? N * N * N : N * N;
   constexpr int NC = EQN == GF_EQN_BURGERS ? DIM : 1;
   constexpr int NV = EQN == GF_EQN_HEAT ? 0 : DIM;
