@@ -26,7 +26,7 @@ GF_DSS_SUM, GF_DSS_SMOOTH, GF_DSS_MAX, GF_DSS_MIN = 0, 1, 2, 3
 GF_NORM_INF, GF_NORM_EUC, GF_NORM_L2, GF_NORM_L1 = 0, 1, 2, 3
 GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV = 0, 1, 2
 GF_CG_FP64, GF_CG_MIXED = 0, 1
-GF_GEOM_AFFINE, GF_GEOM_REGULAR = 0, 1
+GF_GEOM_AFFINE, GF_GEOM_REGULAR, GF_GEOM_DEFORMED, GF_GEOM_EMBEDDED = 0, 1, 2, 3
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
 GF_RK1, GF_RK2, GF_RK3, GF_RK4, GF_SSP22, GF_SSP33, GF_SSP34 = 1, 2, 3, 4, 22, 33, 34
 # gf_integrate_noalloc: fixed scratch of GF_NOALLOC_MAX_BLOCKS blocks of GF_NOALLOC_CHUNK
@@ -40,7 +40,7 @@ class ProblemDesc(C.Structure):
         ("D", P_double), ("W", P_double), ("geom", c_int),
         ("elem_geom", P_double), ("node_geom", P_double), ("mask", P_double),
         ("nclass", c_int64), ("class_ptr", P_int32), ("members", P_int32),
-        ("box_ne", c_int * 3), ("box_periodic", c_int * 3),
+        ("box_ne", c_int * 3), ("box_periodic", c_int * 3), ("node_xyz", P_double),
     ]
 
 
@@ -96,6 +96,7 @@ SIGNATURES = {
     "gf_rk_advance_host": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
                                    c_double, c_int]),
     "gf_integrate_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "gf_constrain2sphere": (c_int, [c_void_p, c_int, P_void, P_void]),
     "gf_dudt_vjp": (c_int, [c_void_p, c_int, c_int, c_double, c_int, P_void, P_void, P_void,
                             P_void]),
     "gf_dss_T": (c_int, [c_void_p, c_int, c_int, c_void_p]),

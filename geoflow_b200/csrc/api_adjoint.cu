@@ -525,6 +525,8 @@ extern "C" int gf_dudt_vjp(gf_problem_t prob, int dtype, int eqn, double nu, int
                            void *const *ubar) {
   if (!prob) return GF_ERR_ARG;
   gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, prob->geom <= GF_GEOM_REGULAR,
+             "the adjoint path covers affine and regular (diagonal-metric) grids");
   GF_REQUIRE(ctx, dtype == GF_F64, "the adjoint path is FP64");
   GF_REQUIRE(ctx, eqn == GF_EQN_ADVECT || eqn == GF_EQN_BURGERS || eqn == GF_EQN_HEAT,
              "unknown equation %d", eqn);
@@ -546,6 +548,8 @@ extern "C" int gf_rk_step_vjp(gf_problem_t prob, int dtype, const gf_rk_traits *
                               void *const *lam) {
   if (!prob) return GF_ERR_ARG;
   gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, prob->geom <= GF_GEOM_REGULAR,
+             "the adjoint path covers affine and regular (diagonal-metric) grids");
   GF_REQUIRE(ctx, dtype == GF_F64, "the adjoint path is FP64");
   int rc = gfrk::check_traits(prob, traits, u0, c);
   if (rc) return rc;
@@ -576,6 +580,8 @@ extern "C" int gf_adjoint_gradient(gf_problem_t prob, const gf_rk_traits *traits
                                    int checkpoint_every, double *J, double *const *grad) {
   if (!prob) return GF_ERR_ARG;
   gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, prob->geom <= GF_GEOM_REGULAR,
+             "the adjoint path covers affine and regular (diagonal-metric) grids");
   int rc = gfrk::check_traits(prob, traits, (const void *const *)u0, (const void *const *)c);
   if (rc) return rc;
   GF_REQUIRE(ctx, u_obs && grad && nsteps >= 0 && checkpoint_every >= 1, "bad arguments");

@@ -689,9 +689,13 @@ __global__ void k_fcg_w(int64_t nL, double *__restrict__ w, const float *__restr
 }
 
 // local diagonal of p L + q M at every element-local node
+// gmet (deformed / embedded elements): packed G_ij with W and Jac; the
+// diagonal is then sum_i sum_m D(m,l_i)^2 G_ii(line node m) plus, for
+// i != j, D(l_i,l_i) D(l_j,l_j) G_ij at the node itself.
 __global__ void k_helm_diag(int64_t n, int dim, int nb, Basis<double, GF_MAXN> B,
                             const double *__restrict__ egeom, const double *__restrict__ ngeom,
-                            double p, double q, int use_mass, double *__restrict__ diag) {
+                            const double *__restrict__ gmet, double p, double q, int use_mass,
+                            double *__restrict__ diag) {
   const int nn = dim == 2 ? nb * nb : nb * nb * nb;
   GRID_STRIDE(i, n) {
     const int64_t e = i / nn;
@@ -703,6 +707,10 @@ __global__ void k_helm_diag(int64_t n, int dim, int nb, Basis<double, GF_MAXN> B
       for (int m = 0; m < nb; m++) {
         const double Dm = B.D[m + li[d] * nb];
         const int64_t gb = i + (int64_t)(m - li[d]) * stride[d];
+        if (gmet) {
+          s += Dm * Dm * gmet[(int64_t)gpack(d, d, dim) * n + gb];
+          continue;
+        }
         const int b = (int)(gb % nn);
         const int bi = b % nb, bj = (b / nb) % nb, bk = b / (nb * nb);
         double X, J;
@@ -717,6 +725,12 @@ __global__ void k_helm_diag(int64_t n, int dim, int nb, Basis<double, GF_MAXN> B
         s += Dm * Dm * (X * X) * (w * J);
       }
     }
+    if (gmet)
+      for (int a1 = 0; a1 < dim; a1++)
+        for (int a2 = 0; a2 < dim; a2++)
+          if (a1 != a2)
+            s += B.D[li[a1] + li[a1] * nb] * B.D[li[a2] + li[a2] * nb] *
+                 gmet[(int64_t)gpack(a1, a2, dim) * n + i];
     s *= p;
     if (use_mass) {
       const double J = egeom ? egeom[e * (dim + 1) + dim] : ngeom[(int64_t)dim * n + i];
@@ -835,8 +849,8 @@ struct Solver {
     for (int i = 0; i < prob->n * prob->n; i++) B.D[i] = prob->D[i];
     for (int i = 0; i < prob->n; i++) B.W[i] = prob->W[i];
     prob->launches += 3;
-    k_helm_diag<<<gE, 256, 0, st>>>(nE, prob->dim, prob->n, B, prob->egeom_d, prob->ngeom_d, p, q,
-                                    use_mass, dE);
+    k_helm_diag<<<gE, 256, 0, st>>>(nE, prob->dim, prob->n, B, prob->egeom_d, prob->ngeom_d,
+                                    prob->gmet_d, p, q, use_mass, dE);
     k_assemble<MAP, double><<<gL, 256, 0, st>>>(nL, map, dE, dL);
     k_invert<<<gL, 256, 0, st>>>(nL, dL, iL, fL);
     *d64 = iL;

@@ -154,10 +154,26 @@ extern "C" int gf_grefderiv(gf_problem_t prob, int dtype, const void *u, int idi
 extern "C" int gf_deriv(gf_problem_t prob, int dtype, const void *u, int idir, void *du) {
   if (!prob) return GF_ERR_ARG;
   gf_context *ctx = prob->ctx;
-  GF_REQUIRE(ctx, u && du && idir >= 1 && idir <= prob->dim, "bad arguments");
-  int rc = dtype == GF_F64
-               ? deriv_common<double>(prob, (const double *)u, idir, 0, 1, 0, (double *)du)
-               : deriv_common<float>(prob, (const float *)u, idir, 0, 1, 0, (float *)du);
+  const int nphys = prob->nxy ? prob->nxy : prob->dim;
+  GF_REQUIRE(ctx, u && du && idir >= 1 && idir <= nphys, "bad arguments");
+  int rc;
+  if (prob->geom >= GF_GEOM_DEFORMED) {  // sum_j dXi_j/dX_idir D_j u
+    rc = dtype == GF_F64
+             ? dispatch_n<DefLaunch<double, LoadE<double>>::template F>(
+                   prob->n, prob, (int)DEF_DERIV, 0.0, (const double *)nullptr, 0.0,
+                   (const double *)nullptr, 0, LoadE<double>{(const double *)u}, 0,
+                   (const double *const *)nullptr, idir, (double *)du, ctx->stream,
+                   (const double *)nullptr)
+             : dispatch_n<DefLaunch<float, LoadE<float>>::template F>(
+                   prob->n, prob, (int)DEF_DERIV, 0.0f, (const float *)nullptr, 0.0f,
+                   (const float *)nullptr, 0, LoadE<float>{(const float *)u}, 0,
+                   (const float *const *)nullptr, idir, (float *)du, ctx->stream,
+                   (const double *)nullptr);
+  } else {
+    rc = dtype == GF_F64
+             ? deriv_common<double>(prob, (const double *)u, idir, 0, 1, 0, (double *)du)
+             : deriv_common<float>(prob, (const float *)u, idir, 0, 1, 0, (float *)du);
+  }
   if (rc) return gf_fail(ctx, rc, "deriv launch failed");
   GF_CHECK_LAUNCH(ctx);
   return GF_OK;
@@ -183,9 +199,37 @@ extern "C" int gf_grefdiv(gf_problem_t prob, int dtype, const void *const *u, in
 // ---------------------------------------------------------------------
 // advection and Burgers RHS
 // ---------------------------------------------------------------------
+// Deformed / embedded elements: one k_def launch per evolved component,
+// the reference gradient shared by advection and diffusion.  f as for
+// launch_dudt: ADVECT {p, c0, c1, c2}, BURGERS {u0, u1, u2}, HEAT {u}.
+template <typename T>
+static int launch_def_dudt(gf_problem *prob, int eqn, int mode, T nu, const T *const *f,
+                           T *const *o, cudaStream_t st) {
+  const int nv = prob->nxy;
+  if (eqn == GF_EQN_ADVECT) {
+    const T *c[3] = {f[1], f[2], f[3]};
+    return dispatch_n<DefLaunch<T, LoadE<T>>::template F>(
+        prob->n, prob, mode == MODE_ADVECT ? (int)DEF_ADVECT : (int)DEF_DUDT, nu, (const T *)nullptr,
+        T(0), (const T *)nullptr, 0, LoadE<T>{f[0]}, nv, (const T *const *)c, 0, o[0], st,
+        (const double *)nullptr);
+  }
+  if (eqn == GF_EQN_HEAT)
+    return dispatch_n<DefLaunch<T, LoadE<T>>::template F>(
+        prob->n, prob, (int)DEF_DUDT, nu, (const T *)nullptr, T(0), (const T *)nullptr, 0,
+        LoadE<T>{f[0]}, 0, (const T *const *)nullptr, 0, o[0], st, (const double *)nullptr);
+  for (int k = 0; k < nv; k++) {  // Burgers: the velocity is the state
+    int rc = dispatch_n<DefLaunch<T, LoadE<T>>::template F>(
+        prob->n, prob, (int)DEF_DUDT, nu, (const T *)nullptr, T(0), (const T *)nullptr, 0,
+        LoadE<T>{f[k]}, nv, f, 0, o[k], st, (const double *)nullptr);
+    if (rc) return rc;
+  }
+  return GF_OK;
+}
+
 template <typename T>
 int launch_dudt(gf_problem *prob, int eqn, int mode, T nu, const T *const *f, T *const *o,
                 cudaStream_t st) {
+  if (prob->geom >= GF_GEOM_DEFORMED) return launch_def_dudt<T>(prob, eqn, mode, nu, f, o, st);
   return dispatch_n<DudtLaunch<T>::template F>(prob->n, prob, eqn, mode, nu, f, o, st);
 }
 template int launch_dudt<double>(gf_problem *, int, int, double, const double *const *,
@@ -197,17 +241,19 @@ extern "C" int gf_advect_apply(gf_problem_t prob, int dtype, const void *p, int 
                                const void *const *c, void *po) {
   if (!prob) return GF_ERR_ARG;
   gf_context *ctx = prob->ctx;
-  GF_REQUIRE(ctx, p && c && po && ncomp == prob->dim, "advect needs p, dim velocity components, po");
+  const int nvel = prob->nxy ? prob->nxy : prob->dim;
+  GF_REQUIRE(ctx, p && c && po && ncomp == nvel,
+             "advect needs p, %d velocity components (one per physical coordinate), po", nvel);
   for (int k = 0; k < ncomp; k++) GF_REQUIRE(ctx, c[k], "velocity component %d missing", k);
   int rc;
   if (dtype == GF_F64) {
     const double *f[4] = {(const double *)p, (const double *)c[0], (const double *)c[1],
-                          prob->dim > 2 ? (const double *)c[2] : nullptr};
+                          ncomp > 2 ? (const double *)c[2] : nullptr};
     double *o[3] = {(double *)po, nullptr, nullptr};
     rc = launch_dudt<double>(prob, GF_EQN_ADVECT, MODE_ADVECT, 1.0, f, o, ctx->stream);
   } else {
     const float *f[4] = {(const float *)p, (const float *)c[0], (const float *)c[1],
-                         prob->dim > 2 ? (const float *)c[2] : nullptr};
+                         ncomp > 2 ? (const float *)c[2] : nullptr};
     float *o[3] = {(float *)po, nullptr, nullptr};
     rc = launch_dudt<float>(prob, GF_EQN_ADVECT, MODE_ADVECT, 1.0f, f, o, ctx->stream);
   }
@@ -221,10 +267,12 @@ extern "C" int gf_dudt(gf_problem_t prob, int dtype, int eqn, double nu, int nst
   if (!prob) return GF_ERR_ARG;
   gf_context *ctx = prob->ctx;
   GF_REQUIRE(ctx, u && dudt, "u and dudt are required");
+  // velocity components: one per physical coordinate (3 on an embedded surface)
+  const int nvel = prob->nxy ? prob->nxy : prob->dim;
   GF_REQUIRE(ctx, eqn == GF_EQN_ADVECT || eqn == GF_EQN_BURGERS || eqn == GF_EQN_HEAT,
              "unknown equation %d", eqn);
   if (eqn == GF_EQN_BURGERS) {
-    GF_REQUIRE(ctx, nstate == prob->dim, "Burgers evolves dim components");
+    GF_REQUIRE(ctx, nstate == nvel, "Burgers evolves one component per physical coordinate");
   } else if (eqn == GF_EQN_HEAT) {
     // heat evolves each component independently
     for (int k = 0; k < nstate; k++) {
@@ -248,10 +296,10 @@ extern "C" int gf_dudt(gf_problem_t prob, int dtype, int eqn, double nu, int nst
     double *o[3] = {nullptr, nullptr, nullptr};
     if (eqn == GF_EQN_ADVECT) {
       f[0] = (const double *)u[0];
-      for (int k = 0; k < prob->dim; k++) f[1 + k] = (const double *)c[k];
+      for (int k = 0; k < nvel; k++) f[1 + k] = (const double *)c[k];
       o[0] = (double *)dudt[0];
     } else {
-      for (int k = 0; k < prob->dim; k++) {
+      for (int k = 0; k < nvel; k++) {
         f[k] = (const double *)u[k];
         o[k] = (double *)dudt[k];
       }
@@ -262,10 +310,10 @@ extern "C" int gf_dudt(gf_problem_t prob, int dtype, int eqn, double nu, int nst
     float *o[3] = {nullptr, nullptr, nullptr};
     if (eqn == GF_EQN_ADVECT) {
       f[0] = (const float *)u[0];
-      for (int k = 0; k < prob->dim; k++) f[1 + k] = (const float *)c[k];
+      for (int k = 0; k < nvel; k++) f[1 + k] = (const float *)c[k];
       o[0] = (float *)dudt[0];
     } else {
-      for (int k = 0; k < prob->dim; k++) {
+      for (int k = 0; k < nvel; k++) {
         f[k] = (const float *)u[k];
         o[k] = (float *)dudt[k];
       }
@@ -364,5 +412,30 @@ extern "C" int gf_integrate(gf_problem_t prob, int dtype, const void *u, double 
   GF_CHECK_LAUNCH(ctx);
   GF_CUDA(ctx, cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   GF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GF_OK;
+}
+
+// ---------------------------------------------------------------------
+// GMTK::constrain2sphere (2) (blas/gmtk.ipp:2957-2976)
+// ---------------------------------------------------------------------
+extern "C" int gf_constrain2sphere(gf_problem_t prob, int dtype, void *const *v,
+                                   const void *const *xyz) {
+  if (!prob) return GF_ERR_ARG;
+  gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, v && xyz, "v and xyz are required");
+  for (int k = 0; k < 3; k++) GF_REQUIRE(ctx, v[k] && xyz[k], "component %d missing", k);
+  GF_REQUIRE(ctx, dtype == GF_F64 || dtype == GF_F32, "unknown dtype %d", dtype);
+  if (prob->geom != GF_GEOM_EMBEDDED) return GF_OK;  // as the reference: only on 2-d surfaces
+  const unsigned g = grid_for(prob->nlocal, 256, ctx->sm_count * 8);
+  prob->launches++;
+  if (dtype == GF_F64)
+    k_constrain2sphere<double><<<g, 256, 0, ctx->stream>>>(
+        prob->nlocal, (double *)v[0], (double *)v[1], (double *)v[2], (const double *)xyz[0],
+        (const double *)xyz[1], (const double *)xyz[2]);
+  else
+    k_constrain2sphere<float><<<g, 256, 0, ctx->stream>>>(
+        prob->nlocal, (float *)v[0], (float *)v[1], (float *)v[2], (const float *)xyz[0],
+        (const float *)xyz[1], (const float *)xyz[2]);
+  GF_CHECK_LAUNCH(ctx);
   return GF_OK;
 }

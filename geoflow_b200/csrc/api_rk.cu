@@ -101,7 +101,7 @@ int Stepper<T>::rhs(T *const *u, T *const *K) {
   T *o[3] = {nullptr, nullptr, nullptr};
   if (eqn == GF_EQN_ADVECT) {
     f[0] = u[0];
-    for (int k = 0; k < prob->dim; k++) f[1 + k] = c[k];
+    for (int k = 0; k < gf_nvel(prob); k++) f[1 + k] = c[k];
     o[0] = K[0];
     return launch_dudt<T>(prob, eqn, 0, nu, f, o, st);
   }
@@ -114,7 +114,7 @@ int Stepper<T>::rhs(T *const *u, T *const *K) {
     }
     return GF_OK;
   }
-  for (int k = 0; k < prob->dim; k++) {
+  for (int k = 0; k < gf_nvel(prob); k++) {
     f[k] = u[k];
     o[k] = K[k];
   }
@@ -124,6 +124,15 @@ int Stepper<T>::rhs(T *const *u, T *const *K) {
 template <typename T>
 void Stepper<T>::smooth(T *v) {
   launch_dss<T>(prob, GF_DSS_SMOOTH, v, st);
+}
+
+template <typename T>
+void Stepper<T>::constrain(T *const *u) {
+  if (prob->geom != GF_GEOM_EMBEDDED || nstate < 3 || !prob->xyz_d) return;
+  const T *x = sizeof(T) == 8 ? (const T *)prob->xyz_d : (const T *)prob->xyz_f;
+  const unsigned g = grid_for(n, 256, prob->ctx->sm_count * 8);
+  prob->launches++;
+  k_constrain2sphere<T><<<g, 256, 0, st>>>(n, u[0], u[1], u[2], x, x + n, x + 2 * n);
 }
 
 template <typename T>
@@ -161,12 +170,14 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
                                           (T)beta[m][0] * h, (T)beta[m][1] * h,
                                           (T)beta[m][2] * h, um[k]);
       }
+      constrain(um);
       if ((rc = rhs(um, K[m]))) return rc;
       for (int k = 0; k < nstate; k++) {
         smooth(K[m][k]);
         prob->launches++;
         k_accum<T><<<g, 256, 0, st>>>(n, K[m][k], (T)cc[m] * h, uout[k]);
       }
+      constrain(uout);
     }
     T *const *uf = stage_in(ns - 1);
     for (int k = 0; k < nstate; k++) {
@@ -176,6 +187,7 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
                                         (T)beta[ns - 1][2] * h, uf[k]);
       smooth(uf[k]);
     }
+    constrain(uf);
     // the final stage result goes to the last K slot (K[0] in the
     // reference, whose earlier content is no longer needed)
     T *const *Kf = K[0];
@@ -186,6 +198,7 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
       k_accum<T><<<g, 256, 0, st>>>(n, Kf[k], (T)cc[ns - 1] * h, uout[k]);
       smooth(uout[k]);
     }
+    constrain(uout);
     return GF_OK;
   }
   // SSP stage inputs are uin and the substep results left in K[0..ns-2]
@@ -291,14 +304,15 @@ int check_traits(gf_problem *prob, const gf_rk_traits *tr, const void *const *u,
   GF_REQUIRE(ctx, (s >= 1 && s <= 4) || s == GF_SSP22 || s == GF_SSP33 || s == GF_SSP34,
              "unknown RK scheme %d", s);
   if (tr->eqn == GF_EQN_BURGERS)
-    GF_REQUIRE(ctx, tr->nstate == prob->dim, "Burgers evolves dim components");
+    GF_REQUIRE(ctx, tr->nstate == gf_nvel(prob),
+               "Burgers evolves one component per physical coordinate");
   else if (tr->eqn == GF_EQN_ADVECT)
     GF_REQUIRE(ctx, tr->nstate == 1 && c, "pure advection: one component and dim velocities");
   else
     GF_REQUIRE(ctx, tr->nstate >= 1 && tr->nstate <= 3, "heat: 1..3 components");
   for (int k = 0; k < tr->nstate; k++) GF_REQUIRE(ctx, u[k], "state component %d missing", k);
   if (tr->eqn == GF_EQN_ADVECT)
-    for (int k = 0; k < prob->dim; k++) GF_REQUIRE(ctx, c[k], "velocity component %d missing", k);
+    for (int k = 0; k < gf_nvel(prob); k++) GF_REQUIRE(ctx, c[k], "velocity component %d missing", k);
   return GF_OK;
 }
 
@@ -352,7 +366,7 @@ extern "C" int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_trai
     GF_CUDA(ctx, cudaMemcpyAsync(du[k], u[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
   }
   if (tr->eqn == GF_EQN_ADVECT) {
-    for (int k = 0; k < prob->dim; k++) {
+    for (int k = 0; k < gf_nvel(prob); k++) {
       void *d = gf_work(prob, 93 + k, bytes);
       if (!d) return gf_fail(ctx, GF_ERR_NOMEM, "staging allocation failed");
       GF_CUDA(ctx, cudaMemcpyAsync(d, c[k], bytes, cudaMemcpyHostToDevice, ctx->stream));

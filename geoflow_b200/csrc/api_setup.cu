@@ -427,7 +427,8 @@ extern "C" int gf_problem_destroy(gf_problem_t prob) {
                   prob->mask_f, prob->imass_d, prob->imass_f, prob->mass_d, prob->imult_d,
                   prob->imult_f, prob->class_ptr, prob->members, prob->node_class, prob->sh_ptr,
                   prob->sh_members, prob->scal_d, prob->partials, prob->counter,
-                  prob->massL, prob->maskL8, prob->multL8};
+                  prob->massL, prob->maskL8, prob->multL8, prob->dgeom_d, prob->dgeom_f,
+                  prob->gmet_d, prob->gmet_f, prob->xyz_d, prob->xyz_f};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (prob->scal_h) cudaFreeHost(prob->scal_h);
@@ -449,9 +450,10 @@ extern "C" int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *d, gf_prob
   GF_REQUIRE(ctx, d->n >= 2 && d->n <= GF_MAXN, "n must be in [2,%d] (got %d)", GF_MAXN, d->n);
   GF_REQUIRE(ctx, d->ne >= 1, "ne must be positive");
   GF_REQUIRE(ctx, d->D && d->W, "D and W are required");
-  GF_REQUIRE(ctx, d->geom == GF_GEOM_AFFINE || d->geom == GF_GEOM_REGULAR, "unknown geometry kind");
+  GF_REQUIRE(ctx, d->geom >= GF_GEOM_AFFINE && d->geom <= GF_GEOM_EMBEDDED, "unknown geometry kind");
   GF_REQUIRE(ctx, d->geom != GF_GEOM_AFFINE || d->elem_geom, "elem_geom required for AFFINE");
-  GF_REQUIRE(ctx, d->geom != GF_GEOM_REGULAR || d->node_geom, "node_geom required for REGULAR");
+  GF_REQUIRE(ctx, d->geom == GF_GEOM_AFFINE || d->node_geom, "node_geom required");
+  GF_REQUIRE(ctx, d->geom != GF_GEOM_EMBEDDED || d->dim == 2, "EMBEDDED grids are 2-d surfaces");
   GF_REQUIRE(ctx, d->class_ptr && d->members && d->nclass >= 1, "gather-scatter CSR required");
   GF_CUDA(ctx, cudaSetDevice(ctx->device));
   const int dim = d->dim, n = d->n;
@@ -496,11 +498,52 @@ extern "C" int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *d, gf_prob
     p->egeom_f = upload(to_f32(eg));
     for (int64_t e = 0; e < d->ne; e++)
       for (int64_t a = 0; a < nn; a++) jac[e * nn + a] = eg[e * (dim + 1) + dim];
-  } else {
+  } else if (d->geom == GF_GEOM_REGULAR) {
     std::vector<double> ng(d->node_geom, d->node_geom + (dim + 1) * N);
     p->ngeom_d = upload(ng);
     p->ngeom_f = upload(to_f32(ng));
     for (int64_t i = 0; i < N; i++) jac[i] = ng[dim * N + i];
+  } else {
+    // deformed / embedded: full dXi/dX, Jac, and the metric
+    // G_ij = sum_k X_ik X_jk W Jac (GHelmholtz::def_init, ghelmholtz.ipp:416-519,
+    // in its 2-d branch's order: each (i,j) accumulated once)
+    const int nxy = d->geom == GF_GEOM_EMBEDDED ? 3 : dim;
+    p->nxy = nxy;
+    const double *X = d->node_geom;
+    for (int64_t i = 0; i < N; i++) jac[i] = X[(int64_t)dim * nxy * N + i];
+    std::vector<double> xg(X, X + (int64_t)dim * nxy * N);
+    p->dgeom_d = upload(xg);
+    p->dgeom_f = upload(to_f32(xg));
+    std::vector<double> ng((dim + 1) * N, 0.0);  // zero diagonal planes, then Jac
+    for (int64_t i = 0; i < N; i++) ng[dim * N + i] = jac[i];
+    p->ngeom_d = upload(ng);
+    p->ngeom_f = upload(to_f32(ng));
+    const int npack = dim == 2 ? 3 : 6;
+    std::vector<double> gm((size_t)npack * N, 0.0);
+    const int pk3[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}}, pk2[3][3] = {{0, 1, 0}, {1, 2, 0}};
+    for (int64_t e = 0; e < d->ne; e++)
+      for (int64_t a = 0; a < nn; a++) {
+        const int64_t node = e * nn + a;
+        const int l = (int)(a % n), m = (int)((a / n) % n), pz = (int)(a / ((int64_t)n * n));
+        for (int j = 0; j < dim; j++)
+          for (int i = j; i < dim; i++) {
+            double s = 0.0;
+            for (int k = 0; k < nxy; k++) {
+              double t = X[((int64_t)i * nxy + k) * N + node] * X[((int64_t)j * nxy + k) * N + node] *
+                         d->W[l] * d->W[m];
+              if (dim > 2) t = t * d->W[pz];
+              s += t * jac[node];
+            }
+            gm[(size_t)(dim == 2 ? pk2[i][j] : pk3[i][j]) * N + node] = s;
+          }
+      }
+    p->gmet_d = upload(gm);
+    p->gmet_f = upload(to_f32(gm));
+  }
+  if (d->node_xyz) {
+    std::vector<double> xyz(d->node_xyz, d->node_xyz + 3 * N);
+    p->xyz_d = upload(xyz);
+    p->xyz_f = upload(to_f32(xyz));
   }
   // local mass W (x) W (x) W * Jac (gmass.ipp:134-220)
   std::vector<double> mass(N);

@@ -46,8 +46,13 @@ struct gf_problem {
   // device geometry (both precisions)
   double *egeom_d = nullptr;  // ne*(dim+1) (AFFINE)
   float *egeom_f = nullptr;
-  double *ngeom_d = nullptr;  // (dim+1)*nlocal (REGULAR)
+  double *ngeom_d = nullptr;  // (dim+1)*nlocal (REGULAR; DEFORMED/EMBEDDED: 0 planes + Jac)
   float *ngeom_f = nullptr;
+  // DEFORMED / EMBEDDED: full dXi/dX (dim*nxy planes), packed metric G_ij
+  // with W and Jac (dim(dim+1)/2 planes), node coordinates (optional)
+  int nxy = 0;
+  double *dgeom_d = nullptr, *gmet_d = nullptr, *xyz_d = nullptr;
+  float *dgeom_f = nullptr, *gmet_f = nullptr, *xyz_f = nullptr;
   double *mask_d = nullptr;   // nlocal or null
   float *mask_f = nullptr;
   double *imass_d = nullptr;  // 1/Smooth(mass), nlocal
@@ -97,6 +102,10 @@ int gf_fail(gf_context *ctx, int code, const char *fmt, ...);
   do {                                                                         \
     if (!(cond)) return gf_fail((ctx), GF_ERR_ARG, __VA_ARGS__);               \
   } while (0)
+
+// Velocity components of the advection terms: one per physical coordinate
+// (3 on a 2-d surface embedded in 3-d space).
+inline int gf_nvel(const gf_problem *p) { return p->nxy ? p->nxy : p->dim; }
 
 // Returns a device buffer of at least `bytes` from slot `slot` of the
 // problem's scratch list (allocated once, reused).

@@ -1,0 +1,170 @@
+// k_def.cuh -- operators on deformed (GE_DEFORMED) and 2-d embedded
+// (GE_2DEMBEDDED) elements, where the metric is a full per-node matrix:
+//   GHelmholtz::def_prod / embed_prod (sem/ghelmholtz.ipp:109-293)
+//     uo = p sum_j D_j^T (sum_i G_ij D_i u) + q M u,
+//     G_ij = sum_k dXi_i/dX_k dXi_j/dX_k W Jac   (def_init, 416-519)
+//   GGrid::deriv, deformed branch (grid/ggrid.ipp:1177-1186)
+//     du/dx_k = sum_j dXi_j/dX_k D_j u,  k < nxy
+//   GAdvect::apply (sem/gadvect.ipp:58-100) with nxy velocity components
+//   GBurgers::dudt_impl (pdes/gburgers.ipp:203-257) built from them.
+// One element per block; the element's values, its reference gradient and
+// the metric-weighted gradient live in shared memory, and threads stride
+// over the element's nodes in each pass.  The reference gradient is
+// computed once and shared by the diffusion and advection terms.
+#pragma once
+#include "k_maps.cuh"
+#include "k_tensor.cuh"
+
+namespace gfk {
+
+template <typename T>
+struct DefGeom {
+  const T *X;  // dim*nxy planes, plane i*nxy + k = dXi_i/dX_k
+  const T *G;  // packed symmetric metric with W and Jac: (00,01[,02],11[,12],22)
+  const T *J;  // Jacobian plane
+  int nxy;     // physical coordinates (dim, or 3 on an embedded surface)
+  int64_t nlocal;
+};
+
+__device__ __forceinline__ int gpack(int i, int j, int dim) {
+  if (i > j) {
+    const int t = i;
+    i = j;
+    j = t;
+  }
+  return dim == 2 ? (i == 0 ? j : 2) : (i == 0 ? j : (i == 1 ? 2 + j : 5));
+}
+
+template <typename T> inline DefGeom<T> def_of(const gf_problem *p);
+template <> inline DefGeom<double> def_of<double>(const gf_problem *p) {
+  return DefGeom<double>{p->dgeom_d, p->gmet_d, p->ngeom_d + (int64_t)p->dim * p->nlocal, p->nxy,
+                         p->nlocal};
+}
+template <> inline DefGeom<float> def_of<float>(const gf_problem *p) {
+  return DefGeom<float>{p->dgeom_f, p->gmet_f, p->ngeom_f + (int64_t)p->dim * p->nlocal, p->nxy,
+                        p->nlocal};
+}
+
+enum { DEF_HELM = 0, DEF_DUDT = 1, DEF_ADVECT = 2, DEF_DERIV = 3 };
+
+// mode DEF_HELM: uo = p L u (+ q M u); DEF_DUDT: uo = Minv(-nu L u - adv)
+// (heat when nv == 0); DEF_ADVECT: uo = adv = M sum_k c_k du/dx_k;
+// DEF_DERIV: uo = du/dx_{idir}.  nv velocity components c0..c2.
+template <typename T, int N, int DIM, class LD, typename TO>
+__global__ void __launch_bounds__(256)
+    k_def(const __grid_constant__ Basis<T, N> B, const DefGeom<T> g, int64_t ne, int mode, T p,
+          const T *__restrict__ pvec, T q, const T *__restrict__ qvec, int use_mass, const LD ld,
+          int nv, const T *__restrict__ c0, const T *__restrict__ c1, const T *__restrict__ c2,
+          int idir, const T *__restrict__ imass, TO *__restrict__ uo,
+          const double *__restrict__ stop) {
+  if (stop && stop[0] != 0.0) return;
+  constexpr int NN = N * N, NE = DIM == 3 ? NN * N : NN;
+  extern __shared__ __align__(16) unsigned char smem_def[];
+  T *su = reinterpret_cast<T *>(smem_def);
+  T *sd = su + NE;        // DIM planes: D_j u
+  T *sg = sd + DIM * NE;  // DIM planes: sum_i G_ij D_i u
+  const int64_t e = blockIdx.x;
+  if (e >= ne) return;
+  const int64_t base = e * NE;
+  const T *cv[3] = {c0, c1, c2};
+  const int64_t nl = g.nlocal;
+  // load
+  if (DIM == 3) {
+    for (int ij = threadIdx.x; ij < NN; ij += blockDim.x) {
+      typename LD::value_type lv[N];
+      ld.template zline<N>(e, ij % N, ij / N, lv);
+#pragma unroll
+      for (int k = 0; k < N; k++) su[k * NN + ij] = (T)lv[k];
+    }
+  } else {
+    for (int a = threadIdx.x; a < NN; a += blockDim.x)
+      su[a] = (T)ld.template point2<N>(e, a % N, a / N);
+  }
+  __syncthreads();
+  const int st[3] = {1, N, NN};
+  // reference gradient D_j u
+  for (int a = threadIdx.x; a < NE; a += blockDim.x) {
+    const int li[3] = {a % N, (a / N) % N, DIM == 3 ? a / NN : 0};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const int b0 = a - li[d] * st[d];
+      T s = B.D[li[d]] * su[b0];
+#pragma unroll
+      for (int m = 1; m < N; m++) s = fma(B.D[li[d] + m * N], su[b0 + m * st[d]], s);
+      sd[d * NE + a] = s;
+    }
+  }
+  __syncthreads();
+  // pointwise metric terms
+  for (int a = threadIdx.x; a < NE; a += blockDim.x) {
+    const int64_t node = base + a;
+    if (mode == DEF_DERIV) {
+      T du = sd[a] * g.X[(0 * g.nxy + idir - 1) * nl + node];
+      for (int j = 1; j < DIM; j++) du += sd[j * NE + a] * g.X[(j * g.nxy + idir - 1) * nl + node];
+      uo[node] = (TO)du;
+      continue;
+    }
+    if (mode != DEF_ADVECT) {
+#pragma unroll
+      for (int j = 0; j < DIM; j++) {
+        T gj = T(0);
+#pragma unroll
+        for (int i = 0; i < DIM; i++) gj += sd[i * NE + a] * g.G[gpack(i, j, DIM) * nl + node];
+        if (mode == DEF_HELM && pvec) gj *= pvec[node];
+        sg[j * NE + a] = gj;
+      }
+    }
+    if (mode == DEF_ADVECT || (mode == DEF_DUDT && nv > 0)) {
+      const int li[3] = {a % N, (a / N) % N, DIM == 3 ? a / NN : 0};
+      T mass = B.W[li[0]] * B.W[li[1]];
+      if (DIM == 3) mass *= B.W[li[2]];
+      mass *= g.J[node];
+      T po = T(0);
+      for (int k = 0; k < nv; k++) {
+        T dk = sd[a] * g.X[(0 * g.nxy + k) * nl + node];
+        for (int j = 1; j < DIM; j++) dk += sd[j * NE + a] * g.X[(j * g.nxy + k) * nl + node];
+        dk *= cv[k][node];
+        po = k == 0 ? dk : po + dk;
+      }
+      po *= mass;
+      if (mode == DEF_ADVECT) {
+        uo[node] = (TO)po;
+        continue;
+      }
+      su[a] = po;  // u itself is no longer needed by the rhs
+    }
+  }
+  if (mode == DEF_ADVECT || mode == DEF_DERIV) return;
+  __syncthreads();
+  // transposed divergence sum_j D_j^T g_j, then the mode's combination
+  for (int a = threadIdx.x; a < NE; a += blockDim.x) {
+    const int64_t node = base + a;
+    const int li[3] = {a % N, (a / N) % N, DIM == 3 ? a / NN : 0};
+    T o = T(0);
+#pragma unroll
+    for (int j = 0; j < DIM; j++) {
+      const int b0 = a - li[j] * st[j];
+      T s = B.D[li[j] * N] * sg[j * NE + b0];
+#pragma unroll
+      for (int m = 1; m < N; m++) s = fma(B.D[m + li[j] * N], sg[j * NE + b0 + m * st[j]], s);
+      o = j == 0 ? s : o + s;
+    }
+    if (mode == DEF_HELM) {
+      if (!pvec) o *= p;
+      if (use_mass) {
+        T mass = B.W[li[0]] * B.W[li[1]];
+        if (DIM == 3) mass *= B.W[li[2]];
+        T t = (mass * g.J[node]) * su[a];
+        t *= qvec ? qvec[node] : q;
+        o += t;
+      }
+      uo[node] = (TO)o;
+    } else {  // DEF_DUDT
+      o *= p;  // p = nu
+      const T r = nv > 0 ? T(-1) * o + T(-1) * su[a] : T(-1) * o;
+      uo[node] = (TO)(imass[node] * r);
+    }
+  }
+}
+
+}  // namespace gfk

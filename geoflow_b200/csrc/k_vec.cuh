@@ -112,4 +112,43 @@ __global__ void __launch_bounds__(RED_THREADS)
   }
 }
 
+// ---- GMTK::constrain2sphere (2) (blas/gmtk.ipp:2957-2976) ----
+// In place, in the reference's order: v0 first, then v1 from the updated
+// v0, then v2 from both; r^2 of node 0.  Explicit round-to-nearest
+// operations keep the compiler from contracting them into FMAs, so the
+// result is the reference's bit for bit.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+template <typename T>
+__global__ void k_constrain2sphere(int64_t n, T *__restrict__ v0, T *__restrict__ v1,
+                                   T *__restrict__ v2, const T *__restrict__ x,
+                                   const T *__restrict__ y, const T *__restrict__ z) {
+  const T r2 = add_rn(add_rn(mul_rn(x[0], x[0]), mul_rn(y[0], y[0])), mul_rn(z[0], z[0]));
+  const T ri = div_rn(T(1), r2);
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const T xj = x[j], yj = y[j], zj = z[j];
+    T a = v0[j], b = v1[j], c = v2[j];
+    a = mul_rn(sub_rn(sub_rn(mul_rn(a, sub_rn(r2, mul_rn(xj, xj))), mul_rn(mul_rn(b, xj), yj)),
+                      mul_rn(mul_rn(c, xj), zj)),
+               ri);
+    b = mul_rn(sub_rn(add_rn(mul_rn(mul_rn(-a, yj), xj), mul_rn(b, sub_rn(r2, mul_rn(yj, yj)))),
+                      mul_rn(mul_rn(c, yj), zj)),
+               ri);
+    c = mul_rn(add_rn(sub_rn(mul_rn(mul_rn(-a, zj), xj), mul_rn(mul_rn(b, zj), yj)),
+                      mul_rn(c, sub_rn(r2, mul_rn(zj, zj)))),
+               ri);
+    v0[j] = a;
+    v1[j] = b;
+    v2[j] = c;
+  }
+}
+
 }  // namespace gfk

@@ -5,6 +5,7 @@
 #include <unordered_map>
 
 #include "gf_common.cuh"
+#include "k_def.cuh"
 #include "k_dudt.cuh"
 #include "k_helm_k1.cuh"
 #include "k_tensor.cuh"
@@ -23,12 +24,54 @@ inline void set_smem(K kern, size_t bytes) {
   }
 }
 
+// Deformed / embedded elements (k_def.cuh): one element per block.
+template <typename T, class LD>
+struct DefLaunch {
+  template <int N>
+  struct F {
+    static int run(gf_problem *prob, int mode, T p, const T *pvec, T q, const T *qvec,
+                   int use_mass, LD ld, int nv, const T *const *c, int idir, T *uo,
+                   cudaStream_t st, const double *stop) {
+      const Basis<T, N> B = make_basis<T, N>(prob);
+      const DefGeom<T> g = def_of<T>(prob);
+      const T *cc[3] = {nullptr, nullptr, nullptr};
+      for (int k = 0; k < nv; k++) cc[k] = c[k];
+      const int NE = prob->dim == 3 ? N * N * N : N * N;
+      const size_t smem = sizeof(T) * (1 + 2 * prob->dim) * NE;
+      const int threads = NE < 256 ? ((NE + 31) / 32) * 32 : 256;
+      prob->launches++;
+      if (prob->dim == 3) {
+        auto kern = k_def<T, N, 3, LD, T>;
+        set_smem(kern, smem);
+        kern<<<(unsigned)prob->ne, threads, smem, st>>>(B, g, prob->ne, mode, p, pvec, q, qvec,
+                                                        use_mass, ld, nv, cc[0], cc[1], cc[2], idir,
+                                                        imass_of<T>(prob), uo, stop);
+      } else {
+        auto kern = k_def<T, N, 2, LD, T>;
+        set_smem(kern, smem);
+        kern<<<(unsigned)prob->ne, threads, smem, st>>>(B, g, prob->ne, mode, p, pvec, q, qvec,
+                                                        use_mass, ld, nv, cc[0], cc[1], cc[2], idir,
+                                                        imass_of<T>(prob), uo, stop);
+      }
+      return GF_OK;
+    }
+  };
+};
+
 template <typename T, class LD, typename TO = T>
 struct HelmLaunch {
   template <int N>
   struct F {
     static int run(gf_problem *prob, T p, const T *pvec, T q, const T *qvec, int use_mass,
                    LD ld, TO *uo, cudaStream_t st, const double *stop) {
+      if (prob->geom >= GF_GEOM_DEFORMED) {  // full per-node metric
+        if constexpr (!std::is_same<T, TO>::value) {
+          return GF_ERR_UNSUPPORTED;
+        } else {
+          return DefLaunch<T, LD>::template F<N>::run(prob, DEF_HELM, p, pvec, q, qvec, use_mass,
+                                                      ld, 0, nullptr, 0, uo, st, stop);
+        }
+      }
       const Geom<T> g = geom_of<T>(prob);
       constexpr int P = Pad<N>::P;
       if (prob->dim == 3 && g.egeom && !pvec) {

@@ -25,11 +25,14 @@ struct Stepper {
       : prob(p), st(p->ctx->stream), n(p->nlocal), eqn(tr->eqn), nstate(tr->nstate),
         scheme(tr->scheme), nu((T)tr->nu) {
     if (cv)
-      for (int k = 0; k < p->dim; k++) c[k] = (const T *)cv[k];
+      for (int k = 0; k < gf_nvel(p); k++) c[k] = (const T *)cv[k];
   }
   bool alloc();
   int rhs(T *const *u, T *const *Kout);
   void smooth(T *v);
+  // GMTK::constrain2sphere on the state where step_b calls it, on embedded
+  // surfaces with node coordinates and a state of >= 3 components
+  void constrain(T *const *u);
   // One step uin -> uout.  With a tape (pointers tape[3*m + k], m = 0 ..
   // stages-1), stage m's input state (the argument of its RHS call) is left
   // in tape[3*m + k] for the adjoint sweep.

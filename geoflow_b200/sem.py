@@ -132,12 +132,19 @@ class Problem:
     """Device-resident grid, operators and gather-scatter map (gf_problem)."""
 
     def __init__(self, ctx: Context, grid: GridBox, dirichlet_mask: bool = True,
-                 structured: bool = True, geometry: str = "affine"):
+                 structured: bool = True, geometry: str = "affine", node_geom=None,
+                 node_xyz=None):
         """geometry: "affine" passes one (dXi/dX, Jac) set per element;
         "regular" passes the same factors per node (the GGrid per-node
-        planes dXidX, Jac of a deformed grid)."""
+        planes dXidX, Jac); "deformed" (GE_DEFORMED) and "embedded"
+        (GE_2DEMBEDDED, a 2-d surface in 3-d space) take the caller's
+        node_geom = [dXi_i/dX_k planes (i < dim, k < nxy), Jac] as one array
+        of (dim*nxy + 1) * ndof values, nxy = dim or 3.  node_xyz (3 * ndof,
+        optional) are the node coordinates used by constrain2sphere."""
         self.ctx, self.grid = ctx, grid
         self.dim, self.n, self.nlocal = grid.dim, grid.n, grid.ndof()
+        # velocity components: one per physical coordinate
+        self.nvel = 3 if geometry == "embedded" else grid.dim
         d = A.ProblemDesc()
         d.dim, d.ne, d.n = grid.dim, grid.nelems, grid.n
         self._keep = [grid.D, grid.W, grid.elem_geom, grid.mask, grid.class_ptr, grid.members]
@@ -155,6 +162,15 @@ class Problem:
             d.geom = A.GF_GEOM_REGULAR
             d.elem_geom = None
             d.node_geom = A.ptr(ng)
+        elif geometry in ("deformed", "embedded"):
+            nxy = 3 if geometry == "embedded" else grid.dim
+            ng = np.ascontiguousarray(node_geom, dtype=np.float64).ravel()
+            if ng.size != (grid.dim * nxy + 1) * grid.ndof():
+                raise ValueError("node_geom must hold (dim*nxy + 1) * ndof values")
+            self._keep.append(ng)
+            d.geom = A.GF_GEOM_EMBEDDED if geometry == "embedded" else A.GF_GEOM_DEFORMED
+            d.elem_geom = None
+            d.node_geom = A.ptr(ng)
         else:
             raise ValueError(f"unknown geometry {geometry!r}")
         d.mask = A.ptr(grid.mask) if dirichlet_mask else None
@@ -164,6 +180,10 @@ class Problem:
             for k in range(grid.dim):
                 d.box_ne[k] = grid.ne[k]
                 d.box_periodic[k] = grid.periodic[k]
+        if node_xyz is not None:
+            xyz = np.ascontiguousarray(node_xyz, dtype=np.float64).ravel()
+            self._keep.append(xyz)
+            d.node_xyz = A.ptr(xyz)
         h = C.c_void_p()
         ctx.check(_lib().gf_problem_create(ctx.handle, C.byref(d), C.byref(h)), "gf_problem_create")
         self.handle = h
@@ -330,7 +350,7 @@ class GBurgers:
 
     def __init__(self, prob: Problem, eqn: int, nu: float, scheme: int = A.GF_RK4):
         self.prob, self.eqn, self.nu, self.scheme = prob, eqn, float(nu), scheme
-        self.nstate = prob.dim if eqn == A.GF_EQN_BURGERS else 1
+        self.nstate = prob.nvel if eqn == A.GF_EQN_BURGERS else 1
 
     def traits(self) -> A.RKTraits:
         t = A.RKTraits()

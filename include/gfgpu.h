@@ -55,7 +55,8 @@ enum { GF_NORM_INF = 0, GF_NORM_EUC = 1, GF_NORM_L2 = 2, GF_NORM_L1 = 3 }; /* li
  * no reference counterpart */
 enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1, GF_PRECOND_CHEBYSHEV = 2 };
 enum { GF_CG_FP64 = 0, GF_CG_MIXED = 1 };            /* plain FP64 / FP32 apply + FP64 refinement */
-enum { GF_GEOM_AFFINE = 0, GF_GEOM_REGULAR = 1 };     /* see gf_problem_desc */
+/* see gf_problem_desc; DEFORMED = GE_DEFORMED, EMBEDDED = GE_2DEMBEDDED */
+enum { GF_GEOM_AFFINE = 0, GF_GEOM_REGULAR = 1, GF_GEOM_DEFORMED = 2, GF_GEOM_EMBEDDED = 3 };
 enum { GF_EQN_ADVECT = 0, GF_EQN_BURGERS = 1, GF_EQN_HEAT = 2 }; /* GBurgers traits */
 /* GExRKStepper schemes: Butcher orders 1..4 (gbutcherrk.ipp:69-125) and
  * the SSP schemes (gexrk_stepper.ipp:533-780) */
@@ -113,11 +114,16 @@ typedef struct {
   int n;                   /* GLL points per direction (p+1), 2..12 */
   const double *D;         /* host, n*n column-major 1-d derivative */
   const double *W;         /* host, n GLL weights */
-  int geom;                /* GF_GEOM_AFFINE or GF_GEOM_REGULAR */
+  int geom;                /* GF_GEOM_* */
   /* GF_GEOM_AFFINE: host ne*(dim+1): dXidX_0..dim-1, Jac per element */
   const double *elem_geom;
   /* GF_GEOM_REGULAR: host (dim+1)*N_local: dXidX_0..dim-1, Jac per node
-   * (GGrid::dXidX(k,0), GGrid::Jac of reg_geom_init, ggrid.ipp:707-797) */
+   * (GGrid::dXidX(k,0), GGrid::Jac of reg_geom_init, ggrid.ipp:707-797).
+   * GF_GEOM_DEFORMED / GF_GEOM_EMBEDDED (dim 2 surface in 3-d space):
+   * host (dim*nxy+1)*N_local, nxy = dim (DEFORMED) or 3 (EMBEDDED):
+   * plane i*nxy+k = dXi_i/dX_k (GGrid::dXidX(i,k), def_geom_init), then Jac.
+   * The Laplacian uses G_ij = sum_k dXi_i/dX_k dXi_j/dX_k W Jac
+   * (GHelmholtz::def_init, ghelmholtz.ipp:416-519). */
   const double *node_geom;
   const double *mask;      /* host N_local, or NULL (all ones) */
   /* gather-scatter map (GGFX::recv_map_ as CSR) */
@@ -131,6 +137,9 @@ typedef struct {
    * index arrays in the solver. */
   int box_ne[3];
   int box_periodic[3];
+  /* optional host 3*N_local node coordinates (GGrid::xNodes); used by
+   * constrain2sphere in the RK stepper on EMBEDDED grids */
+  const double *node_xyz;
 } gf_problem_desc;
 
 int gf_problem_create(gf_ctx_t ctx, const gf_problem_desc *desc, gf_problem_t *out);
@@ -182,6 +191,13 @@ int gf_mult(gf_problem_t prob, int inverse, double *mult);
 /* GGrid::integrate (ggrid.ipp:1077-1147): returns the integral in *result
  * (host).  Synchronises. */
 int gf_integrate(gf_problem_t prob, int dtype, const void *u, double *result);
+/* GMTK::constrain2sphere (2) (blas/gmtk.ipp:2957-2976): v[0..2] (device,
+ * N_local each) projected in place onto the sphere through the node
+ * coordinates xyz[0..2] (device), with the reference's order: components
+ * updated in turn, each from the already-updated earlier ones, r^2 of
+ * node 0.  Does nothing unless the problem is GF_GEOM_EMBEDDED, as the
+ * reference does nothing unless the grid is GE_2DEMBEDDED. */
+int gf_constrain2sphere(gf_problem_t prob, int dtype, void *const *v, const void *const *xyz);
 
 /* ---- conjugate gradient (solvers/gcg.ipp:239-429) ---- */
 typedef struct {

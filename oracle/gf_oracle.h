@@ -121,6 +121,39 @@ void gfo_dudt(const gfo_grid *g, int kind, double nu, const double *imass,
               int nstate, const double *const *u, const double *const *c,
               double *const *dudt);
 
+/* ---- deformed (GE_DEFORMED) and 2-d embedded (GE_2DEMBEDDED) elements ----
+ * X[i][k] = dXi_i/dX_k per node, i < dim, k < nxy (nxy = dim, or 3 for a
+ * 2-d surface embedded in 3-d space); base->Jac, base->mass as for regular
+ * grids (base->dXidX unused). */
+typedef struct {
+  const gfo_grid *base;
+  int nxy;
+  const double *X[3][3];
+} gfo_defgrid;
+/* GHelmholtz::def_init (ghelmholtz.ipp:416-519): G(i,j) = sum_k X[i][k]
+ * X[j][k] W Jac for i,j < dim, as the 2-d branch computes it (the 3-d
+ * branch accumulates each off-diagonal twice through the shared storage of
+ * G(i,j) and G(j,i); the formula in its comment is followed here). */
+void gfo_def_metric(const gfo_defgrid *g, double *const G[3][3]);
+/* GHelmholtz::def_prod / embed_prod (ghelmholtz.ipp:109-293). */
+void gfo_def_helmholtz(const gfo_defgrid *g, const double *const G[3][3], const double *u,
+                       double p_scalar, const double *p_vec, const double *q_vec,
+                       double *uo);
+/* GGrid::deriv (ggrid.ipp:1163-1190), deformed branch: idir = 1..nxy. */
+void gfo_def_deriv(const gfo_defgrid *g, const double *u, int idir, double *du);
+/* GAdvect::apply (gadvect.ipp:58-100) with nxy velocity components. */
+void gfo_def_advect(const gfo_defgrid *g, const double *p, const double *const *c,
+                    double *po);
+/* GBurgers::dudt_impl on a deformed/embedded grid: kind as gfo_dudt;
+ * Burgers evolves nxy components. */
+void gfo_def_dudt(const gfo_defgrid *g, const double *const G[3][3], int kind, double nu,
+                  const double *imass, int nstate, const double *const *u,
+                  const double *const *c, double *const *dudt);
+/* GMTK::constrain2sphere (2) (gmtk.ipp:2957-2976), in place on v[0..2] of
+ * N nodes at coordinates xyz[0..2]: components updated in order, each from
+ * the already-updated earlier ones, r^2 taken at node 0. */
+void gfo_constrain2sphere(size_t N, const double *const *xyz, double *const *v);
+
 /* ---- GExRKStepper (gexrk_stepper.ipp) on the Burgers RHS ----
  * scheme: 1..4 Butcher step_b(1) of that order, 22/33/34 SSP schemes.
  * u[nstate] updated in place over nsteps steps of size dt. */

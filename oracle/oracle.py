@@ -32,6 +32,10 @@ class GfoGrid(C.Structure):
                 ("mass", P_double)]
 
 
+class GfoDefGrid(C.Structure):
+    _fields_ = [("base", C.POINTER(GfoGrid)), ("nxy", C.c_int), ("X", (P_double * 3) * 3)]
+
+
 class GfoBurgers(C.Structure):
     _fields_ = [("g", C.POINTER(GfoGrid)), ("kind", C.c_int), ("nu", C.c_double),
                 ("imass", P_double), ("c", C.POINTER(P_double)), ("nclass", c_size_t),
@@ -228,3 +232,91 @@ class OracleBox:
                                  ip(self.class_ptr), ip(self.members), dp(dinv), C.byref(tr),
                                  dp(b), dp(xb), dp(x), C.byref(it), dp(res))
         return rc, it.value, res[: it.value]
+
+
+class OracleDef:
+    """Deformed (GE_DEFORMED) or 2-d embedded (GE_2DEMBEDDED) geometry on the
+    elements, GLL basis and GGFX classes of an OracleBox: X[i][k] =
+    dXi_i/dX_k per node (i < dim, k < nxy) and Jac, as the caller's grid
+    would supply them."""
+
+    def __init__(self, box, X, Jac, nxy):
+        lib = load()
+        self.box, self.dim, self.nxy, self.N = box, box.dim, nxy, box.N
+        self.X = [[np.ascontiguousarray(X[i][k], dtype=np.float64) for k in range(nxy)]
+                  for i in range(self.dim)]
+        self.Jac = np.ascontiguousarray(Jac, dtype=np.float64)
+        g = GfoGrid()
+        g.dim, g.Ne = box.dim, box.nelems
+        for d in range(3):
+            g.n[d] = box.n
+            g.D[d] = dp(box.D)
+            g.W[d] = dp(box.W)
+            g.dXidX[d] = dp(box.dXidX[d])
+        g.Jac = dp(self.Jac)
+        self.mass = np.zeros(self.N)
+        lib.gfo_mass(C.byref(g), dp(self.mass))
+        g.mass = dp(self.mass)
+        self._g = g
+        dg = GfoDefGrid()
+        dg.base = C.pointer(self._g)
+        dg.nxy = nxy
+        for i in range(self.dim):
+            for k in range(nxy):
+                dg.X[i][k] = dp(self.X[i][k])
+        self._dg = dg
+        self.G = [[np.zeros(self.N) for _ in range(3)] for _ in range(3)]
+        self._Garr = self._mat(self.G)
+        lib.gfo_def_metric(C.byref(dg), self._Garr)
+        sm = self.mass.copy()
+        box.dss(sm, SMOOTH)
+        self.imass = 1.0 / sm
+
+    @staticmethod
+    def _mat(G):
+        arr = ((P_double * 3) * 3)()
+        for i in range(3):
+            for j in range(3):
+                arr[i][j] = dp(G[i][j])
+        return arr
+
+    def node_geom(self):
+        """[dXi_i/dX_k planes (i, k), Jac] as one array (gf_problem_desc)."""
+        planes = [self.X[i][k] for i in range(self.dim) for k in range(self.nxy)]
+        return np.concatenate(planes + [self.Jac])
+
+    def helmholtz(self, u, p=1.0, p_vec=None, q_vec=None):
+        uo = np.zeros(self.N)
+        load().gfo_def_helmholtz(C.byref(self._dg), self._Garr, dp(u), C.c_double(p), dp(p_vec),
+                                 dp(q_vec), dp(uo))
+        return uo
+
+    def deriv(self, u, idir):
+        du = np.zeros(self.N)
+        load().gfo_def_deriv(C.byref(self._dg), dp(u), idir, dp(du))
+        return du
+
+    def advect(self, p, c):
+        arr = (P_double * 3)(*[dp(a) for a in c] + [None] * (3 - len(c)))
+        po = np.zeros(self.N)
+        load().gfo_def_advect(C.byref(self._dg), dp(p), arr, dp(po))
+        return po
+
+    def dudt(self, kind, nu, u, c=None):
+        nst = len(u)
+        ua = (P_double * 3)(*[dp(a) for a in u] + [None] * (3 - nst))
+        nc = len(c) if c else 0
+        ca = (P_double * 3)(*([dp(a) for a in c] if c else []) + [None] * (3 - nc))
+        out = [np.zeros(self.N) for _ in range(nst)]
+        oa = (P_double * 3)(*[dp(a) for a in out] + [None] * (3 - nst))
+        load().gfo_def_dudt(C.byref(self._dg), self._Garr, kind, C.c_double(nu), dp(self.imass),
+                            nst, ua, ca, oa)
+        return out
+
+
+def constrain2sphere(xyz, v):
+    """GMTK::constrain2sphere (2) in place on v[0..2] (numpy FP64)."""
+    xa = (P_double * 3)(*[dp(a) for a in xyz])
+    va = (P_double * 3)(*[dp(a) for a in v])
+    load().gfo_constrain2sphere(c_size_t(len(v[0])), xa, va)
+    return v

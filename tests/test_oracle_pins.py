@@ -205,3 +205,41 @@ def test_oracle_vs_ref_build_if_present():
         b = O.gll(p)
         for u, v in zip(a, b):
             assert np.array_equal(bits(u), bits(v))
+
+
+def test_deformed_oracle_reduces_to_regular():
+    """The deformed-element oracle (def_prod, deriv, GAdvect, dudt with a
+    full metric) equals the regular-element oracle when dXi/dX is diagonal."""
+    b = O.OracleBox(3, [2, 1, 2], 5, periodic=[1, 0, 0])
+    rng = np.random.default_rng(4)
+    N = b.N
+    X = [[b.dXidX[i] if i == k else np.zeros(N) for k in range(3)] for i in range(3)]
+    d = O.OracleDef(b, X, b.Jac, 3)
+    u = rng.standard_normal(N)
+    c = [rng.standard_normal(N) for _ in range(3)]
+    ref = b.helmholtz(u, p=0.7, q_vec=np.full(N, 0.3))
+    assert np.max(np.abs(d.helmholtz(u, p=0.7, q_vec=np.full(N, 0.3)) - ref)) <= 1e-14 * np.max(np.abs(ref))
+    for k in (1, 2, 3):
+        assert np.array_equal(d.deriv(u, k), b.deriv(u, k))
+    ra = b.advect(u, c)
+    assert np.max(np.abs(d.advect(u, c) - ra)) <= 1e-14 * np.max(np.abs(ra))
+    for kind, nst in ((0, 1), (1, 3), (2, 1)):
+        us = [rng.standard_normal(N) for _ in range(nst)]
+        r1 = d.dudt(kind, 0.02, us, c if kind == 0 else None)
+        r2 = b.dudt(kind, 0.02, us, c if kind == 0 else None)
+        for a, bb in zip(r1, r2):
+            assert np.max(np.abs(a - bb)) <= 1e-13 * np.max(np.abs(bb))
+
+
+def test_constrain2sphere_oracle_known_values():
+    """GMTK::constrain2sphere (2) updates the components in turn: a radial
+    vector loses its x component exactly, and y then sees the updated x."""
+    xyz = [np.array([1.0, 0.0]), np.array([2.0, 0.0]), np.array([2.0, 3.0])]
+    v = [xyz[0].copy(), xyz[1].copy(), xyz[2].copy()]
+    O.constrain2sphere(xyz, v)
+    r2 = 9.0
+    assert v[0][0] == 0.0
+    assert v[1][0] == (2.0 * (r2 - 4.0) - 2.0 * 2.0 * 2.0) / r2
+    # node 1 (0, 0, 3): only z survives the x/y terms
+    assert v[0][1] == 0.0 and v[1][1] == 0.0
+    assert v[2][1] == (3.0 * (r2 - 9.0)) / r2
