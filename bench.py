@@ -75,7 +75,8 @@ def parse():
                     help="FP32 applies per Chebyshev preconditioner application")
     ap.add_argument("--poly-ratio", type=float, default=0.0,
                     help="b/a of the Chebyshev interval (0: library default)")
-    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply", "adjoint"], default=None,
+    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply", "adjoint", "graphs"],
+                    default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
 
@@ -376,6 +377,85 @@ def adjoint_bench(ctx, ne=16, p=6, nsteps=50, ck=10, reps=3):
 
 
 # ---------------------------------------------------------------------------
+def graph_bench(ctx, reps=3):
+    """Small, launch-bound workloads: (1) 2-d periodic advection-diffusion on
+    16^2 elements p = 4 (c = (1, 0.5), nu = 0.01, dt = 1e-4, RK4, 200 steps)
+    by direct calls vs one CUDA graph; (2) an ensemble of 16 independent
+    2-d periodic boxes (8^2..64^2 elements, p = 3..8, seeded) advanced 20
+    RK4 steps, member by member vs one ensemble graph."""
+    import torch
+    from geoflow_b200 import GBurgers, Graph, GridBox, Problem
+    from geoflow_b200 import _abi as A
+    dev = ctx.torch_device
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e) / 1e3)
+        return statistics.median(ts)
+
+    def box(ne, p, seed):
+        g = GridBox(2, [ne, ne], p, periodic=[1, 1])
+        prob = Problem(ctx, g, dirichlet_mask=False)
+        rng = np.random.default_rng(seed)
+        first = g.members[g.class_ptr[:-1]][g.node_class]
+        x, y = g.xyz
+        u0 = np.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / 0.01)[first]
+        u0 = u0 + rng.uniform(-1e-3, 1e-3, g.nclass)[g.node_class]
+        u = [torch.from_numpy(u0).to(dev)]
+        c = [torch.ones(g.ndof(), dtype=torch.float64, device=dev),
+             torch.full((g.ndof(),), 0.5, dtype=torch.float64, device=dev)]
+        return g, prob, GBurgers(prob, A.GF_EQN_ADVECT, 0.01, scheme=A.GF_RK4), u, c
+
+    out = {}
+    g, prob, B, u, c = box(16, 4, SEED + 5)
+    nsteps = 200
+    t_direct = timed(lambda: B.step(u, c, dt=1e-4, nsteps=nsteps))
+    G = B.capture(u, c, dt=1e-4, nsteps=nsteps)
+    t_graph = timed(G.launch)
+    stages = 4 * nsteps
+    out["config1"] = {
+        "workload": "2d periodic advection-diffusion, 16^2 elements p=4, RK4, 200 steps, FP64",
+        "n_local": prob.nlocal, "direct_s": t_direct, "graph_s": t_graph,
+        "gdofs_per_stage_direct": prob.nlocal * stages / t_direct / 1e9,
+        "gdofs_per_stage_graph": prob.nlocal * stages / t_graph / 1e9,
+        "graph_nodes": G.nodes()}
+    G.close()
+    rng = np.random.default_rng(SEED + 6)
+    members = [box(int(rng.choice([8, 16, 24, 32, 48, 64])), int(rng.integers(3, 9)), SEED + 10 + i)
+               for i in range(16)]
+    steps = 20
+
+    def seq():
+        for _, _, Bm, um, cm in members:
+            Bm.step(um, cm, dt=1e-4, nsteps=steps)
+
+    t_seq = timed(seq)
+    graphs = [Bm.capture(um, cm, dt=1e-4, nsteps=steps) for _, _, Bm, um, cm in members]
+    E = Graph.ensemble(graphs)
+    t_ens = timed(E.launch)
+    ndof = sum(pm.nlocal for _, pm, _, _, _ in members)
+    out["ensemble"] = {
+        "workload": ("16 independent 2d periodic advection boxes (8^2..64^2 elements, p=3..8), "
+                     "RK4, 20 steps each, FP64"),
+        "members": [[gm.ne[0], gm.p] for gm, _, _, _, _ in members], "n_local_total": ndof,
+        "sequential_s": t_seq, "ensemble_graph_s": t_ens,
+        "gdofs_per_stage_sequential": ndof * 4 * steps / t_seq / 1e9,
+        "gdofs_per_stage_ensemble": ndof * 4 * steps / t_ens / 1e9}
+    E.close()
+    for gr in graphs:
+        gr.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 def cpu_oracle_iteration_time(sample_ne, p, iters=6):
     """Seconds per FP64 Jacobi-PCG iteration of the CPU oracle (a plain-C
     restatement of GCG::solve_impl + GHelmholtz::reg_prod + GGFX::doOp) on a
@@ -465,6 +545,9 @@ def main():
     tr_cheb = CGTraits(precision=A.GF_CG_MIXED, check_every=4, poly_degree=args.poly,
                        poly_ratio=args.poly_ratio,
                        **dict(common, precond=A.GF_PRECOND_CHEBYSHEV))
+    if args.only == "graphs":
+        print(json.dumps({"only": "graphs", "graphs": graph_bench(ctx)}), flush=True)
+        return
     if args.only == "adjoint":
         print(json.dumps({"only": "adjoint", "adjoint": adjoint_bench(ctx)}), flush=True)
         return
@@ -522,10 +605,11 @@ def main():
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    rk = adj = None
+    rk = adj = graphs = None
     if not args.no_rk:
         rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p)
         adj = adjoint_bench(ctx)
+        graphs = graph_bench(ctx)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         t_node, nsample, wall = cpu_oracle_iteration_time(args.cpu_sample_ne, args.p, args.cpu_iters)
@@ -562,6 +646,7 @@ def main():
         "kernels": {"helm3d": roof, "dss_sum": dss},
         "rk_stage": rk,
         "adjoint": adj,
+        "graphs": graphs,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": per_step_launches * args.steps,

@@ -5,8 +5,8 @@ the Python host-side mirror of the reference interfaces over that ABI.
 """
 from . import _abi
 from ._abi import GFError, load
-from .sem import (CGTraits, Context, GBurgers, GCG, GGFX, GHelmholtz, GMass, GridBox, Problem,
-                  gll_basis)
+from .sem import (CGTraits, Context, GBurgers, GCG, GGFX, GHelmholtz, GMass, Graph, GridBox,
+                  Problem, gll_basis)
 
 __all__ = ["GFError", "load", "CGTraits", "Context", "GBurgers", "GCG", "GGFX", "GHelmholtz",
-           "GMass", "GridBox", "Problem", "gll_basis", "_abi"]
+           "GMass", "Graph", "GridBox", "Problem", "gll_basis", "_abi"]

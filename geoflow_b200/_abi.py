@@ -97,6 +97,12 @@ SIGNATURES = {
                                    c_double, c_int]),
     "gf_integrate_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gf_constrain2sphere": (c_int, [c_void_p, c_int, P_void, P_void]),
+    "gf_rk_graph_create": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
+                                   c_int, P_void]),
+    "gf_graph_ensemble": (c_int, [c_int, P_void, P_void]),
+    "gf_graph_launch": (c_int, [c_void_p]),
+    "gf_graph_nodes": (c_int, [c_void_p]),
+    "gf_graph_destroy": (c_int, [c_void_p]),
     "gf_dudt_vjp": (c_int, [c_void_p, c_int, c_int, c_double, c_int, P_void, P_void, P_void,
                             P_void]),
     "gf_dss_T": (c_int, [c_void_p, c_int, c_int, c_void_p]),

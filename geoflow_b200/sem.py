@@ -369,6 +369,16 @@ class GBurgers:
                                                  A.ptr_array(u), A.ptr_array(c or []), t0, dt,
                                                  nsteps), "GBurgers::step")
 
+    def capture(self, u, c=None, dt=1e-4, nsteps=1):
+        """Record `nsteps` steps advancing u in place as a CUDA graph
+        (Graph.launch replays them; same result as step())."""
+        tr = self.traits()
+        h = C.c_void_p()
+        self.prob.ctx.check(_lib().gf_rk_graph_create(
+            self.prob.handle, _dtype_code(u[0]), C.byref(tr), A.ptr_array(u),
+            A.ptr_array(c or []), dt, nsteps, C.byref(h)), "GBurgers::capture")
+        return Graph(self.prob.ctx, h, [u, c, self.prob])
+
     # ---- adjoint (no reference counterpart; FP64 only) ----
     def dudt_vjp(self, u, c, lam, ubar):
         """ubar = (d dudt/du)^T lam at state u (velocity c for advection)."""
@@ -398,3 +408,38 @@ class GBurgers:
             A.ptr_array(u_obs), dt, nsteps, checkpoint_every, C.byref(J), A.ptr_array(grad)),
             "GBurgers::adjoint_gradient")
         return J.value, grad
+
+
+class Graph:
+    """A CUDA graph of RK steps (GBurgers.capture) or an ensemble of such
+    graphs (Graph.ensemble): launch() replays the recorded work in one call.
+    Keeps the tensors it was recorded with alive."""
+
+    def __init__(self, ctx: Context, handle, keep):
+        self.ctx, self.handle, self._keep = ctx, handle, keep
+
+    @staticmethod
+    def ensemble(graphs):
+        arr = (C.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
+        h = C.c_void_p()
+        ctx = graphs[0].ctx
+        ctx.check(_lib().gf_graph_ensemble(len(graphs), arr, C.byref(h)), "gf_graph_ensemble")
+        return Graph(ctx, h, list(graphs))
+
+    def launch(self):
+        self.ctx.check(_lib().gf_graph_launch(self.handle), "gf_graph_launch")
+
+    def nodes(self) -> int:
+        return _lib().gf_graph_nodes(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib().gf_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -268,6 +268,24 @@ int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
 int gf_integrate_noalloc(int64_t n, const double *mass, const double *u, double *result,
                          void *stream);
 
+/* ---- CUDA graphs (no reference counterpart) ---- */
+/* Records nsteps RK steps of gf_rk_advance (same arguments, same result)
+ * as a CUDA graph; gf_graph_launch replays them on the problem's stream in
+ * one call.  The graph keeps the device pointers u, c and the problem's
+ * work buffers: they must outlive it.  The capture uses a library stream,
+ * so the context's stream may be the legacy default stream. */
+typedef struct gf_graph *gf_graph_t;
+int gf_rk_graph_create(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
+                       void *const *u, const void *const *c, double dt, int nsteps,
+                       gf_graph_t *out);
+/* One graph holding n graphs of independent problems as concurrent
+ * branches (an ensemble advanced by one launch), launched on the stream of
+ * parts[0]'s context. */
+int gf_graph_ensemble(int n, const gf_graph_t *parts, gf_graph_t *out);
+int gf_graph_launch(gf_graph_t g);
+int gf_graph_nodes(gf_graph_t g);  /* kernel/copy nodes recorded */
+int gf_graph_destroy(gf_graph_t g);
+
 /* ---- adjoint (no reference counterpart) ---- */
 /* Vector-Jacobian product of gf_dudt: given u (and c) and a cotangent
  * lam[nstate] on dudt, returns ubar[nstate] = (d dudt/du)^T lam. */
