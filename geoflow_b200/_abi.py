@@ -97,6 +97,8 @@ SIGNATURES = {
                                    c_double, c_int]),
     "gf_integrate_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gf_constrain2sphere": (c_int, [c_void_p, c_int, P_void, P_void]),
+    "gf_tensor_apply": (c_int, [c_void_p, c_int, P_double, P_double, P_double, c_void_p,
+                                c_void_p]),
     "gf_rk_graph_create": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
                                    c_int, P_void]),
     "gf_graph_ensemble": (c_int, [c_int, P_void, P_void]),

@@ -245,6 +245,17 @@ class GGFX:
         return m
 
 
+def tensor_apply(prob: Problem, A1, A2, A3, u, out):
+    """out = (A3 x A2 x A1) u in every element (GMTK::D3_X_D2_X_D1 /
+    D2_X_D1 with the matrices as given, n x n column-major numpy arrays;
+    A3 unused in 2-d).  A spectral filter is A_d = the filter matrix."""
+    mats = [np.ascontiguousarray(a, dtype=np.float64).ravel(order="F") if a is not None else None
+            for a in (A1, A2, A3)]
+    prob.ctx.check(_lib().gf_tensor_apply(prob.handle, _dtype_code(u), A.ptr(mats[0]),
+                                          A.ptr(mats[1]), A.ptr(mats[2]), A.ptr(u), A.ptr(out)),
+                   "tensor_apply")
+
+
 class GMass:
     """Lumped mass W x W (x W) x Jac; inverse=True uses 1/Smooth(M)."""
 

@@ -191,6 +191,14 @@ int gf_mult(gf_problem_t prob, int inverse, double *mult);
 /* GGrid::integrate (ggrid.ipp:1077-1147): returns the integral in *result
  * (host).  Synchronises. */
 int gf_integrate(gf_problem_t prob, int dtype, const void *u, double *result);
+/* Full tensor product of per-direction n x n matrices (host, column-major
+ * like D): out = (A3 (x) A2 (x) A1) u in every element, A3 ignored in 2-d.
+ * GMTK::D2_X_D1 (blas/gmtk.ipp:1570-1619), D3_X_D2_X_D1 (1930-1996) and the
+ * weighted forms (1639-1911, 2311-2519) with the weights folded into A_d;
+ * GBoydFilter::apply_impl (sem/gboyd_filter.ipp) is A_d = the basis' filter
+ * matrix F. out must not alias u. */
+int gf_tensor_apply(gf_problem_t prob, int dtype, const double *A1, const double *A2,
+                    const double *A3, const void *u, void *out);
 /* GMTK::constrain2sphere (2) (blas/gmtk.ipp:2957-2976): v[0..2] (device,
  * N_local each) projected in place onto the sphere through the node
  * coordinates xyz[0..2] (device), with the reference's order: components

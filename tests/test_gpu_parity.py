@@ -361,3 +361,56 @@ def test_box_description_must_match_classes(ctx):
     g.ne = [4, 2, 1]  # same element count, different lattice
     with pytest.raises(A.GFError):
         Problem(ctx, g)
+
+
+@pytest.mark.parametrize("dim,ne,p", [(3, [2, 3, 2], 4), (3, [1, 2, 2], 7), (2, [3, 4], 5),
+                                      (2, [2, 2], 11)])
+def test_tensor_apply_matches_oracle_composition(ctx, dim, ne, p):
+    """(A3 x A2 x A1) u against the oracle's single-direction GMTK products
+    (I3_X_I2_X_D1, I3_X_D2_X_I1, D3_X_I2_X_I1; 2-d I2_X_D1, D2_X_I1)."""
+    from geoflow_b200.sem import tensor_apply
+    g, prob, o = setup(ctx, dim, ne, p)
+    n = p + 1
+    rng = np.random.default_rng(31 + p)
+    mats = [rng.standard_normal((n, n)) for _ in range(3)]
+    u = rng.standard_normal(g.ndof())
+    out = prob.zeros()
+    tensor_apply(prob, mats[0], mats[1], mats[2] if dim == 3 else None, dev(u), out)
+    lib, Ne = O.load(), g.nelems
+    col = lambda m: np.ascontiguousarray(m.ravel(order="F"))
+    y1, y2 = np.zeros(g.ndof()), np.zeros(g.ndof())
+    if dim == 3:
+        y3 = np.zeros(g.ndof())
+        lib.gfo_I3_X_I2_X_D1(O.dp(col(mats[0])), O.dp(u), n, n, n, Ne, O.dp(y1))
+        lib.gfo_I3_X_D2_X_I1(O.dp(col(mats[1].T)), O.dp(y1), n, n, n, Ne, O.dp(y2))
+        lib.gfo_D3_X_I2_X_I1(O.dp(col(mats[2].T)), O.dp(y2), n, n, n, Ne, O.dp(y3))
+        ref = y3
+    else:
+        lib.gfo_I2_X_D1(O.dp(col(mats[0])), O.dp(u), n, n, Ne, O.dp(y1))
+        lib.gfo_D2_X_I1(O.dp(col(mats[1].T)), O.dp(y1), n, n, Ne, O.dp(y2))
+        ref = y2
+    assert relerr(host(out), ref) < 1e-13
+
+
+def test_filter_through_tensor_apply_keeps_low_modes(ctx):
+    """A Boyd-type filter F = L Lambda L^-1 (L_ij = P_j(xi_i), Lambda = 1 on
+    modes below the cut-off) applied as (F x F x F) u leaves a field of
+    degree below the cut-off unchanged and damps the highest mode."""
+    from numpy.polynomial import legendre as leg
+    from geoflow_b200.sem import tensor_apply
+    p, cut = 6, 4
+    g, prob, o = setup(ctx, 3, [2, 2, 2], p)
+    n = p + 1
+    L = np.stack([leg.legval(g.xi, np.eye(n)[j]) for j in range(n)], 1)
+    lam = np.ones(n)
+    lam[cut:] = 0.5 * ((np.arange(cut, n) - cut) / (n - cut)) ** 2
+    F = L @ np.diag(lam) @ np.linalg.inv(L)
+    x, y, z = g.xyz
+    u = (1 + x + x ** 2 * y - 0.5 * y ** 3 + z ** 3 * x)  # degree < cut in each direction
+    out = prob.zeros()
+    tensor_apply(prob, F, F, F, dev(u), out)
+    assert relerr(host(out), u) < 1e-12
+    top = L[:, n - 1]  # the highest Legendre mode along x in every element
+    v = np.tile(np.tile(top, n * n), g.nelems)
+    tensor_apply(prob, F, F, F, dev(v), out)
+    assert relerr(host(out), lam[n - 1] * v) < 1e-12
