@@ -75,7 +75,7 @@ def parse():
                     help="FP32 applies per Chebyshev preconditioner application")
     ap.add_argument("--poly-ratio", type=float, default=0.0,
                     help="b/a of the Chebyshev interval (0: library default)")
-    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply", "adjoint", "graphs"],
+    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "apply", "adjoint", "graphs", "rk"],
                     default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
@@ -545,6 +545,11 @@ def main():
     tr_cheb = CGTraits(precision=A.GF_CG_MIXED, check_every=4, poly_degree=args.poly,
                        poly_ratio=args.poly_ratio,
                        **dict(common, precond=A.GF_PRECOND_CHEBYSHEV))
+    if args.only == "rk":
+        print(json.dumps({"only": "rk", "rk_stage": rk_stage_bench(ctx, args.rk_ne, args.rk_p,
+                                                                  steps=args.steps,
+                                                                  warmup=args.warmup)}), flush=True)
+        return
     if args.only == "graphs":
         print(json.dumps({"only": "graphs", "graphs": graph_bench(ctx)}), flush=True)
         return

@@ -71,30 +71,6 @@ __global__ void k_stage_sum(int64_t n, const T *__restrict__ uin, int nk, const 
   }
 }
 
-// uout += K * ch
-template <typename T>
-__global__ void k_accum(int64_t n, const T *__restrict__ K, T ch, T *__restrict__ uout) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    T s = K[i];
-    s *= ch;
-    uout[i] += s;
-  }
-}
-
-// x = dt*x + 1*uin (step_euler), then x = a*x + b*y (saxpby) when a != 1 || y
-template <typename T>
-__global__ void k_euler(int64_t n, T *__restrict__ x, T dt, const T *__restrict__ uin, T a,
-                        const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    T v = dt * x[i] + T(1) * uin[i];
-    if (y) v = a * v + b * y[i];
-    if (y2) v = a2 * v + b2 * y2[i];
-    x[i] = v;
-  }
-}
-
 template <typename T>
 int Stepper<T>::rhs(T *const *u, T *const *K) {
   const T *f[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -124,6 +100,34 @@ int Stepper<T>::rhs(T *const *u, T *const *K) {
 template <typename T>
 void Stepper<T>::smooth(T *v) {
   launch_dss<T>(prob, GF_DSS_SMOOTH, v, st);
+}
+
+// gather-scatter Smooth fused with the stage update around it (k_dss.cuh)
+template <typename T>
+void Stepper<T>::euler_smooth(T *x, T dt, const T *uin, T a, const T *y, T b, T a2, const T *y2,
+                              T b2) {
+  prob->launches++;
+  k_dss_rk_csr<T, FUSE_EULER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256, 0,
+                                st>>>(x, prob->class_ptr, prob->members, prob->nclass, dt, uin,
+                                      a, y, b, a2, y2, b2, nullptr, nullptr, T(0));
+}
+
+template <typename T>
+void Stepper<T>::smooth_accum(T *K, T ch, T *uout) {
+  prob->launches++;
+  k_dss_rk_csr<T, FUSE_ACCUM_AFTER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256,
+                                      0, st>>>(K, prob->class_ptr, prob->members, prob->nclass,
+                                               T(0), nullptr, T(0), nullptr, T(0), T(0),
+                                               nullptr, T(0), uout, nullptr, ch);
+}
+
+template <typename T>
+void Stepper<T>::accum_smooth(T *uout, const T *K, T ch) {
+  prob->launches++;
+  k_dss_rk_csr<T, FUSE_ACCUM_BEFORE><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16),
+                                       256, 0, st>>>(uout, prob->class_ptr, prob->members,
+                                                     prob->nclass, T(0), nullptr, T(0), nullptr,
+                                                     T(0), T(0), nullptr, T(0), nullptr, K, ch);
 }
 
 template <typename T>
@@ -172,11 +176,7 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
       }
       constrain(um);
       if ((rc = rhs(um, K[m]))) return rc;
-      for (int k = 0; k < nstate; k++) {
-        smooth(K[m][k]);
-        prob->launches++;
-        k_accum<T><<<g, 256, 0, st>>>(n, K[m][k], (T)cc[m] * h, uout[k]);
-      }
+      for (int k = 0; k < nstate; k++) smooth_accum(K[m][k], (T)cc[m] * h, uout[k]);
       constrain(uout);
     }
     T *const *uf = stage_in(ns - 1);
@@ -193,11 +193,7 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
     T *const *Kf = K[0];
     if ((rc = rhs(uf, Kf))) return rc;
     for (int k = 0; k < nstate; k++) smooth(Kf[k]);
-    for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_accum<T><<<g, 256, 0, st>>>(n, Kf[k], (T)cc[ns - 1] * h, uout[k]);
-      smooth(uout[k]);
-    }
+    for (int k = 0; k < nstate; k++) accum_smooth(uout[k], Kf[k], (T)cc[ns - 1] * h);
     constrain(uout);
     return GF_OK;
   }
@@ -222,70 +218,45 @@ int Stepper<T>::step_ssp(T *const *uin, T *const *uout, T dt) {
   if (scheme == GF_SSP22) {
     if ((rc = rhs(uin, K[0]))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
-      smooth(K[0][k]);
+      euler_smooth(K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
     }
     if ((rc = rhs(K[0], uout))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, uout[k], dt, K[0][k], T(0.5), uin[k], T(0.5), one, nullptr,
-                                    T(0));
-      smooth(uout[k]);
+      euler_smooth(uout[k], dt, K[0][k], T(0.5), uin[k], T(0.5), one, nullptr, T(0));
     }
     return GF_OK;
   }
   if (scheme == GF_SSP33) {
     if ((rc = rhs(uin, K[0]))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
-      smooth(K[0][k]);
+      euler_smooth(K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
     }
     if ((rc = rhs(K[0], K[1]))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, K[1][k], dt, K[0][k], T(0.25), uin[k], T(0.75), one,
-                                    nullptr, T(0));
-      smooth(K[1][k]);
+      euler_smooth(K[1][k], dt, K[0][k], T(0.25), uin[k], T(0.75), one, nullptr, T(0));
     }
     if ((rc = rhs(K[1], uout))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, uout[k], dt, K[1][k], T(2.0 / 3.0), uin[k], T(1.0 / 3.0),
-                                    one, nullptr, T(0));
-      smooth(uout[k]);
+      euler_smooth(uout[k], dt, K[1][k], T(2.0 / 3.0), uin[k], T(1.0 / 3.0), one, nullptr, T(0));
     }
     return GF_OK;
   }
   if (scheme == GF_SSP34) {
     if ((rc = rhs(uin, K[0]))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, K[0][k], dt, uin[k], T(0.5), uin[k], T(0.5), one, nullptr,
-                                    T(0));
-      smooth(K[0][k]);
+      euler_smooth(K[0][k], dt, uin[k], T(0.5), uin[k], T(0.5), one, nullptr, T(0));
     }
     if ((rc = rhs(K[0], K[1]))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, K[1][k], dt, K[0][k], T(0.5), K[0][k], T(0.5), one, nullptr,
-                                    T(0));
-      smooth(K[1][k]);
+      euler_smooth(K[1][k], dt, K[0][k], T(0.5), K[0][k], T(0.5), one, nullptr, T(0));
     }
     if ((rc = rhs(K[1], K[2]))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, K[2][k], dt, K[1][k], T(1.0 / 6.0), K[1][k], T(1.0 / 6.0),
-                                    one, uin[k], T(2.0 / 3.0));
-      smooth(K[2][k]);
+      euler_smooth(K[2][k], dt, K[1][k], T(1.0 / 6.0), K[1][k], T(1.0 / 6.0), one, uin[k], T(2.0 / 3.0));
     }
     if ((rc = rhs(K[2], uout))) return rc;
     for (int k = 0; k < nstate; k++) {
-      prob->launches++;
-      k_euler<T><<<g, 256, 0, st>>>(n, uout[k], dt, K[2][k], T(0.5), K[2][k], T(0.5), one, nullptr,
-                                    T(0));
-      smooth(uout[k]);
+      euler_smooth(uout[k], dt, K[2][k], T(0.5), K[2][k], T(0.5), one, nullptr, T(0));
     }
     return GF_OK;
   }

@@ -60,4 +60,57 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---- gather-scatter fused with the RK stage updates (api_rk.cu) ----
+// The stage arithmetic of GExRKStepper, with explicit round-to-nearest
+// operations so that it rounds the same wherever it runs:
+//   step_euler + saxpby (gexrk_stepper.ipp:809-819, 533-780):
+//     v = dt x + 1 uin;  v = a v + b y (if y);  v = a2 v + b2 y2 (if y2)
+//   step_b accumulation (252-341): uout += (K * ch)
+template <typename T>
+__device__ __forceinline__ T rk_euler_point(T x, T dt, T uin, T a, const T *y, T b, T a2,
+                                            const T *y2, T b2, int64_t i) {
+  T v = add_rn(mul_rn(dt, x), mul_rn(T(1), uin));
+  if (y) v = add_rn(mul_rn(a, v), mul_rn(b, y[i]));
+  if (y2) v = add_rn(mul_rn(a2, v), mul_rn(b2, y2[i]));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T rk_accum_point(T uout, T K, T ch) {
+  return add_rn(uout, mul_rn(K, ch));
+}
+
+enum { FUSE_EULER = 0, FUSE_ACCUM_AFTER = 1, FUSE_ACCUM_BEFORE = 2 };
+
+// One thread per class, members in ascending local id, Smooth fold:
+//   FUSE_EULER:        x_m <- rk_euler_point(x_m, ...) folded           (SSP substep)
+//   FUSE_ACCUM_AFTER:  x_m <- fold(x);  acc_m <- rk_accum_point(acc_m, fold, ch)
+//                      (Smooth K_m, then uout += c_m h K_m)
+//   FUSE_ACCUM_BEFORE: x_m <- fold(rk_accum_point(x_m, K_m, ch))
+//                      (uout += c h K, then Smooth uout)
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256)
+    k_dss_rk_csr(T *__restrict__ x, const int32_t *__restrict__ ptr,
+                 const int32_t *__restrict__ mem, int64_t nclass, T dt, const T *__restrict__ uin,
+                 T a, const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2,
+                 T *__restrict__ acc_out, const T *__restrict__ K, T ch) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nclass;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t b0 = ptr[c], e0 = ptr[c + 1];
+    T acc = T(0);
+    for (int32_t k = b0; k < e0; k++) {
+      const int64_t m = mem[k];
+      T v = x[m];
+      if (MODE == FUSE_EULER) v = rk_euler_point(v, dt, uin[m], a, y, b, a2, y2, b2, m);
+      if (MODE == FUSE_ACCUM_BEFORE) v = rk_accum_point(v, K[m], ch);
+      acc = __fadd_rn_t(acc, v);
+    }
+    acc = acc / (T)(e0 - b0);
+    for (int32_t k = b0; k < e0; k++) {
+      const int64_t m = mem[k];
+      x[m] = acc;
+      if (MODE == FUSE_ACCUM_AFTER) acc_out[m] = rk_accum_point(acc_out[m], acc, ch);
+    }
+  }
+}
+
 }  // namespace gfk

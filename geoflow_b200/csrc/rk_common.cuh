@@ -33,6 +33,10 @@ struct Stepper {
   // GMTK::constrain2sphere on the state where step_b calls it, on embedded
   // surfaces with node coordinates and a state of >= 3 components
   void constrain(T *const *u);
+  // Smooth fused with the stage update before or after it
+  void euler_smooth(T *x, T dt, const T *uin, T a, const T *y, T b, T a2, const T *y2, T b2);
+  void smooth_accum(T *K, T ch, T *uout);
+  void accum_smooth(T *uout, const T *K, T ch);
   // One step uin -> uout.  With a tape (pointers tape[3*m + k], m = 0 ..
   // stages-1), stage m's input state (the argument of its RHS call) is left
   // in tape[3*m + k] for the adjoint sweep.
