@@ -3,10 +3,10 @@
 The compute lives in libgfgpu.so (C ABI, include/gfgpu.h); this package is
 the Python host-side mirror of the reference interfaces over that ABI.
 """
-from . import _abi
+from . import _abi, gio
 from ._abi import GFError, load
 from .sem import (CGTraits, Context, GBurgers, GCG, GGFX, GHelmholtz, GMass, Graph, GridBox,
                   Problem, gll_basis)
 
 __all__ = ["GFError", "load", "CGTraits", "Context", "GBurgers", "GCG", "GGFX", "GHelmholtz",
-           "GMass", "Graph", "GridBox", "Problem", "gll_basis", "_abi"]
+           "GMass", "Graph", "GridBox", "Problem", "gll_basis", "_abi", "gio"]

@@ -19,7 +19,7 @@ P_void = C.POINTER(C.c_void_p)
 GF_OK = 0
 GF_CG_NOCONVERGE, GF_CG_SOLVE, GF_CG_PRECOND, GF_CG_BADITERNUM = 1, 2, 3, 4
 GF_ERR_ARG, GF_ERR_CUDA, GF_ERR_UNSUPPORTED, GF_ERR_NOMEM = -1, -2, -3, -4
-GF_ERR_NONFINITE, GF_ERR_WATCHDOG = -5, -6
+GF_ERR_NONFINITE, GF_ERR_WATCHDOG, GF_ERR_IO = -5, -6, -7
 # enums
 GF_F64, GF_F32 = 0, 1
 GF_DSS_SUM, GF_DSS_SMOOTH, GF_DSS_MAX, GF_DSS_MIN = 0, 1, 2, 3
@@ -55,6 +55,15 @@ class CGTraits(C.Structure):
 
 class RKTraits(C.Structure):
     _fields_ = [("eqn", c_int), ("nu", c_double), ("nstate", c_int), ("scheme", c_int)]
+
+
+class GioHeader(C.Structure):
+    _fields_ = [
+        ("ivers", c_int), ("dim", c_int), ("nelems", C.c_uint64), ("gtype", c_int),
+        ("cycle", C.c_uint64), ("time", c_double), ("multivar", c_int),
+        ("float_bytes", c_int), ("header_bytes", C.c_uint64), ("ndata", C.c_uint64),
+        ("porder_rows", c_int64),
+    ]
 
 
 # name -> (restype, argtypes); every symbol declared in include/gfgpu.h
@@ -101,6 +110,19 @@ SIGNATURES = {
                                 c_void_p]),
     "gf_rk_graph_create": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
                                    c_int, P_void]),
+    "gf_gio_header_bytes": (c_int64, [c_int, c_int, C.c_uint64, c_int]),
+    "gf_gio_write": (c_int, [c_void_p, C.c_char_p, C.POINTER(GioHeader), c_void_p, c_void_p,
+                             c_int, c_void_p, C.c_uint64]),
+    "gf_gio_write_header": (c_int, [c_void_p, C.c_char_p, C.POINTER(GioHeader), c_void_p,
+                                    c_void_p, c_int]),
+    "gf_gio_write_data": (c_int, [c_void_p, C.c_char_p, c_int, c_void_p, C.c_uint64,
+                                  C.c_uint64]),
+    "gf_gio_read_data": (c_int, [c_void_p, C.c_char_p, c_int, c_void_p, C.c_uint64,
+                                 C.c_uint64]),
+    "gf_gio_read_header": (c_int, [c_void_p, C.c_char_p, c_int, C.POINTER(GioHeader), c_void_p,
+                                   c_int64, c_void_p, c_int64]),
+    "gf_gio_read": (c_int, [c_void_p, C.c_char_p, c_int, c_void_p, C.c_uint64,
+                            C.POINTER(GioHeader)]),
     "gf_graph_ensemble": (c_int, [c_int, P_void, P_void]),
     "gf_graph_launch": (c_int, [c_void_p]),
     "gf_graph_nodes": (c_int, [c_void_p]),

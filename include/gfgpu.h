@@ -43,7 +43,8 @@ enum {
   GF_ERR_UNSUPPORTED = -3,
   GF_ERR_NOMEM = -4,
   GF_ERR_NONFINITE = -5,
-  GF_ERR_WATCHDOG = -6
+  GF_ERR_WATCHDOG = -6,
+  GF_ERR_IO = -7
 };
 
 /* ---- enumerations ---- */
@@ -275,6 +276,56 @@ int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
 #define GF_NOALLOC_MAX_BLOCKS 32768
 int gf_integrate_noalloc(int64_t n, const double *mass, const double *u, double *result,
                          void *stream);
+
+/* ---- GIO state files (io/gio.ipp POSIX format) ----
+ * One field of one rank per file: the GIO header (io/gio.ipp:459-503)
+ * followed by the field's values, straight from / into device memory
+ * through pinned double-buffered staging.  Ftype is the dtype (GF_F64:
+ * double, GF_F32: float); the header's time is stored as Ftype. */
+typedef struct {
+  int ivers;             /* 0: one porder row for all elements, else one per element */
+  int dim;
+  uint64_t nelems;
+  int gtype;             /* GElemType: 0 GE_REGULAR, 1 GE_DEFORMED, 2 GE_2DEMBEDDED */
+  uint64_t cycle;
+  double time;
+  int multivar;
+  /* filled by the readers */
+  int float_bytes;       /* sizeof(Ftype) */
+  uint64_t header_bytes; /* GIO::sz_header (io/gio.ipp:676-690) */
+  uint64_t ndata;        /* Ftype values after the header (io/gio.ipp:416-429) */
+  int64_t porder_rows;   /* 1 if ivers == 0, else nelems */
+} gf_gio_header;
+/* Header size in bytes for dtype's Ftype, or GF_ERR_ARG. */
+int64_t gf_gio_header_bytes(int ivers, int dim, uint64_t nelems, int dtype);
+/* The header alone, creating (truncating) path; GIO::write_header_posix
+ * (io/gio.ipp:459-503).  ctx may be NULL. */
+int gf_gio_write_header(gf_ctx_t ctx, const char *path, const gf_gio_header *h,
+                        const int *porder, const uint64_t *elemids, int dtype);
+/* n values of device memory u into the existing file path at byte offset
+ * (no truncation): one rank's slab of a collective file
+ * (GIO::write_coll, io/gio.ipp:735-790) or the data of a POSIX file. */
+int gf_gio_write_data(gf_ctx_t ctx, const char *path, int dtype, const void *u, uint64_t n,
+                      uint64_t offset);
+/* n values from byte offset of path into device memory u (GIO::read_coll's
+ * slab read, io/gio.ipp:806-860). */
+int gf_gio_read_data(gf_ctx_t ctx, const char *path, int dtype, void *u, uint64_t n,
+                     uint64_t offset);
+/* GIO::write_posix (io/gio.ipp:347-377): porder is porder_rows x dim
+ * int32, elemids nelems keys (NULL: all 0, as GGridBox leaves them); n must
+ * equal the count the orders give. */
+int gf_gio_write(gf_ctx_t ctx, const char *path, const gf_gio_header *h, const int *porder,
+                 const uint64_t *elemids, int dtype, const void *u, uint64_t n);
+/* GIO::read_header (io/gio.ipp:587-660).  dtype -1 infers Ftype from the
+ * file size.  porder / elemids may be NULL; else they need porder_rows*dim
+ * and nelems entries (caps checked).  ctx may be NULL (no device is
+ * touched; messages then go to stderr). */
+int gf_gio_read_header(gf_ctx_t ctx, const char *path, int dtype, gf_gio_header *h, int *porder,
+                       int64_t porder_cap, uint64_t *elemids, int64_t elemids_cap);
+/* GIO::read_posix (io/gio.ipp:392-444): reads the n values into device
+ * memory u; n must equal the header's count.  hout may be NULL. */
+int gf_gio_read(gf_ctx_t ctx, const char *path, int dtype, void *u, uint64_t n,
+                gf_gio_header *hout);
 
 /* ---- CUDA graphs (no reference counterpart) ---- */
 /* Records nsteps RK steps of gf_rk_advance (same arguments, same result)
