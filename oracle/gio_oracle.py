@@ -11,9 +11,12 @@ product never imports it.  Follows GeoFLOW src/cdg/io/gio.ipp:
   - collective layout: init (100-128, each rank's slab at the prefix sum of
     the ranks' ndof) and write_coll (735-790, component j of a multivar file
     at header + j * global ndof * sizeof(Ftype)).
-Parity is pinned to the reference's own byte layout read from those lines:
-the reference's writer cannot produce a golden file (write_posix reopens the
-file with "wb" after the header, gio.ipp:356-359, which truncates it).
+Parity is pinned to the reference's own byte layout read from those lines,
+and to the header fields the reference's Python reader
+(analysis/python/g2vtk:158-195) parses from files of this layout
+(tests/golden/gio_g2vtk.json).  The reference's writer cannot produce a
+golden file (write_posix reopens the file with "wb" after the header,
+gio.ipp:356-359, which truncates it).
 """
 from __future__ import annotations
 

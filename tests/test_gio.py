@@ -110,6 +110,41 @@ def test_read_header_rejects_bad_files(tmp_path):
                                   small.ctypes.data_as(C.c_void_p), 1) == A.GF_ERR_ARG
 
 
+def test_files_match_reference_g2vtk_reader(tmp_path):
+    """Pins: files of the oracle's layout, and the header fields the
+    reference's own Python reader (analysis/python/g2vtk) parsed from them
+    (tests/golden/make_gio_golden.py).  The library writes the same bytes
+    and parses the same fields.  g2vtk stops after `time` (it predates the
+    multivar flag and element keys of gio.ipp:489-496): its data offset is
+    that of the multivar field."""
+    import json
+    from pathlib import Path
+    golden = json.loads((Path(__file__).parent / "golden" / "gio_g2vtk.json").read_text())
+    lib = A.load()
+    for g in golden:
+        dim, ne, p, fb, gtype, cycle, time = g["case"]
+        raw = bytes.fromhex(g["file_hex"])
+        hbytes = GO.header_bytes(0, dim, ne, fb)
+        h, porder = _hdr(0, dim, ne, p, gtype=gtype, cycle=cycle, time=time)
+        ids = np.arange(ne, dtype=np.uint64) * 11 + 5
+        path = str(tmp_path / "g.out")
+        dt = A.GF_F64 if fb == 8 else A.GF_F32
+        assert lib.gf_gio_write_header(None, path.encode(), C.byref(h),
+                                       porder.ctypes.data_as(C.c_void_p),
+                                       ids.ctypes.data_as(C.c_void_p), dt) == 0
+        assert open(path, "rb").read() == raw[:hbytes]
+        open(path, "wb").write(raw)
+        r = A.GioHeader()
+        po = np.zeros(dim, np.int32)
+        assert lib.gf_gio_read_header(None, path.encode(), -1, C.byref(r),
+                                      po.ctypes.data_as(C.c_void_p), dim, None, 0) == 0
+        ref = g["g2vtk"]
+        assert (r.ivers, r.dim, r.nelems, list(po), r.gtype, r.cycle, r.time) == (
+            ref["vers"], ref["dim"], ref["nelems"], ref["porder"], ref["gtype"], ref["cycle"],
+            ref["time"])
+        assert r.float_bytes == fb and ref["skip"] == hbytes - 4 - 8 * ne
+
+
 class _Grid:
     def __init__(self, dim, nelems, p):
         self.dim, self.p, self.n, self.nelems = dim, p, p + 1, nelems
