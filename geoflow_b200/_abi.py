@@ -24,7 +24,7 @@ GF_ERR_NONFINITE, GF_ERR_WATCHDOG, GF_ERR_IO = -5, -6, -7
 GF_F64, GF_F32 = 0, 1
 GF_DSS_SUM, GF_DSS_SMOOTH, GF_DSS_MAX, GF_DSS_MIN = 0, 1, 2, 3
 GF_NORM_INF, GF_NORM_EUC, GF_NORM_L2, GF_NORM_L1 = 0, 1, 2, 3
-GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV = 0, 1, 2
+GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV, GF_PRECOND_PMG = 0, 1, 2, 3
 GF_CG_FP64, GF_CG_MIXED = 0, 1
 GF_GEOM_AFFINE, GF_GEOM_REGULAR, GF_GEOM_DEFORMED, GF_GEOM_EMBEDDED = 0, 1, 2, 3
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2

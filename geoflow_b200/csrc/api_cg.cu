@@ -621,6 +621,28 @@ __device__ __forceinline__ void fcg_finish(double rz, double zq, double *scal, d
   }
 }
 
+// Fletcher-Reeves form for the multigrid preconditioner (a fixed symmetric
+// operator up to FP32 rounding): beta = <r, z> / <r_old, z_old>.
+__device__ __forceinline__ void fcg_finish_fr(double rz, double *scal, double *partials,
+                                              unsigned int *counter, double *sh) {
+  double pv[1] = {rz};
+  if (publish_partials<1>(pv, partials, counter, gridDim.x)) {
+    const double rz_t = fold_partials<false>(partials, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      const double beta = scal[S_FIRST] != 0.0 ? 0.0 : rz_t / scal[S_ZR];
+      scal[S_BETA] = beta;
+      scal[S_ZR] = rz_t;
+      scal[S_RHO] = rz_t;
+      scal[S_FIRST] = 0.0;
+      if (!isfinite(beta) || !isfinite(rz_t) || !(rz_t > 0.0)) {
+        scal[S_FLAG] = 1.0;
+        scal[S_DONE] = 2.0;
+      }
+      *counter = 0;
+    }
+  }
+}
+
 // res = (float) r, d = z = dinv res / theta  (last: also the FCG scalars)
 __global__ void __launch_bounds__(RED_THREADS)
     k_cheb_init(int64_t nL, const double *__restrict__ r, const float *__restrict__ dinv, float c0,
@@ -750,6 +772,219 @@ __global__ void k_invert(int64_t n, const double *__restrict__ d, double *__rest
   }
 }
 
+// ---- multigrid preconditioner kernels (FP32, lattice L-vectors) ----
+// Transfers between the lattices of two levels are tensor products of 1-d
+// operators, P = P_z (x) P_y (x) P_x: a fine lattice point takes the
+// coarse element's GLL interpolant at its position, and the restriction
+// is P^T.  Each is applied one direction at a time.
+
+// 1-d operator along direction d as CSR rows (row = output coordinate)
+struct Line1D {
+  const int32_t *ptr = nullptr, *col = nullptr;
+  const float *val = nullptr;
+};
+
+// out(g) = sum_k val[k] in(g with g_d = col[k]); in and out are lattices
+// of extents ei and eo that differ only in direction d.
+// mode 0: out = s; 1: out += s; 2: out = mask ? s : 0 (mask of the output)
+__global__ void k_line1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1, Line1D T,
+                         const float *__restrict__ in, float *__restrict__ out,
+                         const uint8_t *__restrict__ mask, int mode, const double *stop) {
+  if (stop && *stop != 0.0) return;
+  GRID_STRIDE(o, nout) {
+    const int g0 = (int)(o % eo0);
+    const int64_t rr = o / eo0;
+    const int g1 = (int)(rr % eo1), g2 = (int)(rr / eo1);
+    int64_t base, stride;
+    int gd;
+    if (d == 0) {
+      gd = g0;
+      base = (int64_t)ei0 * (g1 + (int64_t)ei1 * g2);
+      stride = 1;
+    } else if (d == 1) {
+      gd = g1;
+      base = g0 + (int64_t)ei0 * ei1 * g2;
+      stride = ei0;
+    } else {
+      gd = g2;
+      base = g0 + (int64_t)ei0 * g1;
+      stride = (int64_t)ei0 * ei1;
+    }
+    float s = 0.0f;
+    for (int k = T.ptr[gd]; k < T.ptr[gd + 1]; k++)
+      s = fmaf(T.val[k], in[base + (int64_t)T.col[k] * stride], s);
+    if (mode == 2 && mask && !mask[o]) s = 0.0f;
+    if (mode == 1) out[o] += s;
+    else out[o] = s;
+  }
+}
+
+// Chebyshev smoothing of A x = b from x = 0 (the recurrence of k_cheb_*):
+// res = b, d = c0 Dinv res, x = d.  With r64 the level's b is first taken
+// from the FP64 outer residual.
+__global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, float *__restrict__ b,
+                           const float *__restrict__ dinv, float c0, float *__restrict__ res,
+                           float *__restrict__ d, float *__restrict__ x, const double *stop) {
+  if (stop && *stop != 0.0) return;
+  GRID_STRIDE(c, nL) {
+    const float bc = r64 ? (float)r64[c] : b[c];
+    if (r64) b[c] = bc;
+    res[c] = bc;
+    const float dc = c0 * (dinv[c] * bc);
+    d[c] = dc;
+    x[c] = dc;
+  }
+}
+
+// Passes that fold the element-local qE into the lattice (s = mask * sum
+// of copies) and update the smoother state:
+//   MG_STEP     qE = A d:  res -= s; d = c1 d + c2 Dinv res; x += d
+//   MG_RESID    qE = A d:  res -= s                (res = b - A x after a smoothing)
+//   MG_RESTART  qE = A x:  res = b - s; d = c1 Dinv res; x += d
+//                          (smoothing of the residual equation from an existing x)
+// DOTS (last pass of the finest level): <b, x> (b = the FP32 copy of the
+// outer residual) for the CG step, finished by fcg_finish_fr.
+enum { MG_STEP = 0, MG_RESID = 1, MG_RESTART = 2 };
+
+// The passes run on the box lattice, one thread per lattice point in
+// lattice order: the state vectors stream fully coalesced (a warp reads 128
+// contiguous bytes of each), and a point's element copies are gathered
+// from qE, where the copies of one element row are one aligned 32-byte
+// sector shared by the warp's neighbouring points.  Copies are added in
+// ascending element id.  Lattice and element-local sizes are below 2^31
+// (checked when the problem is created).
+template <int P>
+__device__ __forceinline__ int lattice_cands(int g, int ne, int per, int (&ec)[2], int (&l)[2]) {
+  const int q = g / P, r = g - q * P;
+  if (r != 0) {
+    ec[0] = q;
+    l[0] = r;
+    return 1;
+  }
+  if (per) {  // (q-1, P) and (q, 0), wrapping; one element twice when ne == 1
+    if (q == 0) {
+      ec[0] = 0;
+      l[0] = 0;
+      ec[1] = ne - 1;
+      l[1] = P;
+    } else {
+      ec[0] = q - 1;
+      l[0] = P;
+      ec[1] = q;
+      l[1] = 0;
+    }
+    return 2;
+  }
+  int k = 0;
+  if (q >= 1) {
+    ec[k] = q - 1;
+    l[k++] = P;
+  }
+  if (q < ne) {
+    ec[k] = q;
+    l[k++] = 0;
+  }
+  return k;
+}
+
+// sum of the element copies of lattice point c (ascending element id)
+template <int N>
+__device__ __forceinline__ float lattice_fold(const MapBox<N> &map, const float *__restrict__ qE,
+                                              int c, int M0, int M1, bool d3) {
+  constexpr int P = N - 1, NN = N * N;
+  const int nn = d3 ? NN * N : NN;
+  const int ne0 = map.ne[0], ne1 = map.ne[1];
+  const int row = c / M0, g0 = c - row * M0;
+  const int g1 = row % M1, g2 = row / M1;
+  int ex[2], lx[2], ey[2], ly[2], ez[2] = {0, 0}, lz[2] = {0, 0};
+  const int nx = lattice_cands<P>(g0, ne0, map.per[0], ex, lx);
+  const int ny = lattice_cands<P>(g1, ne1, map.per[1], ey, ly);
+  const int nz = d3 ? lattice_cands<P>(g2, map.ne[2], map.per[2], ez, lz) : 1;
+  float s = 0.0f;
+  for (int az = 0; az < nz; az++)
+    for (int ay = 0; ay < ny; ay++) {
+      const int eyz = ne0 * (ey[ay] + ne1 * ez[az]);
+      const int off = N * ly[ay] + NN * lz[az];
+      for (int ax = 0; ax < nx; ax++)
+        s = __fadd_rn(s, qE[(int64_t)(ex[ax] + eyz) * nn + off + lx[ax]]);
+    }
+  return s;
+}
+
+// One thread per lattice point in lattice order: consecutive threads take
+// consecutive points, so the state vectors stream coalesced and a warp's
+// copies of one element row share one sector.  (Measured on B200: giving a
+// thread several points, consecutive or a grid stride apart, was slower.)
+template <int N, int MODE, bool DOTS>
+__global__ void __launch_bounds__(RED_THREADS)
+    k_mg_pass_lat(MapBox<N> map, Weights wt, const float *__restrict__ qE,
+                  const float *__restrict__ b, const float *__restrict__ dinv, float c1, float c2,
+                  float *__restrict__ res, float *__restrict__ d, float *__restrict__ x,
+                  double *scal, double *partials, unsigned int *counter) {
+  __shared__ double sh[32];
+  if (scal[S_DONE] != 0.0) return;
+  double rz = 0.0;
+  const bool d3 = map.dim > 2;
+  const int M0 = (int)map.M[0], M1 = (int)map.M[1];
+  const int nL = M0 * M1 * (d3 ? (int)map.M[2] : 1);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nL; c += gridDim.x * blockDim.x) {
+    float s = lattice_fold<N>(map, qE, c, M0, M1, d3);
+    if (wt.maskL && !wt.maskL[c]) s = 0.0f;
+    if (MODE == MG_RESID) {
+      res[c] = res[c] - s;
+      continue;
+    }
+    float rc, dc;
+    if (MODE == MG_STEP) {
+      rc = res[c] - s;
+      dc = c1 * d[c] + c2 * (dinv[c] * rc);
+    } else {
+      rc = b[c] - s;
+      dc = c1 * (dinv[c] * rc);
+    }
+    const float xc = x[c] + dc;
+    x[c] = xc;
+    res[c] = rc;
+    d[c] = dc;
+    if (DOTS) rz += (double)b[c] * (double)xc;
+  }
+  if (!DOTS) return;
+  rz = block_reduce<false>(rz, sh);
+  fcg_finish_fr(rz, scal, partials, counter, sh);
+}
+
+// deterministic pseudo-random vector in [-1, 1) (zero where masked): the
+// start of the eigenvalue estimates
+__global__ void k_fill_hash(int64_t n, const uint8_t *__restrict__ mask, double *__restrict__ v) {
+  GRID_STRIDE(i, n) {
+    uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const double u = (double)(h >> 11) * (1.0 / 9007199254740992.0);
+    v[i] = (mask && !mask[i]) ? 0.0 : 2.0 * u - 1.0;
+  }
+}
+
+// coarsest-level solve x[free_i] = sum_j Ainv(i, j) b[free_j]: one block
+// per row (the masked points of x stay 0)
+__global__ void __launch_bounds__(128)
+    k_dense_solve(int64_t nfree, const float *__restrict__ ainv, const int32_t *__restrict__ idx,
+                  const float *__restrict__ b, float *__restrict__ x, const double *stop) {
+  if (stop && *stop != 0.0) return;
+  __shared__ float sh[4];
+  for (int64_t i = blockIdx.x; i < nfree; i += gridDim.x) {
+    const float *row = ainv + i * nfree;
+    float s = 0.0f;
+    for (int64_t j = threadIdx.x; j < nfree; j += blockDim.x) s = fmaf(row[j], b[idx[j]], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) x[idx[i]] = (sh[0] + sh[1]) + (sh[2] + sh[3]);
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------
 // Largest eigenvalue of the Lanczos tridiagonal built from n PCG steps
 // (alpha_j, beta_j = rho_{j+1}/rho_j): T_jj = 1/alpha_j + beta_{j-1}/alpha_{j-1},
@@ -786,6 +1021,17 @@ double lanczos_max(const double *ab, int n) {
   }
   return hi;
 }
+
+template <class MAP>
+struct Solver;
+// multigrid preconditioner (defined after Solver): set-up or reuse of the
+// hierarchy, and the FP64 flexible CG that applies it
+template <class MAP>
+int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass);
+template <class MAP>
+int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass,
+             const double *bL, double *xL, double *rL, double *qE, double *hist, int *total,
+             double *rn);
 
 template <class MAP>
 struct Solver {
@@ -1075,7 +1321,13 @@ struct Solver {
     if (!bL || !xL || !rL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
     double *d64 = nullptr;
     float *d32 = nullptr;
-    if (tr.precond != GF_PRECOND_NONE) {
+    if (tr.precond == GF_PRECOND_PMG) {
+      // the hierarchy's set-up runs its own short solves on this problem's
+      // scalar block and work slots, so it comes before the solve's state
+      int rc = mg_prepare(*this, tr, p, q, use_mass);
+      if (rc) return rc;
+    }
+    if (tr.precond != GF_PRECOND_NONE && tr.precond != GF_PRECOND_PMG) {
       int rc = jacobi(p, q, use_mass, &d64, &d32);
       if (rc) return gf_fail(ctx, rc, "Jacobi set-up failed");
     }
@@ -1093,6 +1345,9 @@ struct Solver {
     double rn = 0.0;
     if (tr.precond == GF_PRECOND_CHEBYSHEV) {
       rc = solve_poly(tr, p, q, use_mass, bL, xL, rL, qE, d64, d32, hist, &total, &rn);
+      if (rc < 0) return rc;
+    } else if (tr.precond == GF_PRECOND_PMG) {
+      rc = solve_mg(*this, tr, p, q, use_mass, bL, xL, rL, qE, hist, &total, &rn);
       if (rc < 0) return rc;
     } else if (tr.precision == GF_CG_FP64) {
       double *w = (double *)gf_work(prob, 4, sizeof(double) * nL);
@@ -1184,6 +1439,796 @@ struct Solver {
   }
 };
 
+// ---------------------------------------------------------------------
+// p/h multigrid preconditioner for structured affine boxes.
+//
+// Levels: the problem's own order p, then p/2, p/4, ... down to 1 on the
+// same elements, then the p = 1 box with the element counts halved while
+// they stay even and >= 2.  Each coarser level is the same SEM Helmholtz
+// operator rediscretised (GLL quadrature of its order, element geometry
+// merged under h-coarsening), held as a light gf_problem: basis, K1,
+// element geometry and box lattice, no gather-scatter arrays.  One V-cycle
+// in FP32 on the lattice (unique-node) vectors:
+//   x = S b;  r = b - A x;  x_c = V(R r);  x += P x_c;  x += S (b - A x)
+// S = Chebyshev-Jacobi polynomial of degree m on [lmax/ratio, 1.1 lmax]
+// (the same polynomial before and after, so the cycle is symmetric), R =
+// P^T with the coarse mask, and on the coarsest level a higher-degree
+// Chebyshev solve.  2m + 2 applies of each level's operator per cycle.
+
+// h-coarsening stops at a level with at most MG_DENSE_SMALL free lattice
+// points; a coarsest level with at most MG_DENSE_MAX is solved exactly
+// with a dense inverse (one kernel), a larger one with a Chebyshev solve.
+constexpr int64_t MG_DENSE_SMALL = 512, MG_DENSE_MAX = 729;
+
+struct MGLevelBase {
+  gf_problem *prob = nullptr;
+  bool owned = false;
+  int dim = 3;
+  int64_t nL = 0, nE = 0;
+  int M[3] = {1, 1, 1};
+  float *dinv = nullptr, *b = nullptr, *x = nullptr, *res = nullptr, *d = nullptr, *qE = nullptr;
+  const uint8_t *maskL = nullptr;  // lattice Dirichlet mask (null: none)
+  int m = 0;  // smoothing degree (the coarsest level: its solve degree)
+  float c0 = 0.0f;
+  std::vector<float> c1, c2;
+  double lmax = 0.0;
+  // coarsest level: x = Ainv b on the free lattice points (dense inverse)
+  int64_t nfree = 0;
+  const float *ainv = nullptr;
+  const int32_t *free_idx = nullptr;
+  // transfer to the next coarser level
+  Line1D P[3], PT[3];
+  float *t1 = nullptr, *t2 = nullptr;
+  std::vector<void *> mem;
+  float *alloc_f(int64_t n) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(float) * std::max<int64_t>(n, 1)) != cudaSuccess) return nullptr;
+    mem.push_back(p);
+    return (float *)p;
+  }
+  template <typename V>
+  V *upload(const std::vector<V> &h) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(V) * std::max<size_t>(h.size(), 1)) != cudaSuccess) return nullptr;
+    mem.push_back(p);
+    cudaMemcpy(p, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice);
+    return (V *)p;
+  }
+  virtual ~MGLevelBase() {
+    for (void *p : mem) cudaFree(p);
+    if (owned && prob) gf_problem_destroy(prob);
+  }
+  virtual int apply(const float *in, double p, double q, int use_mass, const double *stop,
+                    cudaStream_t st) = 0;
+  virtual void pass(int mode, bool dots, float a1, float a2, gf_problem *outer,
+                    cudaStream_t st) = 0;
+  virtual int jacobi(double p, double q, int use_mass) = 0;
+  virtual int estimate(double p, double q, int use_mass, int64_t nfree) = 0;
+};
+
+template <int N>
+struct MGLevel : MGLevelBase {
+  Solver<MapBox<N>> S;
+  MGLevel(gf_problem *lp, bool own, bool masked) : S(lp, MapBox<N>::make(lp->box), masked) {
+    prob = lp;
+    owned = own;
+    dim = lp->dim;
+    nL = lp->nclass;
+    nE = lp->nlocal;
+    for (int k = 0; k < 3; k++) M[k] = (int)lp->box.M[k];
+    maskL = S.wt.maskL;
+  }
+  int apply(const float *in, double p, double q, int use_mass, const double *stop,
+            cudaStream_t st) override {
+    return launch_helm_L<float>(prob, (float)p, (float)q, use_mass, in, qE, st, stop);
+  }
+  template <int MODE, bool DOTS>
+  void run_pass(float a1, float a2, gf_problem *outer, cudaStream_t st) {
+    auto kern = k_mg_pass_lat<N, MODE, DOTS>;
+    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, S.wt, qE, b, dinv, a1, a2, res, d, x,
+                                                 outer->scal_d, outer->partials, outer->counter);
+  }
+  void pass(int mode, bool dots, float a1, float a2, gf_problem *outer,
+            cudaStream_t st) override {
+    outer->launches++;
+    if (mode == MG_RESID) run_pass<MG_RESID, false>(a1, a2, outer, st);
+    else if (mode == MG_STEP && dots) run_pass<MG_STEP, true>(a1, a2, outer, st);
+    else if (mode == MG_STEP) run_pass<MG_STEP, false>(a1, a2, outer, st);
+    else if (dots) run_pass<MG_RESTART, true>(a1, a2, outer, st);
+    else run_pass<MG_RESTART, false>(a1, a2, outer, st);
+  }
+  int jacobi(double p, double q, int use_mass) override {
+    double *d64 = nullptr;
+    float *d32 = nullptr;
+    int rc = S.jacobi(p, q, use_mass, &d64, &d32);
+    if (rc) return rc;
+    return cudaMemcpyAsync(dinv, d32, sizeof(float) * nL, cudaMemcpyDeviceToDevice, S.st) ==
+                   cudaSuccess
+               ? GF_OK
+               : GF_ERR_CUDA;
+  }
+  // Largest eigenvalue of Dinv A: Lanczos Ritz value from min(12, nfree)
+  // FP32 PCG steps on a pseudo-random right-hand side.  Runs on the level
+  // problem's own scalar block and work slots (set-up only).
+  int estimate(double p, double q, int use_mass, int64_t nfree) override {
+    const int K = (int)std::min<int64_t>(12, std::max<int64_t>(nfree, 1));
+    gf_cg_traits tr{};
+    tr.maxit = K;
+    tr.normtype = GF_NORM_INF;
+    tr.tol = 1e-300;
+    tr.check_every = K;
+    tr.precision = GF_CG_FP64;
+    S.set_scalars(tr, K, false);
+    gf_problem *lp = prob;
+    cudaMemcpyAsync(lp->scal_d, lp->scal_h, sizeof(double) * S_COUNT, cudaMemcpyHostToDevice, S.st);
+    double *bL = (double *)gf_work(lp, 0, sizeof(double) * nL);
+    double *xL = (double *)gf_work(lp, 1, sizeof(double) * nL);
+    double *rL = (double *)gf_work(lp, 2, sizeof(double) * nL);
+    double *qE64 = (double *)gf_work(lp, 3, sizeof(double) * nE);
+    float *r32 = (float *)gf_work(lp, 11, sizeof(float) * nL);
+    float *w32 = (float *)gf_work(lp, 12, sizeof(float) * nL);
+    float *x32 = (float *)gf_work(lp, 13, sizeof(float) * nL);
+    float *q32 = (float *)gf_work(lp, 14, sizeof(float) * nL);
+    float *qE32 = (float *)gf_work(lp, 15, sizeof(float) * nE);
+    double *abd = (double *)gf_work(lp, 17, sizeof(double) * 2 * K);
+    if (!bL || !xL || !rL || !qE64 || !r32 || !w32 || !x32 || !q32 || !qE32 || !abd)
+      return GF_ERR_NOMEM;
+    k_fill_hash<<<S.gL, 256, 0, S.st>>>(nL, S.wt.maskL, bL);
+    cudaMemsetAsync(xL, 0, sizeof(double) * nL, S.st);
+    cudaMemsetAsync(x32, 0, sizeof(float) * nL, S.st);
+    int rc = S.template residual<float>(p, q, use_mass, bL, xL, qE64, rL, r32, w32, dinv, 0, 1e-300);
+    if (rc) return rc;
+    int its = 0;
+    S.ab = abd;
+    S.nab = K;
+    rc = S.template iterate<float>(tr, K, p, q, use_mass, x32, r32, w32, q32, qE32, dinv, nullptr,
+                                   &its);
+    S.ab = nullptr;
+    S.nab = 0;
+    if (rc) return rc;
+    std::vector<double> ab(2 * (size_t)std::max(its, 1));
+    if (its > 0 && cudaMemcpy(ab.data(), abd, sizeof(double) * 2 * its, cudaMemcpyDeviceToHost) !=
+                       cudaSuccess)
+      return GF_ERR_CUDA;
+    lmax = its > 0 ? lanczos_max(ab.data(), its) : 0.0;
+    return lmax > 0.0 ? GF_OK : GF_ERR_NONFINITE;
+  }
+};
+
+template <int N>
+struct MakeLevel {
+  static int run(gf_problem *lp, bool own, bool masked, MGLevelBase **out) {
+    *out = new MGLevel<N>(lp, own, masked);
+    return GF_OK;
+  }
+};
+
+struct MGHier {
+  std::vector<MGLevelBase *> lv;
+  double key[6] = {0, 0, 0, 0, 0, 0};
+  // CUDA graph of one batch of CG iterations (captured on the first solve
+  // with these vectors and replayed by later batches and solves)
+  cudaStream_t cs = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *gkey[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int gevery = 0;
+  uint64_t glaunches = 0;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  ~MGHier() {
+    drop_graph();
+    if (cs) cudaStreamDestroy(cs);
+    for (auto *l : lv) delete l;
+  }
+};
+
+void mg_free(void *h) { delete (MGHier *)h; }
+
+// A coarser level as a light problem: what the affine K1 apply, the
+// Jacobi diagonal and the lattice assembly read.
+int mg_light_problem(gf_context *ctx, int dim, const int (&ne)[3], const int (&per)[3], int p,
+                     const std::vector<double> &eg, bool masked, gf_problem **out) {
+  const int n = p + 1;
+  gf_problem *lp = new gf_problem();
+  lp->ctx = ctx;
+  ctx->nprob++;
+  lp->dim = dim;
+  lp->n = n;
+  lp->geom = GF_GEOM_AFFINE;
+  lp->volume = 1.0;
+  int64_t nel = 1, nn = 1;
+  for (int k = 0; k < dim; k++) {
+    nel *= ne[k];
+    nn *= n;
+  }
+  lp->ne = nel;
+  lp->nlocal = nel * nn;
+  std::vector<double> xi(n);
+  gf_gll_basis(p, xi.data(), lp->W, lp->D);
+  gfk::gf_k1_matrix(n, lp->D, lp->W, lp->K1);
+  BoxLattice L{};
+  L.dim = dim;
+  L.p = p;
+  for (int k = 0; k < 3; k++) {
+    L.ne[k] = k < dim ? ne[k] : 1;
+    L.per[k] = k < dim ? per[k] : 0;
+    L.M[k] = k < dim ? (int64_t)L.ne[k] * p + (L.per[k] ? 0 : 1) : 1;
+  }
+  lp->box = L;
+  lp->has_box = true;
+  lp->nclass = L.size();
+  auto up = [](const void *h, size_t bytes) -> void * {
+    void *d = nullptr;
+    if (cudaMalloc(&d, std::max<size_t>(bytes, 1)) != cudaSuccess) return nullptr;
+    cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice);
+    return d;
+  };
+  std::vector<float> egf(eg.begin(), eg.end());
+  lp->egeom_d = (double *)up(eg.data(), sizeof(double) * eg.size());
+  lp->egeom_f = (float *)up(egf.data(), sizeof(float) * egf.size());
+  if (masked) {  // Dirichlet on the non-periodic box faces
+    std::vector<uint8_t> mk((size_t)lp->nclass, 1);
+    for (int64_t c = 0; c < lp->nclass; c++) {
+      int64_t r = c;
+      for (int k = 0; k < dim; k++) {
+        const int64_t g = r % L.M[k];
+        r /= L.M[k];
+        if (!L.per[k] && (g == 0 || g == L.M[k] - 1)) mk[c] = 0;
+      }
+    }
+    lp->maskL8 = (uint8_t *)up(mk.data(), mk.size());
+  }
+  lp->npartials = 2048;
+  cudaMalloc(&lp->partials, sizeof(double) * 4 * lp->npartials);
+  cudaMalloc(&lp->counter, sizeof(unsigned int) * 8);
+  cudaMemset(lp->counter, 0, sizeof(unsigned int) * 8);
+  cudaMalloc(&lp->scal_d, sizeof(double) * 64);
+  cudaMemset(lp->scal_d, 0, sizeof(double) * 64);
+  cudaMallocHost(&lp->scal_h, sizeof(double) * 64);
+  if (!lp->egeom_d || !lp->egeom_f || (masked && !lp->maskL8) || !lp->partials || !lp->counter ||
+      !lp->scal_d || !lp->scal_h) {
+    gf_problem_destroy(lp);
+    return GF_ERR_NOMEM;
+  }
+  *out = lp;
+  return GF_OK;
+}
+
+// 1-d prolongation from (nec elements, order pc) to (nef, pf), nef a
+// multiple of nec: each fine lattice point takes the coarse element's GLL
+// Lagrange interpolant at its position (element-local coordinates; the
+// positions of the fine GLL nodes in a coarse element of uniform children).
+void build_p1d(int nef, int pf, int nec, int pc, bool per, std::vector<int32_t> &ptr,
+               std::vector<int32_t> &col, std::vector<float> &val, std::vector<int32_t> &tptr,
+               std::vector<int32_t> &tcol, std::vector<float> &tval) {
+  const int Mf = nef * pf + (per ? 0 : 1), Mc = nec * pc + (per ? 0 : 1);
+  std::vector<double> xf(pf + 1), xc(pc + 1);
+  gf_gll_basis(pf, xf.data(), nullptr, nullptr);
+  gf_gll_basis(pc, xc.data(), nullptr, nullptr);
+  const int ratio = nef / nec;
+  ptr.assign(1, 0);
+  col.clear();
+  val.clear();
+  std::vector<std::vector<std::pair<int, float>>> cols(Mc);
+  for (int g = 0; g < Mf; g++) {
+    const int ef = std::min(g / pf, nef - 1), i = g - ef * pf;
+    const double s = ef + 0.5 * (xf[i] + 1.0), sc = s / ratio;
+    const int ec = std::min((int)std::floor(sc), nec - 1);
+    const double xi = 2.0 * (sc - ec) - 1.0;
+    for (int a = 0; a <= pc; a++) {
+      double w = 1.0;
+      for (int bb = 0; bb <= pc; bb++)
+        if (bb != a) w *= (xi - xc[bb]) / (xc[a] - xc[bb]);
+      if (std::fabs(w) < 1e-13) continue;
+      int c = ec * pc + a;
+      if (per && c == Mc) c = 0;
+      col.push_back(c);
+      val.push_back((float)w);
+      cols[c].push_back({g, (float)w});
+    }
+    ptr.push_back((int32_t)col.size());
+  }
+  tptr.assign(1, 0);
+  tcol.clear();
+  tval.clear();
+  for (int c = 0; c < Mc; c++) {
+    for (auto &e : cols[c]) {
+      tcol.push_back(e.first);
+      tval.push_back(e.second);
+    }
+    tptr.push_back((int32_t)tcol.size());
+  }
+}
+
+// The fine mask must be the box-face Dirichlet mask for the coarse levels'
+// masks to be its restriction: count the lattice points where it differs.
+__global__ void k_boxmask_mismatch(int64_t nL, BoxLattice L, const uint8_t *__restrict__ mask,
+                                   unsigned int *count) {
+  GRID_STRIDE(c, nL) {
+    int64_t r = c;
+    uint8_t want = 1;
+    for (int k = 0; k < L.dim; k++) {
+      const int64_t g = r % L.M[k];
+      r /= L.M[k];
+      if (!L.per[k] && (g == 0 || g == L.M[k] - 1)) want = 0;
+    }
+    if ((mask[c] != 0) != (want != 0)) atomicAdd(count, 1u);
+  }
+}
+
+// The assembled operator of an affine box level on its free lattice points,
+// inverted in FP64: element matrices
+//   A_e(a, b) = p sum_d X_d^2 J K1(a_d, b_d) prod_{k != d} W(a_k) delta(a_k, b_k)
+//             + q J prod_k W(a_k) delta(a, b)       (K1 = D^T W D, lumped mass)
+// summed into the lattice, Cholesky-factored and inverted.  Returns false
+// when the matrix is not positive definite (the level then keeps its
+// Chebyshev solve).
+bool mg_dense_inverse(const gf_problem *lp, const std::vector<double> &eg, double p, double q,
+                      int use_mass, const uint8_t *maskL_host, std::vector<float> &ainv,
+                      std::vector<int32_t> &free_idx) {
+  const BoxLattice &L = lp->box;
+  const int dim = lp->dim, n = lp->n;
+  const int64_t nL = lp->nclass;
+  std::vector<int64_t> pos(nL, -1);
+  free_idx.clear();
+  for (int64_t c = 0; c < nL; c++)
+    if (!maskL_host || maskL_host[c]) {
+      pos[c] = (int64_t)free_idx.size();
+      free_idx.push_back((int32_t)c);
+    }
+  const int64_t nf = (int64_t)free_idx.size();
+  if (nf == 0) return false;
+  std::vector<double> A((size_t)nf * nf, 0.0);
+  const int nn = dim == 3 ? n * n * n : n * n;
+  std::vector<int64_t> gidx(nn);
+  for (int64_t e = 0; e < lp->ne; e++) {
+    int ec[3];
+    L.elem_coords(e, ec);
+    for (int a = 0; a < nn; a++) {
+      const int la[3] = {a % n, (a / n) % n, dim == 3 ? a / (n * n) : 0};
+      int64_t g = L.g1(0, ec[0], la[0]) + L.M[0] * L.g1(1, ec[1], la[1]);
+      if (dim == 3) g += L.M[0] * L.M[1] * L.g1(2, ec[2], la[2]);
+      gidx[a] = g;
+    }
+    const double *geo = &eg[(size_t)e * (dim + 1)];
+    const double J = geo[dim];
+    for (int a = 0; a < nn; a++) {
+      const int64_t ia = pos[gidx[a]];
+      if (ia < 0) continue;
+      const int la[3] = {a % n, (a / n) % n, dim == 3 ? a / (n * n) : 0};
+      for (int b = 0; b < nn; b++) {
+        const int64_t ib = pos[gidx[b]];
+        if (ib < 0) continue;
+        const int lb[3] = {b % n, (b / n) % n, dim == 3 ? b / (n * n) : 0};
+        double v = 0.0;
+        for (int d = 0; d < dim; d++) {
+          bool same = true;
+          double w = 1.0;
+          for (int k = 0; k < dim; k++)
+            if (k != d) {
+              if (la[k] != lb[k]) same = false;
+              w *= lp->W[la[k]];
+            }
+          if (same) v += geo[d] * geo[d] * J * lp->K1[la[d] + lb[d] * n] * w;
+        }
+        v *= p;
+        if (use_mass && a == b) {
+          double w = J;
+          for (int k = 0; k < dim; k++) w *= lp->W[la[k]];
+          v += q * w;
+        }
+        A[(size_t)ia * nf + ib] += v;
+      }
+    }
+  }
+  // Cholesky A = L L^T (lower, in place)
+  for (int64_t j = 0; j < nf; j++) {
+    double dj = A[(size_t)j * nf + j];
+    for (int64_t k = 0; k < j; k++) dj -= A[(size_t)j * nf + k] * A[(size_t)j * nf + k];
+    if (!(dj > 0.0)) return false;
+    dj = std::sqrt(dj);
+    A[(size_t)j * nf + j] = dj;
+    for (int64_t i = j + 1; i < nf; i++) {
+      double v = A[(size_t)i * nf + j];
+      for (int64_t k = 0; k < j; k++) v -= A[(size_t)i * nf + k] * A[(size_t)j * nf + k];
+      A[(size_t)i * nf + j] = v / dj;
+    }
+  }
+  // inverse column by column: L y = e_c, L^T z = y
+  ainv.assign((size_t)nf * nf, 0.0f);
+  std::vector<double> y(nf);
+  for (int64_t c = 0; c < nf; c++) {
+    for (int64_t i = 0; i < nf; i++) {
+      double v = i == c ? 1.0 : 0.0;
+      for (int64_t k = c; k < i; k++) v -= A[(size_t)i * nf + k] * y[k];
+      y[i] = i < c ? 0.0 : v / A[(size_t)i * nf + i];
+    }
+    for (int64_t i = nf - 1; i >= 0; i--) {
+      double v = y[i];
+      for (int64_t k = i + 1; k < nf; k++) v -= A[(size_t)k * nf + i] * y[k];
+      y[i] = v / A[(size_t)i * nf + i];
+    }
+    for (int64_t i = 0; i < nf; i++) ainv[(size_t)i * nf + c] = (float)y[i];
+  }
+  return true;
+}
+
+void mg_coefficients(MGLevelBase &L, int m, double ratio) {
+  const double bb = 1.1 * L.lmax, a = bb / ratio;
+  const double theta = 0.5 * (bb + a), delta = 0.5 * (bb - a), sigma = theta / delta;
+  L.m = m;
+  L.c0 = (float)(1.0 / theta);
+  L.c1.assign(m + 1, 0.0f);
+  L.c2.assign(m + 1, 0.0f);
+  double rho = 1.0 / sigma;
+  for (int j = 1; j <= m; j++) {
+    const double rn1 = 1.0 / (2.0 * sigma - rho);
+    L.c1[j] = (float)(rn1 * rho);
+    L.c2[j] = (float)(2.0 * rn1 / delta);
+    rho = rn1;
+  }
+}
+
+template <class MAP>
+struct IsBox : std::false_type {};
+template <int N>
+struct IsBox<MapBox<N>> : std::true_type {};
+
+template <class MAP>
+int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass) {
+  gf_problem *prob = S.prob;
+  gf_context *ctx = S.ctx;
+  if constexpr (!IsBox<MAP>::value) {
+    return gf_fail(ctx, GF_ERR_UNSUPPORTED, "PMG needs a structured box (box_ne)");
+  } else {
+    GF_REQUIRE(ctx, prob->geom == GF_GEOM_AFFINE && prob->egeom_d,
+               "PMG needs affine elements (GF_GEOM_AFFINE)");
+    const bool masked = S.wt.maskL != nullptr;
+    const int m = std::max(0, tr.poly_degree);
+    const double ratio = tr.poly_ratio > 1.0 ? tr.poly_ratio : 8.0;
+    const double key[6] = {p, q, (double)use_mass, masked ? 1.0 : 0.0, (double)m, ratio};
+    if (prob->mg) {
+      MGHier *H = (MGHier *)prob->mg;
+      if (std::equal(key, key + 6, H->key)) return GF_OK;
+      prob->mg_free(prob->mg);
+      prob->mg = nullptr;
+    }
+    const int dim = prob->dim;
+    const BoxLattice &B = prob->box;
+    cudaStream_t st = S.st;
+    if (masked) {
+      unsigned int *cnt = (unsigned int *)gf_work(prob, 18, sizeof(unsigned int));
+      if (!cnt) return gf_fail(ctx, GF_ERR_NOMEM, "PMG set-up allocation failed");
+      unsigned int h = 0;
+      GF_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned int), st));
+      k_boxmask_mismatch<<<S.gL, 256, 0, st>>>(S.nL, B, prob->maskL8, cnt);
+      GF_CUDA(ctx, cudaMemcpyAsync(&h, cnt, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+      GF_CUDA(ctx, cudaStreamSynchronize(st));
+      GF_REQUIRE(ctx, h == 0, "PMG needs the box-face Dirichlet mask (%u points differ)", h);
+    }
+    std::vector<double> eg((size_t)prob->ne * (dim + 1));
+    GF_CUDA(ctx, cudaMemcpy(eg.data(), prob->egeom_d, sizeof(double) * eg.size(),
+                            cudaMemcpyDeviceToHost));
+    // level descriptions: order, element counts, element geometry
+    struct Desc {
+      int p, ne[3];
+      std::vector<double> eg;
+    };
+    std::vector<Desc> ds;
+    Desc d0;
+    d0.p = prob->n - 1;
+    for (int k = 0; k < 3; k++) d0.ne[k] = B.ne[k];
+    d0.eg = eg;
+    ds.push_back(d0);
+    while (ds.back().p > 1) {
+      Desc d = ds.back();
+      d.p = std::max(1, d.p / 2);
+      ds.push_back(d);
+    }
+    // free lattice points of a level (the dense coarsest solve's size)
+    auto nfree_of = [&](const Desc &d) {
+      int64_t nf = 1;
+      for (int k = 0; k < dim; k++) {
+        const int64_t Mk = (int64_t)d.ne[k] * d.p + (B.per[k] ? 0 : 1);
+        nf *= (masked && !B.per[k]) ? Mk - 2 : Mk;
+      }
+      return nf;
+    };
+    for (;;) {
+      const Desc &f = ds.back();
+      bool ok = nfree_of(f) > MG_DENSE_SMALL;
+      for (int k = 0; k < dim; k++) ok = ok && f.ne[k] % 2 == 0 && f.ne[k] / 2 >= 2;
+      if (!ok) break;
+      Desc c;
+      c.p = 1;
+      for (int k = 0; k < 3; k++) c.ne[k] = k < dim ? f.ne[k] / 2 : 1;
+      const int64_t nec = (int64_t)c.ne[0] * c.ne[1] * c.ne[2];
+      c.eg.assign((size_t)nec * (dim + 1), 0.0);
+      for (int64_t e = 0; e < nec; e++) {
+        const int ec[3] = {(int)(e % c.ne[0]), (int)((e / c.ne[0]) % c.ne[1]),
+                           (int)(e / ((int64_t)c.ne[0] * c.ne[1]))};
+        double jac = 1.0;
+        for (int k = 0; k < dim; k++) {
+          // width along k: the two children along k (at the first child
+          // position in the other directions), width = 2 / dXi/dX
+          double w = 0.0;
+          for (int s = 0; s < 2; s++) {
+            int fc[3] = {2 * ec[0], 2 * ec[1], 2 * ec[2]};
+            fc[k] += s;
+            const int64_t fe = fc[0] + (int64_t)f.ne[0] * (fc[1] + (int64_t)f.ne[1] * fc[2]);
+            w += 2.0 / f.eg[(size_t)fe * (dim + 1) + k];
+          }
+          c.eg[(size_t)e * (dim + 1) + k] = 2.0 / w;
+          jac *= 0.5 * w;
+        }
+        c.eg[(size_t)e * (dim + 1) + dim] = jac;
+      }
+      ds.push_back(c);
+    }
+    MGHier *H = new MGHier();
+    std::copy(key, key + 6, H->key);
+    auto fail = [&](int rc, const char *what) {
+      delete H;
+      return gf_fail(ctx, rc, "PMG set-up: %s", what);
+    };
+    for (size_t l = 0; l < ds.size(); l++) {
+      gf_problem *lp = prob;
+      if (l > 0) {
+        const int per[3] = {B.per[0], B.per[1], B.per[2]};
+        int rc = mg_light_problem(ctx, dim, ds[l].ne, per, ds[l].p, ds[l].eg, masked, &lp);
+        if (rc) return fail(rc, "level allocation failed");
+      }
+      MGLevelBase *L = nullptr;
+      int rc = dispatch_n<MakeLevel>(ds[l].p + 1, lp, l > 0, masked, &L);
+      if (rc || !L) {
+        if (l > 0) gf_problem_destroy(lp);
+        return fail(GF_ERR_UNSUPPORTED, "order out of range");
+      }
+      H->lv.push_back(L);
+      L->dinv = L->alloc_f(L->nL);
+      L->b = L->alloc_f(L->nL);
+      L->x = L->alloc_f(L->nL);
+      L->res = L->alloc_f(L->nL);
+      L->d = L->alloc_f(L->nL);
+      L->qE = L->alloc_f(L->nE);
+      if (!L->dinv || !L->b || !L->x || !L->res || !L->d || !L->qE)
+        return fail(GF_ERR_NOMEM, "vector allocation failed");
+      const bool coarsest = l + 1 == ds.size();
+      const int64_t nfree = nfree_of(ds[l]);
+      bool dense = false;
+      if (coarsest && l > 0 && nfree <= MG_DENSE_MAX) {
+        // exact coarsest solve: the dense inverse of the assembled operator
+        std::vector<uint8_t> mk;
+        if (masked) {
+          mk.assign((size_t)L->nL, 0);
+          GF_CUDA(ctx, cudaMemcpy(mk.data(), L->maskL, L->nL, cudaMemcpyDeviceToHost));
+        }
+        std::vector<float> ai;
+        std::vector<int32_t> fi;
+        if (mg_dense_inverse(lp, ds[l].eg, p, q, use_mass, masked ? mk.data() : nullptr, ai, fi)) {
+          L->ainv = L->upload(ai);
+          L->free_idx = L->upload(fi);
+          L->nfree = (int64_t)fi.size();
+          if (!L->ainv || !L->free_idx) return fail(GF_ERR_NOMEM, "coarse inverse allocation failed");
+          GF_CUDA(ctx, cudaMemset(L->x, 0, sizeof(float) * L->nL));
+          dense = true;
+        }
+      }
+      if (!dense) {
+        if ((rc = L->jacobi(p, q, use_mass))) return fail(rc, "Jacobi diagonal failed");
+        if ((rc = L->estimate(p, q, use_mass, nfree)))
+          return fail(rc, "eigenvalue estimate failed");
+        int mc = 0;
+        for (int k = 0; k < dim; k++) mc = std::max(mc, L->M[k]);
+        if (coarsest) mg_coefficients(*L, std::min(64, std::max(4, 2 * mc)), 30.0);
+        else mg_coefficients(*L, m, ratio);
+      }
+      if (l > 0) {  // transfer between levels l-1 (fine) and l
+        MGLevelBase *F = H->lv[l - 1];
+        for (int k = 0; k < dim; k++) {
+          std::vector<int32_t> pp, pc, tp, tc;
+          std::vector<float> pv, tv;
+          build_p1d(ds[l - 1].ne[k], ds[l - 1].p, ds[l].ne[k], ds[l].p, B.per[k] != 0, pp, pc, pv,
+                    tp, tc, tv);
+          F->P[k] = Line1D{F->upload(pp), F->upload(pc), F->upload(pv)};
+          F->PT[k] = Line1D{F->upload(tp), F->upload(tc), F->upload(tv)};
+          if (!F->P[k].ptr || !F->P[k].col || !F->P[k].val || !F->PT[k].ptr || !F->PT[k].col ||
+              !F->PT[k].val)
+            return fail(GF_ERR_NOMEM, "transfer allocation failed");
+        }
+        // sweep intermediates: restriction (c, f, f), (c, c, f); prolongation
+        // (f, c, c), (f, f, c)
+        const int64_t f0 = F->M[0], f1 = F->M[1], f2 = F->M[2];
+        const int64_t c0 = L->M[0], c1 = L->M[1], c2 = L->M[2];
+        F->t1 = F->alloc_f(std::max(c0 * f1 * f2, f0 * c1 * c2));
+        F->t2 = F->alloc_f(std::max(c0 * c1 * f2, f0 * f1 * c2));
+        if (!F->t1 || !F->t2) return fail(GF_ERR_NOMEM, "transfer allocation failed");
+      }
+    }
+    GF_CUDA(ctx, cudaStreamSynchronize(st));
+    for (size_t l = 1; l < H->lv.size(); l++) H->lv[l]->prob->launches = 0;
+    prob->mg = H;
+    prob->mg_free = mg_free;
+    return GF_OK;
+  }
+}
+
+// restriction lv[l].res -> lv[l+1].b (coarse mask), prolongation
+// lv[l].x += P lv[l+1].x; one k_line1d sweep per direction
+void mg_restrict(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t st) {
+  const double *stop = outer->scal_d + S_DONE;
+  const int dim = F.dim;
+  int e[3] = {F.M[0], F.M[1], F.M[2]};
+  const float *in = F.res;
+  for (int k = 0; k < dim; k++) {
+    int eo[3] = {e[0], e[1], e[2]};
+    eo[k] = C.M[k];
+    const bool last = k == dim - 1;
+    float *out = last ? C.b : (k == 0 ? F.t1 : F.t2);
+    const int64_t nout = (int64_t)eo[0] * eo[1] * eo[2];
+    k_line1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(
+        nout, k, eo[0], eo[1], e[0], e[1], F.PT[k], in, out, last ? C.maskL : nullptr,
+        last ? 2 : 0, stop);
+    outer->launches++;
+    in = out;
+    e[k] = C.M[k];
+  }
+}
+
+void mg_prolong(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t st) {
+  const double *stop = outer->scal_d + S_DONE;
+  const int dim = F.dim;
+  int e[3] = {C.M[0], C.M[1], C.M[2]};
+  const float *in = C.x;
+  for (int k = 0; k < dim; k++) {
+    int eo[3] = {e[0], e[1], e[2]};
+    eo[k] = F.M[k];
+    const bool last = k == dim - 1;
+    float *out = last ? F.x : (k == 0 ? F.t1 : F.t2);
+    const int64_t nout = (int64_t)eo[0] * eo[1] * eo[2];
+    k_line1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(nout, k, eo[0], eo[1], e[0], e[1],
+                                                            F.P[k], in, out, nullptr,
+                                                            last ? 1 : 0, stop);
+    outer->launches++;
+    in = out;
+    e[k] = F.M[k];
+  }
+}
+
+// One V-cycle from level l: lv[l].x ~= A_l^-1 lv[l].b.  At l = 0 the input
+// is the FP64 outer residual r64 and the last pass reduces <r, z> for the
+// CG step.
+void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem *outer,
+               const double *r64, cudaStream_t st) {
+  MGLevelBase &L = *H.lv[l];
+  const double *stop = outer->scal_d + S_DONE;
+  const bool top = l == 0, last = l + 1 == H.lv.size();
+  if (last && L.ainv) {  // coarsest: dense solve (never the finest level)
+    k_dense_solve<<<(unsigned)std::min<int64_t>(L.nfree, 148 * 8), 128, 0, st>>>(
+        L.nfree, L.ainv, L.free_idx, L.b, L.x, stop);
+    outer->launches++;
+    return;
+  }
+  k_mg_start<<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(L.nL, top ? r64 : nullptr, L.b, L.dinv,
+                                                          L.c0, L.res, L.d, L.x, stop);
+  outer->launches++;
+  if (last) {  // coarsest: Chebyshev solve from zero
+    for (int j = 1; j <= L.m; j++) {
+      L.apply(L.d, p, q, use_mass, stop, st);
+      L.pass(MG_STEP, top && j == L.m, L.c1[j], L.c2[j], outer, st);
+    }
+    return;
+  }
+  for (int j = 1; j <= L.m; j++) {  // pre-smoothing x = S b
+    L.apply(L.d, p, q, use_mass, stop, st);
+    L.pass(MG_STEP, false, L.c1[j], L.c2[j], outer, st);
+  }
+  L.apply(L.d, p, q, use_mass, stop, st);  // res = b - A x
+  L.pass(MG_RESID, false, 0.0f, 0.0f, outer, st);
+  mg_restrict(L, *H.lv[l + 1], outer, st);
+  mg_vcycle(H, l + 1, p, q, use_mass, outer, r64, st);
+  mg_prolong(L, *H.lv[l + 1], outer, st);
+  L.apply(L.x, p, q, use_mass, stop, st);  // post-smoothing x += S (b - A x)
+  L.pass(MG_RESTART, top && L.m == 0, L.c0, 0.0f, outer, st);
+  for (int j = 1; j <= L.m; j++) {
+    L.apply(L.d, p, q, use_mass, stop, st);
+    L.pass(MG_STEP, top && j == L.m, L.c1[j], L.c2[j], outer, st);
+  }
+}
+
+// FP64 CG (Fletcher-Reeves beta, fcg_finish_fr) with one FP32 V-cycle as
+// the preconditioner; per iteration the FP64 apply, assembly with
+// <w,q>, the x/r update with the stop test, the V-cycle and w = z + beta w.
+template <class MAP>
+int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass,
+             const double *bL, double *xL, double *rL, double *qE, double *hist, int *total,
+             double *rn) {
+  gf_problem *prob = S.prob;
+  gf_context *ctx = S.ctx;
+  MGHier *H = (MGHier *)prob->mg;
+  if (!H) return gf_fail(ctx, GF_ERR_ARG, "PMG hierarchy missing");
+  cudaStream_t st = S.st;
+  const int64_t nL = S.nL;
+  double *w = (double *)gf_work(prob, 4, sizeof(double) * nL);
+  double *qL = (double *)gf_work(prob, 5, sizeof(double) * nL);
+  if (!w || !qL) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
+  GF_CUDA(ctx, cudaMemsetAsync(qL, 0, sizeof(double) * nL, st));
+  int rc = S.template residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, w, nullptr, 0, tr.tol);
+  if (rc) return gf_fail(ctx, rc, "residual failed");
+  const float *z = H->lv[0]->x;
+  double *scal = prob->scal_d;
+  auto precondition = [&](cudaStream_t ls) {
+    mg_vcycle(*H, 0, p, q, use_mass, prob, rL, ls);
+    prob->launches++;
+    k_fcg_w<<<S.gL, 256, 0, ls>>>(nL, w, z, scal);
+  };
+  auto iterations = [&](int k, cudaStream_t ls) {
+    for (int i = 0; i < k; i++) {
+      launch_helm_L<double>(prob, p, q, use_mass, w, qE, ls, scal + S_DONE);
+      k_asm_dot<double, MAP><<<S.rgrid(k_asm_dot<double, MAP>), RED_THREADS, 0, ls>>>(
+          nL, S.map, S.wt, qE, w, qL, scal, prob->partials, prob->counter);
+      k_update<double, MAP><<<S.rgrid(k_update<double, MAP>), RED_THREADS, 0, ls>>>(
+          nL, S.map, S.wt, xL, w, rL, qL, nullptr, hist, nullptr, 0, scal, prob->partials,
+          prob->counter);
+      prob->launches += 2;
+      precondition(ls);
+    }
+  };
+  auto level_launches = [&]() {
+    uint64_t n = prob->launches;
+    for (size_t l = 1; l < H->lv.size(); l++) n += H->lv[l]->prob->launches;
+    return n;
+  };
+  prob->scal_h[S_FIRST] = 1.0;
+  GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_d + S_FIRST, prob->scal_h + S_FIRST, sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+  precondition(st);
+  // A batch of `every` iterations is a fixed sequence of some 130 launches
+  // per iteration (most of them small coarse-level kernels) whose scalars
+  // live on the device, so it is captured once as a CUDA graph and
+  // replayed; iterations past convergence return at once (`done` flag), so
+  // a full batch may be replayed where fewer iterations remain (the
+  // residual history is written only below maxit, which the device holds).
+  const int every = tr.check_every > 0 ? tr.check_every : 16;
+  const void *gk[7] = {xL, rL, w, qL, qE, bL, hist};
+  if (!(H->exec && H->gevery == every && std::equal(gk, gk + 7, H->gkey))) {
+    H->drop_graph();
+    if (!H->cs) GF_CUDA(ctx, cudaStreamCreateWithFlags(&H->cs, cudaStreamNonBlocking));
+    const uint64_t n0 = level_launches();
+    cudaError_t e = cudaStreamBeginCapture(H->cs, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+      iterations(every, H->cs);
+      e = cudaStreamEndCapture(H->cs, &H->graph);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&H->exec, H->graph, 0);
+    H->glaunches = level_launches() - n0;
+    for (size_t l = 1; l < H->lv.size(); l++) H->lv[l]->prob->launches = 0;
+    prob->launches = n0;
+    if (e != cudaSuccess) {
+      H->drop_graph();
+      return gf_fail(ctx, GF_ERR_CUDA, "CG batch capture failed: %s", cudaGetErrorString(e));
+    }
+    H->gevery = every;
+    std::copy(gk, gk + 7, H->gkey);
+  }
+  rc = S.batches(tr, tr.maxit, total, [&](int) {
+    cudaGraphLaunch(H->exec, st);
+    prob->launches += H->glaunches;
+  });
+  for (size_t l = 1; l < H->lv.size(); l++) {  // the levels' applies count as this problem's
+    prob->launches += H->lv[l]->prob->launches;
+    H->lv[l]->prob->launches = 0;
+  }
+  if (rc) return rc;
+  *rn = prob->scal_h[S_RNORM];
+  return (*total >= tr.maxit && *rn > prob->scal_h[S_RTOL]) ? GF_CG_NOCONVERGE : GF_OK;
+}
+
 template <int N>
 struct BoxSolve {
   static int run(gf_problem *prob, const gf_cg_traits *tr, double p, double q, int use_mass,
@@ -1205,11 +2250,10 @@ extern "C" int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *tr, double p, 
   GF_REQUIRE(ctx, tr->maxit >= 0, "maxit must be >= 0");
   GF_REQUIRE(ctx, tr->normtype >= GF_NORM_INF && tr->normtype <= GF_NORM_L1, "bad norm type");
   GF_REQUIRE(ctx, tr->precision == GF_CG_FP64 || tr->precision == GF_CG_MIXED, "bad precision");
-  GF_REQUIRE(ctx, tr->precond == GF_PRECOND_NONE || tr->precond == GF_PRECOND_JACOBI ||
-                      tr->precond == GF_PRECOND_CHEBYSHEV,
+  GF_REQUIRE(ctx, tr->precond >= GF_PRECOND_NONE && tr->precond <= GF_PRECOND_PMG,
              "bad preconditioner");
-  GF_REQUIRE(ctx, tr->precond != GF_PRECOND_CHEBYSHEV || (tr->poly_degree >= 0 &&
-                                                         tr->poly_degree <= 64),
+  GF_REQUIRE(ctx, tr->precond < GF_PRECOND_CHEBYSHEV || (tr->poly_degree >= 0 &&
+                                                        tr->poly_degree <= 64),
              "poly_degree must be 0..64");
   GF_CUDA(ctx, cudaSetDevice(ctx->device));
   double *hist = nullptr;
@@ -1231,7 +2275,10 @@ extern "C" int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *tr, double p, 
   if (rc < 0) return rc;
   if (iters) *iters = it;
   if (final_norm) *final_norm = rn;
-  if (residuals && hist && it > 0 && tr->precision == GF_CG_FP64) {
+  // the history holds FP64 (outer) iterations: plain FP64 and the FP64
+  // flexible CG of the polynomial and multigrid preconditioners
+  if (residuals && hist && it > 0 &&
+      (tr->precision == GF_CG_FP64 || tr->precond >= GF_PRECOND_CHEBYSHEV)) {
     GF_CUDA(ctx, cudaMemcpyAsync(residuals, hist, sizeof(double) * std::min(it, tr->maxit),
                                  cudaMemcpyDeviceToHost, ctx->stream));
   }

@@ -423,6 +423,7 @@ extern "C" int gf_problem_destroy(gf_problem_t prob) {
   if (!prob) return GF_ERR_ARG;
   cudaSetDevice(prob->ctx->device);
   cudaStreamSynchronize(prob->ctx->stream);
+  if (prob->mg && prob->mg_free) prob->mg_free(prob->mg);
   void *ptrs[] = {prob->egeom_d, prob->egeom_f, prob->ngeom_d, prob->ngeom_f, prob->mask_d,
                   prob->mask_f, prob->imass_d, prob->imass_f, prob->mass_d, prob->imult_d,
                   prob->imult_f, prob->class_ptr, prob->members, prob->node_class, prob->sh_ptr,

@@ -83,6 +83,9 @@ struct gf_problem {
   unsigned int *counter = nullptr;
   int npartials = 0;
   uint64_t launches = 0;  // kernels launched on this problem (instrumentation)
+  // cached multigrid hierarchy of the CG preconditioner (api_cg.cu)
+  void *mg = nullptr;
+  void (*mg_free)(void *) = nullptr;
 };
 
 // ---- error helpers ----

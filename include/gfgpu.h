@@ -54,7 +54,15 @@ enum { GF_NORM_INF = 0, GF_NORM_EUC = 1, GF_NORM_L2 = 2, GF_NORM_L1 = 3 }; /* li
 /* CHEBYSHEV: FP64 flexible CG whose preconditioner is a Chebyshev
  * polynomial in D^-1 A applied in FP32 (poly_degree FP32 applies per step);
  * no reference counterpart */
-enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1, GF_PRECOND_CHEBYSHEV = 2 };
+/* PMG: FP64 flexible CG whose preconditioner is one FP32 multigrid V-cycle:
+ * p-coarsening p -> p/2 -> ... -> 1 on the same elements, then h-coarsening
+ * of the p = 1 box by 2 in every direction while the element counts stay
+ * even, with Chebyshev-Jacobi smoothing of degree poly_degree on every
+ * level (interval [lmax/poly_ratio, lmax], lmax from a Lanczos estimate).
+ * Structured affine boxes only (box_ne set, GF_GEOM_AFFINE, mask absent or
+ * the box-face Dirichlet mask); the hierarchy is kept with the problem and
+ * reused while p, q and the traits stay the same.  No reference counterpart. */
+enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1, GF_PRECOND_CHEBYSHEV = 2, GF_PRECOND_PMG = 3 };
 enum { GF_CG_FP64 = 0, GF_CG_MIXED = 1 };            /* plain FP64 / FP32 apply + FP64 refinement */
 /* see gf_problem_desc; DEFORMED = GE_DEFORMED, EMBEDDED = GE_2DEMBEDDED */
 enum { GF_GEOM_AFFINE = 0, GF_GEOM_REGULAR = 1, GF_GEOM_DEFORMED = 2, GF_GEOM_EMBEDDED = 3 };
@@ -223,10 +231,12 @@ typedef struct {
   int relative;     /* 1: stop at norm(r) <= tol*norm(b) even when norm(b) < 1 */
   int mixed_apply;  /* MIXED, 3-d: 0 FP32 arithmetic in the FP32 solve's applies,
                        1 FP64 arithmetic on the FP32-stored vectors */
-  int poly_degree;  /* CHEBYSHEV: FP32 applies per preconditioner application */
+  int poly_degree;  /* CHEBYSHEV: FP32 applies per preconditioner application;
+                       PMG: Chebyshev smoothing degree per level and side */
   double poly_ratio;/* CHEBYSHEV: b/a of the polynomial's interval [a, b], b from
                        a Lanczos estimate of the largest eigenvalue of D^-1 A
-                       (<= 1: max(4, 2 poly_degree^2)) */
+                       (<= 1: max(4, 2 poly_degree^2)); PMG: the same ratio of
+                       the smoothing interval (<= 1: 8) */
 } gf_cg_traits;
 
 /* Solves (p L + q M) x = b on the assembled space (DSS Sum + mask), as
