@@ -778,41 +778,75 @@ __global__ void k_invert(int64_t n, const double *__restrict__ d, double *__rest
 // coarse element's GLL interpolant at its position, and the restriction
 // is P^T.  Each is applied one direction at a time.
 
-// 1-d operator along direction d as CSR rows (row = output coordinate)
-struct Line1D {
-  const int32_t *ptr = nullptr, *col = nullptr;
-  const float *val = nullptr;
+// 1-d transfer between the lattices of two levels along one direction.
+// Each coarse element spans R = ratio * pf fine lattice intervals; the
+// fine point at offset r = 0..R in coarse element ec takes
+// sum_a J[r][a] x_c(ec pc + a) (J[0] and J[R] are unit rows: shared
+// vertices coincide).  The restriction is the transpose, gathered per
+// coarse point.  Periodic directions wrap (Mf = nec R, Mc = nec pc).
+constexpr int MG_XR = 2 * GF_MAXN + 1;
+struct Xfer1D {
+  int R, pc, nec, per, Mf, Mc;
+  float J[MG_XR * GF_MAXN];  // J[r * (pc + 1) + a]
 };
 
-// out(g) = sum_k val[k] in(g with g_d = col[k]); in and out are lattices
+// out = T in along direction d (transpose: T^T); in and out are lattices
 // of extents ei and eo that differ only in direction d.
 // mode 0: out = s; 1: out += s; 2: out = mask ? s : 0 (mask of the output)
-__global__ void k_line1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1, Line1D T,
+__global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1,
+                         const __grid_constant__ Xfer1D T, int transpose,
                          const float *__restrict__ in, float *__restrict__ out,
                          const uint8_t *__restrict__ mask, int mode, const double *stop) {
   if (stop && *stop != 0.0) return;
-  GRID_STRIDE(o, nout) {
-    const int g0 = (int)(o % eo0);
-    const int64_t rr = o / eo0;
-    const int g1 = (int)(rr % eo1), g2 = (int)(rr / eo1);
-    int64_t base, stride;
-    int gd;
+  const int R = T.R, pc = T.pc, nc = T.pc + 1, nec = T.nec;
+  // lattice sizes are below 2^31 (32-bit index arithmetic)
+  const int n32 = (int)nout;
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n32; o += gridDim.x * blockDim.x) {
+    const unsigned uo = (unsigned)o, ue0 = (unsigned)eo0, ue1 = (unsigned)eo1;
+    const unsigned rr = uo / ue0;
+    const int g0 = (int)(uo - rr * ue0);
+    const unsigned q1 = rr / ue1;
+    const int g1 = (int)(rr - q1 * ue1), g2 = (int)q1;
+    int base, stride, gd;
     if (d == 0) {
       gd = g0;
-      base = (int64_t)ei0 * (g1 + (int64_t)ei1 * g2);
+      base = ei0 * (g1 + ei1 * g2);
       stride = 1;
     } else if (d == 1) {
       gd = g1;
-      base = g0 + (int64_t)ei0 * ei1 * g2;
+      base = g0 + ei0 * ei1 * g2;
       stride = ei0;
     } else {
       gd = g2;
-      base = g0 + (int64_t)ei0 * g1;
-      stride = (int64_t)ei0 * ei1;
+      base = g0 + ei0 * g1;
+      stride = ei0 * ei1;
     }
     float s = 0.0f;
-    for (int k = T.ptr[gd]; k < T.ptr[gd + 1]; k++)
-      s = fmaf(T.val[k], in[base + (int64_t)T.col[k] * stride], s);
+    if (!transpose) {  // fine point gd from coarse element ec
+      const int ec = min(gd / R, nec - 1), r = gd - ec * R;
+      for (int a = 0; a < nc; a++) {
+        int c = ec * pc + a;
+        if (c >= T.Mc) c -= T.Mc;
+        s = fmaf(T.J[r * nc + a], in[base + c * stride], s);
+      }
+    } else {  // coarse point gd = ec pc + a
+      const int ec = gd / pc, a = gd - ec * pc;
+      if (a != 0) {
+        for (int r = 1; r < R; r++)
+          s = fmaf(T.J[r * nc + a], in[base + (ec * R + r) * stride], s);
+      } else {
+        s = in[base + (ec * R) * stride];  // the coinciding vertex
+        const bool left = ec > 0 || T.per, right = ec < nec;
+        if (left) {
+          const int el = ec > 0 ? ec - 1 : nec - 1;
+          for (int r = 1; r < R; r++)
+            s = fmaf(T.J[r * nc + pc], in[base + (el * R + r) * stride], s);
+        }
+        if (right)
+          for (int r = 1; r < R; r++)
+            s = fmaf(T.J[r * nc], in[base + (ec * R + r) * stride], s);
+      }
+    }
     if (mode == 2 && mask && !mask[o]) s = 0.0f;
     if (mode == 1) out[o] += s;
     else out[o] = s;
@@ -887,48 +921,57 @@ __device__ __forceinline__ int lattice_cands(int g, int ne, int per, int (&ec)[2
   return k;
 }
 
-// sum of the element copies of lattice point c (ascending element id)
-template <int N>
-__device__ __forceinline__ float lattice_fold(const MapBox<N> &map, const float *__restrict__ qE,
-                                              int c, int M0, int M1, bool d3) {
-  constexpr int P = N - 1, NN = N * N;
-  const int nn = d3 ? NN * N : NN;
-  const int ne0 = map.ne[0], ne1 = map.ne[1];
-  const int row = c / M0, g0 = c - row * M0;
-  const int g1 = row % M1, g2 = row / M1;
-  int ex[2], lx[2], ey[2], ly[2], ez[2] = {0, 0}, lz[2] = {0, 0};
-  const int nx = lattice_cands<P>(g0, ne0, map.per[0], ex, lx);
-  const int ny = lattice_cands<P>(g1, ne1, map.per[1], ey, ly);
-  const int nz = d3 ? lattice_cands<P>(g2, map.ne[2], map.per[2], ez, lz) : 1;
-  float s = 0.0f;
-  for (int az = 0; az < nz; az++)
-    for (int ay = 0; ay < ny; ay++) {
-      const int eyz = ne0 * (ey[ay] + ne1 * ez[az]);
-      const int off = N * ly[ay] + NN * lz[az];
-      for (int ax = 0; ax < nx; ax++)
-        s = __fadd_rn(s, qE[(int64_t)(ex[ax] + eyz) * nn + off + lx[ax]]);
-    }
-  return s;
-}
-
-// One thread per lattice point in lattice order: consecutive threads take
-// consecutive points, so the state vectors stream coalesced and a warp's
-// copies of one element row share one sector.  (Measured on B200: giving a
-// thread several points, consecutive or a grid stride apart, was slower.)
+// One thread per lattice point in lattice order.  A 256-thread block walks
+// lattice rows (fixed y, z), 2^LB threads per row (2^LB >= M0, or segments
+// of 256 for longer rows), so a thread's row and x position come from
+// shifts and masks, the y/z element copies are fixed for the row, and only
+// the x copies vary by thread; consecutive threads take consecutive points
+// (coalesced state vectors, a warp's copies of one element row in one
+// sector).  Copies are added in ascending element id.  Lattice and
+// element-local sizes are below 2^31 (checked when the problem is created).
+// (Measured on B200 against this form: element-ordered walks, several
+// points per thread, z-column walks and a lattice-row layout of qE were all
+// slower.)
 template <int N, int MODE, bool DOTS>
 __global__ void __launch_bounds__(RED_THREADS)
     k_mg_pass_lat(MapBox<N> map, Weights wt, const float *__restrict__ qE,
                   const float *__restrict__ b, const float *__restrict__ dinv, float c1, float c2,
-                  float *__restrict__ res, float *__restrict__ d, float *__restrict__ x,
+                  float *__restrict__ res, float *__restrict__ d, float *__restrict__ x, int LB,
                   double *scal, double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
+  constexpr int P = N - 1, NN = N * N;
   double rz = 0.0;
   const bool d3 = map.dim > 2;
+  const int nn = d3 ? NN * N : NN;
+  const int ne0 = map.ne[0], ne1 = map.ne[1];
   const int M0 = (int)map.M[0], M1 = (int)map.M[1];
-  const int nL = M0 * M1 * (d3 ? (int)map.M[2] : 1);
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nL; c += gridDim.x * blockDim.x) {
-    float s = lattice_fold<N>(map, qE, c, M0, M1, d3);
+  const int nrows = M1 * (d3 ? (int)map.M[2] : 1);
+  const int W = 1 << LB, nseg = (M0 + W - 1) / W;
+  const int upb = RED_THREADS >> LB;  // row segments per block trip
+  const int tx = threadIdx.x & (W - 1), ty = threadIdx.x >> LB;
+  int ex[2], lx[2], nx = 0;
+  if (nseg == 1 && tx < M0) nx = lattice_cands<P>(tx, ne0, map.per[0], ex, lx);
+  for (int unit = blockIdx.x * upb + ty; unit < nrows * nseg; unit += gridDim.x * upb) {
+    int row = unit, g0 = tx;
+    if (nseg > 1) {
+      row = unit / nseg;
+      g0 = (unit - row * nseg) * W + tx;
+      if (g0 < M0) nx = lattice_cands<P>(g0, ne0, map.per[0], ex, lx);
+    }
+    if (g0 >= M0) continue;
+    const int g1 = row % M1, g2 = row / M1;
+    int ey[2], ly[2], ez[2] = {0, 0}, lz[2] = {0, 0};
+    const int ny = lattice_cands<P>(g1, ne1, map.per[1], ey, ly);
+    const int nz = d3 ? lattice_cands<P>(g2, map.ne[2], map.per[2], ez, lz) : 1;
+    float s = 0.0f;
+    for (int az = 0; az < nz; az++)
+      for (int ay = 0; ay < ny; ay++) {
+        const int base = ne0 * (ey[ay] + ne1 * ez[az]) * nn + N * ly[ay] + NN * lz[az];
+        s = __fadd_rn(s, qE[base + ex[0] * nn + lx[0]]);
+        if (nx > 1) s = __fadd_rn(s, qE[base + ex[1] * nn + lx[1]]);
+      }
+    const int c = g0 + M0 * row;
     if (wt.maskL && !wt.maskL[c]) s = 0.0f;
     if (MODE == MG_RESID) {
       res[c] = res[c] - s;
@@ -1477,7 +1520,7 @@ struct MGLevelBase {
   const float *ainv = nullptr;
   const int32_t *free_idx = nullptr;
   // transfer to the next coarser level
-  Line1D P[3], PT[3];
+  Xfer1D X[3];
   float *t1 = nullptr, *t2 = nullptr;
   std::vector<void *> mem;
   float *alloc_f(int64_t n) {
@@ -1517,7 +1560,12 @@ struct MGLevel : MGLevelBase {
     nE = lp->nlocal;
     for (int k = 0; k < 3; k++) M[k] = (int)lp->box.M[k];
     maskL = S.wt.maskL;
+    // lattice row width of the smoother passes: 2^LB >= M0 threads (a
+    // block, 2^8, at most; longer rows in segments)
+    LB = 5;
+    while ((1 << LB) < M[0] && LB < 8) LB++;
   }
+  int LB = 8;
   int apply(const float *in, double p, double q, int use_mass, const double *stop,
             cudaStream_t st) override {
     return launch_helm_L<float>(prob, (float)p, (float)q, use_mass, in, qE, st, stop);
@@ -1525,7 +1573,7 @@ struct MGLevel : MGLevelBase {
   template <int MODE, bool DOTS>
   void run_pass(float a1, float a2, gf_problem *outer, cudaStream_t st) {
     auto kern = k_mg_pass_lat<N, MODE, DOTS>;
-    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, S.wt, qE, b, dinv, a1, a2, res, d, x,
+    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, S.wt, qE, b, dinv, a1, a2, res, d, x, LB,
                                                  outer->scal_d, outer->partials, outer->counter);
   }
   void pass(int mode, bool dots, float a1, float a2, gf_problem *outer,
@@ -1699,50 +1747,34 @@ int mg_light_problem(gf_context *ctx, int dim, const int (&ne)[3], const int (&p
   return GF_OK;
 }
 
-// 1-d prolongation from (nec elements, order pc) to (nef, pf), nef a
-// multiple of nec: each fine lattice point takes the coarse element's GLL
-// Lagrange interpolant at its position (element-local coordinates; the
-// positions of the fine GLL nodes in a coarse element of uniform children).
-void build_p1d(int nef, int pf, int nec, int pc, bool per, std::vector<int32_t> &ptr,
-               std::vector<int32_t> &col, std::vector<float> &val, std::vector<int32_t> &tptr,
-               std::vector<int32_t> &tcol, std::vector<float> &tval) {
-  const int Mf = nef * pf + (per ? 0 : 1), Mc = nec * pc + (per ? 0 : 1);
+// 1-d transfer from (nec elements, order pc) to (nef, pf), nef a multiple
+// of nec: the fine point at offset r in a coarse element takes the coarse
+// element's GLL Lagrange interpolant at its position (element-local
+// coordinates; the fine GLL nodes of uniform children).
+Xfer1D build_xfer(int nef, int pf, int nec, int pc, bool per) {
+  Xfer1D T{};
+  const int ratio = nef / nec;
+  T.R = ratio * pf;
+  T.pc = pc;
+  T.nec = nec;
+  T.per = per ? 1 : 0;
+  T.Mf = nef * pf + (per ? 0 : 1);
+  T.Mc = nec * pc + (per ? 0 : 1);
   std::vector<double> xf(pf + 1), xc(pc + 1);
   gf_gll_basis(pf, xf.data(), nullptr, nullptr);
   gf_gll_basis(pc, xc.data(), nullptr, nullptr);
-  const int ratio = nef / nec;
-  ptr.assign(1, 0);
-  col.clear();
-  val.clear();
-  std::vector<std::vector<std::pair<int, float>>> cols(Mc);
-  for (int g = 0; g < Mf; g++) {
-    const int ef = std::min(g / pf, nef - 1), i = g - ef * pf;
-    const double s = ef + 0.5 * (xf[i] + 1.0), sc = s / ratio;
-    const int ec = std::min((int)std::floor(sc), nec - 1);
-    const double xi = 2.0 * (sc - ec) - 1.0;
+  for (int r = 0; r <= T.R; r++) {
+    const int cf = std::min(r / pf, ratio - 1), i = r - cf * pf;
+    const double xi = 2.0 * (cf + 0.5 * (xf[i] + 1.0)) / ratio - 1.0;
     for (int a = 0; a <= pc; a++) {
       double w = 1.0;
       for (int bb = 0; bb <= pc; bb++)
         if (bb != a) w *= (xi - xc[bb]) / (xc[a] - xc[bb]);
-      if (std::fabs(w) < 1e-13) continue;
-      int c = ec * pc + a;
-      if (per && c == Mc) c = 0;
-      col.push_back(c);
-      val.push_back((float)w);
-      cols[c].push_back({g, (float)w});
+      if (std::fabs(w) < 1e-13) w = 0.0;
+      T.J[r * (pc + 1) + a] = (float)w;
     }
-    ptr.push_back((int32_t)col.size());
   }
-  tptr.assign(1, 0);
-  tcol.clear();
-  tval.clear();
-  for (int c = 0; c < Mc; c++) {
-    for (auto &e : cols[c]) {
-      tcol.push_back(e.first);
-      tval.push_back(e.second);
-    }
-    tptr.push_back((int32_t)tcol.size());
-  }
+  return T;
 }
 
 // The fine mask must be the box-face Dirichlet mask for the coarse levels'
@@ -2030,17 +2062,8 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
       }
       if (l > 0) {  // transfer between levels l-1 (fine) and l
         MGLevelBase *F = H->lv[l - 1];
-        for (int k = 0; k < dim; k++) {
-          std::vector<int32_t> pp, pc, tp, tc;
-          std::vector<float> pv, tv;
-          build_p1d(ds[l - 1].ne[k], ds[l - 1].p, ds[l].ne[k], ds[l].p, B.per[k] != 0, pp, pc, pv,
-                    tp, tc, tv);
-          F->P[k] = Line1D{F->upload(pp), F->upload(pc), F->upload(pv)};
-          F->PT[k] = Line1D{F->upload(tp), F->upload(tc), F->upload(tv)};
-          if (!F->P[k].ptr || !F->P[k].col || !F->P[k].val || !F->PT[k].ptr || !F->PT[k].col ||
-              !F->PT[k].val)
-            return fail(GF_ERR_NOMEM, "transfer allocation failed");
-        }
+        for (int k = 0; k < dim; k++)
+          F->X[k] = build_xfer(ds[l - 1].ne[k], ds[l - 1].p, ds[l].ne[k], ds[l].p, B.per[k] != 0);
         // sweep intermediates: restriction (c, f, f), (c, c, f); prolongation
         // (f, c, c), (f, f, c)
         const int64_t f0 = F->M[0], f1 = F->M[1], f2 = F->M[2];
@@ -2059,7 +2082,7 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
 }
 
 // restriction lv[l].res -> lv[l+1].b (coarse mask), prolongation
-// lv[l].x += P lv[l+1].x; one k_line1d sweep per direction
+// lv[l].x += P lv[l+1].x; one k_xfer1d sweep per direction
 void mg_restrict(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t st) {
   const double *stop = outer->scal_d + S_DONE;
   const int dim = F.dim;
@@ -2071,8 +2094,8 @@ void mg_restrict(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t
     const bool last = k == dim - 1;
     float *out = last ? C.b : (k == 0 ? F.t1 : F.t2);
     const int64_t nout = (int64_t)eo[0] * eo[1] * eo[2];
-    k_line1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(
-        nout, k, eo[0], eo[1], e[0], e[1], F.PT[k], in, out, last ? C.maskL : nullptr,
+    k_xfer1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(
+        nout, k, eo[0], eo[1], e[0], e[1], F.X[k], 1, in, out, last ? C.maskL : nullptr,
         last ? 2 : 0, stop);
     outer->launches++;
     in = out;
@@ -2091,8 +2114,8 @@ void mg_prolong(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t 
     const bool last = k == dim - 1;
     float *out = last ? F.x : (k == 0 ? F.t1 : F.t2);
     const int64_t nout = (int64_t)eo[0] * eo[1] * eo[2];
-    k_line1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(nout, k, eo[0], eo[1], e[0], e[1],
-                                                            F.P[k], in, out, nullptr,
+    k_xfer1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(nout, k, eo[0], eo[1], e[0], e[1],
+                                                            F.X[k], 0, in, out, nullptr,
                                                             last ? 1 : 0, stop);
     outer->launches++;
     in = out;

@@ -65,6 +65,25 @@ def test_pmg_reaches_fp64_solution(ctx, dim, ne, p, per, m):
         assert cgm.get_iteration_count() < cgj.get_iteration_count()
 
 
+@pytest.mark.parametrize("per", [[1, 0, 0], [0, 0, 0]])
+def test_pmg_long_lattice_rows(ctx, per):
+    """Lattice rows longer than a block (40 elements at p = 7 along x) are
+    walked in segments; isotropic elements (box 20 x 1 x 1)."""
+    g = GridBox(3, [40, 2, 2], 7, length=[20.0, 1.0, 1.0], periodic=per)
+    prob = Problem(ctx, g)
+    b = rhs(g, 13)
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    xj = prob.zeros()
+    assert GCG(CGTraits(precond=A.GF_PRECOND_JACOBI, **COMMON), prob).solve(
+        H, dev(b), dev(0 * b), xj) == 0
+    xm = prob.zeros()
+    cgm = GCG(CGTraits(precond=A.GF_PRECOND_PMG, **COMMON), prob)
+    assert cgm.solve(H, dev(b), dev(0 * b), xm) == 0
+    assert relerr(host(xm), host(xj)) < 1e-9
+    assert cgm.get_iteration_count() <= 30
+
+
 def test_pmg_iterations_independent_of_element_count(ctx):
     its = []
     for ne in (2, 4, 8):
