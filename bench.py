@@ -76,7 +76,7 @@ def parse():
                     help="FP32 applies per Chebyshev preconditioner application")
     ap.add_argument("--poly-ratio", type=float, default=0.0,
                     help="b/a of the Chebyshev interval (0: library default)")
-    ap.add_argument("--mg-degree", type=int, default=2,
+    ap.add_argument("--mg-degree", type=int, default=1,
                     help="multigrid: Chebyshev smoothing degree per level and side")
     ap.add_argument("--mg-ratio", type=float, default=0.0,
                     help="multigrid: lmax/lmin of the smoothing interval (0: library default)")

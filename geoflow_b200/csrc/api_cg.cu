@@ -1485,7 +1485,7 @@ struct Solver {
 // ---------------------------------------------------------------------
 // p/h multigrid preconditioner for structured affine boxes.
 //
-// Levels: the problem's own order p, then p/2, p/4, ... down to 1 on the
+// Levels: the problem's own order p, then ceil(p/2), ... down to 1 on the
 // same elements, then the p = 1 box with the element counts halved while
 // they stay even and >= 2.  Each coarser level is the same SEM Helmholtz
 // operator rediscretised (GLL quadrature of its order, element geometry
@@ -1957,9 +1957,9 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
     for (int k = 0; k < 3; k++) d0.ne[k] = B.ne[k];
     d0.eg = eg;
     ds.push_back(d0);
-    while (ds.back().p > 1) {
+    while (ds.back().p > 1) {  // p -> ceil(p/2): 7, 4, 2, 1
       Desc d = ds.back();
-      d.p = std::max(1, d.p / 2);
+      d.p = (d.p + 1) / 2;
       ds.push_back(d);
     }
     // free lattice points of a level (the dense coarsest solve's size)

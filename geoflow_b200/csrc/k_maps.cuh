@@ -38,20 +38,40 @@ struct LoadBox {  // unique-node vector on a box lattice
   using value_type = T;
   const T *w;
   BoxLattice L;
+  // 32-bit index arithmetic: element and lattice counts are below 2^31
+  // (checked when the problem is created)
+  __device__ __forceinline__ void coords32(int64_t e, int &c0, int &c1, int &c2) const {
+    const unsigned ue = (unsigned)e, n0 = (unsigned)L.ne[0], n1 = (unsigned)L.ne[1];
+    const unsigned r = ue / n0, q = r / n1;
+    c0 = (int)(ue - r * n0);
+    c1 = (int)(r - q * n1);
+    c2 = (int)q;
+  }
   template <int N>
   __device__ __forceinline__ void zline(int64_t e, int i, int j, T (&out)[N]) const {
-    int c[3];
-    L.elem_coords(e, c);
-    const int64_t base = L.g1(0, c[0], i) + L.M[0] * L.g1(1, c[1], j);
-    const int64_t plane = L.M[0] * L.M[1];
+    int c0, c1, c2;
+    coords32(e, c0, c1, c2);
+    const int P = L.p, M0 = (int)L.M[0], M1 = (int)L.M[1], M2 = (int)L.M[2];
+    int gx = c0 * P + i, gy = c1 * P + j;
+    if (L.per[0] && gx == M0) gx = 0;
+    if (L.per[1] && gy == M1) gy = 0;
+    const int base = gx + M0 * gy, plane = M0 * M1;
 #pragma unroll
-    for (int k = 0; k < N; k++) out[k] = w[base + plane * L.g1(2, c[2], k)];
+    for (int k = 0; k < N; k++) {
+      int gz = c2 * P + k;
+      if (L.per[2] && gz == M2) gz = 0;
+      out[k] = w[base + plane * gz];
+    }
   }
   template <int N>
   __device__ __forceinline__ T point2(int64_t e, int i, int j) const {
-    int c[3];
-    L.elem_coords(e, c);
-    return w[L.g1(0, c[0], i) + L.M[0] * L.g1(1, c[1], j)];
+    int c0, c1, c2;
+    coords32(e, c0, c1, c2);
+    const int P = L.p, M0 = (int)L.M[0], M1 = (int)L.M[1];
+    int gx = c0 * P + i, gy = c1 * P + j;
+    if (L.per[0] && gx == M0) gx = 0;
+    if (L.per[1] && gy == M1) gy = 0;
+    return w[gx + M0 * gy];
   }
 };
 

@@ -55,7 +55,7 @@ enum { GF_NORM_INF = 0, GF_NORM_EUC = 1, GF_NORM_L2 = 2, GF_NORM_L1 = 3 }; /* li
  * polynomial in D^-1 A applied in FP32 (poly_degree FP32 applies per step);
  * no reference counterpart */
 /* PMG: FP64 flexible CG whose preconditioner is one FP32 multigrid V-cycle:
- * p-coarsening p -> p/2 -> ... -> 1 on the same elements, then h-coarsening
+ * p-coarsening p -> ceil(p/2) -> ... -> 1 on the same elements, then h-coarsening
  * of the p = 1 box by 2 in every direction while the element counts stay
  * even, with Chebyshev-Jacobi smoothing of degree poly_degree on every
  * level (interval [lmax/poly_ratio, lmax], lmax from a Lanczos estimate).
