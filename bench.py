@@ -81,7 +81,7 @@ def parse():
     ap.add_argument("--mg-ratio", type=float, default=0.0,
                     help="multigrid: lmax/lmin of the smoothing interval (0: library default)")
     ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "pmg", "apply", "adjoint", "graphs",
-                                       "rk"],
+                                       "rk", "maps"],
                     default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
@@ -479,6 +479,65 @@ def graph_bench(ctx, reps=3):
 
 
 # ---------------------------------------------------------------------------
+def index_map_bench(ctx):
+    """Gather-scatter class construction (GGFX::init's job) on the host and
+    on the device: box lattice classes at 32^3 p=7 and coordinate matching
+    at 16^3 and 32^3 p=7 (16.8 M nodes; the host matching is timed at 16^3)."""
+    import ctypes as C
+    import torch
+    from geoflow_b200 import GridBox, _abi as A
+    lib = A.load()
+    out = {}
+
+    def dev_time(fn):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()  # warm-up (allocations, module load)
+        torch.cuda.synchronize()
+        s.record()
+        k = fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / 1e3, k
+
+    ne3 = (C.c_int * 3)(32, 32, 32)
+    per3 = (C.c_int * 3)(0, 0, 0)
+    n = 32 ** 3 * 8 ** 3
+    nc, cp, mem = np.zeros(n, np.int32), np.zeros(n + 1, np.int32), np.zeros(n, np.int32)
+    t0 = time.perf_counter()
+    k = lib.gf_box_classes(3, ne3, 7, per3, A.ptr(nc), A.ptr(cp), A.ptr(mem))
+    th = time.perf_counter() - t0
+    dn = torch.zeros(n, dtype=torch.int32, device="cuda")
+    dc = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    dm = torch.zeros(n, dtype=torch.int32, device="cuda")
+    td, kd = dev_time(lambda: lib.gf_box_classes_device(
+        ctx.handle, 3, ne3, 7, per3, C.c_void_p(dn.data_ptr()), C.c_void_p(dc.data_ptr()),
+        C.c_void_p(dm.data_ptr())))
+    same = kd == k and bool((dm.cpu().numpy() == mem).all())
+    out["box_32cube_p7"] = {"nodes": n, "host_s": th, "device_s": td, "identical": same}
+    for ne in (16, 32):
+        g = GridBox(3, [ne] * 3, 7)
+        N = g.ndof()
+        tol = 0.25 * float(np.min(np.diff(g.xi))) * 0.5 / ne
+        dx = [torch.from_numpy(a).cuda() for a in g.xyz]
+        darr = (C.c_void_p * 3)(*[a.data_ptr() for a in dx])
+        dn = torch.zeros(N, dtype=torch.int32, device="cuda")
+        dc = torch.zeros(N + 1, dtype=torch.int32, device="cuda")
+        dm = torch.zeros(N, dtype=torch.int32, device="cuda")
+        td, kd = dev_time(lambda: lib.gf_classes_from_coords_device(
+            ctx.handle, 3, N, darr, tol, C.c_void_p(dn.data_ptr()), C.c_void_p(dc.data_ptr()),
+            C.c_void_p(dm.data_ptr())))
+        rec = {"nodes": N, "device_s": td, "classes": int(kd)}
+        if ne == 16:
+            nc, cp, mem = np.zeros(N, np.int32), np.zeros(N + 1, np.int32), np.zeros(N, np.int32)
+            arr = (A.P_double * 3)(*[A.ptr(a) for a in g.xyz])
+            t0 = time.perf_counter()
+            k = lib.gf_classes_from_coords(3, N, arr, tol, A.ptr(nc), A.ptr(cp), A.ptr(mem))
+            rec["host_s"] = time.perf_counter() - t0
+            rec["identical"] = kd == k and bool((dm.cpu().numpy() == mem).all())
+        out[f"coords_{ne}cube_p7"] = rec
+    return out
+
+
 def cpu_oracle_iteration_time(sample_ne, p, iters=6):
     """Seconds per FP64 Jacobi-PCG iteration of the CPU oracle (a plain-C
     restatement of GCG::solve_impl + GHelmholtz::reg_prod + GGFX::doOp) on a
@@ -619,6 +678,9 @@ def main():
     if args.only == "graphs":
         print(json.dumps({"only": "graphs", "graphs": graph_bench(ctx)}), flush=True)
         return
+    if args.only == "maps":
+        print(json.dumps({"only": "maps", "index_maps": index_map_bench(ctx)}), flush=True)
+        return
     if args.only == "adjoint":
         print(json.dumps({"only": "adjoint", "adjoint": adjoint_bench(ctx)}), flush=True)
         return
@@ -687,11 +749,12 @@ def main():
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    rk = adj = graphs = None
+    rk = adj = graphs = maps = None
     if not args.no_rk:
         rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p)
         adj = adjoint_bench(ctx)
         graphs = graph_bench(ctx)
+        maps = index_map_bench(ctx)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         t_node, cores, nsample, sne, wall = cpu_allcore_iteration_time(args.p, iters=10)
@@ -737,6 +800,7 @@ def main():
         "rk_stage": rk,
         "adjoint": adj,
         "graphs": graphs,
+        "index_maps": maps,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": per_step_launches * args.steps,

@@ -79,6 +79,10 @@ SIGNATURES = {
     "gf_box_classes": (c_int64, [c_int, P_int, c_int, P_int, P_int32, P_int32, P_int32]),
     "gf_classes_from_coords": (c_int64, [c_int, c_int64, C.POINTER(P_double), c_double, P_int32,
                                          P_int32, P_int32]),
+    "gf_box_classes_device": (c_int64, [c_void_p, c_int, P_int, c_int, P_int, c_void_p, c_void_p,
+                                        c_void_p]),
+    "gf_classes_from_coords_device": (c_int64, [c_void_p, c_int, c_int64, P_void, c_double,
+                                                c_void_p, c_void_p, c_void_p]),
     "gf_problem_create": (c_int, [c_void_p, C.POINTER(ProblemDesc), P_void]),
     "gf_problem_destroy": (c_int, [c_void_p]),
     "gf_problem_sizes": (c_int, [c_void_p, C.POINTER(c_int64), C.POINTER(c_int64)]),

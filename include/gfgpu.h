@@ -116,6 +116,21 @@ int64_t gf_classes_from_coords(int dim, int64_t n, const double *const *xyz,
                                double tol, int32_t *node_class,
                                int32_t *class_ptr, int32_t *members);
 
+/* The same two constructions on the device: identical classes, numbering
+ * and CSR (bit for bit), written into DEVICE arrays node_class[n],
+ * class_ptr[n+1] (the first ncls+1 entries are set) and members[n];
+ * returns the class count or a negative error.  xyz is a host array of dim
+ * DEVICE pointers.  The coordinate matching bins nodes in cells of width
+ * 4 tol (at most 2^21 - 2 cells per direction) and takes, for every node,
+ * the smallest id among the nodes whose tolerance boxes meet its own: the
+ * host's classes whenever matches are transitive (tolerance below half the
+ * node spacing, as GGFX::init requires). */
+int64_t gf_box_classes_device(gf_ctx_t ctx, int dim, const int *ne, int p, const int *periodic,
+                              int32_t *node_class, int32_t *class_ptr, int32_t *members);
+int64_t gf_classes_from_coords_device(gf_ctx_t ctx, int dim, int64_t n,
+                                      const double *const *xyz, double tol, int32_t *node_class,
+                                      int32_t *class_ptr, int32_t *members);
+
 /* ---- problem (grid + operators + gather-scatter map) ---- */
 typedef struct {
   int dim;                 /* 2 or 3 */
