@@ -996,6 +996,12 @@ __global__ void __launch_bounds__(RED_THREADS)
   fcg_finish_fr(rz, scal, partials, counter, sh);
 }
 
+// condition of the solve loop's WHILE graph node: continue while the CG
+// state is not done
+__global__ void k_while_more(cudaGraphConditionalHandle h, const double *scal) {
+  cudaGraphSetConditional(h, scal[S_DONE] == 0.0 ? 1u : 0u);
+}
+
 // deterministic pseudo-random vector in [-1, 1) (zero where masked): the
 // start of the eigenvalue estimates
 __global__ void k_fill_hash(int64_t n, const uint8_t *__restrict__ mask, double *__restrict__ v) {
@@ -1654,14 +1660,14 @@ struct MakeLevel {
 struct MGHier {
   std::vector<MGLevelBase *> lv;
   double key[6] = {0, 0, 0, 0, 0, 0};
-  // CUDA graph of one batch of CG iterations (captured on the first solve
-  // with these vectors and replayed by later batches and solves)
+  // CUDA graph of the whole iteration loop: a WHILE conditional node whose
+  // body is one CG iteration followed by k_while_more (captured on the
+  // first solve with these vectors, replayed by later solves)
   cudaStream_t cs = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   const void *gkey[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  int gevery = 0;
-  uint64_t glaunches = 0;
+  uint64_t glaunches = 0;  // launches per iteration
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -2211,43 +2217,62 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
   GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_d + S_FIRST, prob->scal_h + S_FIRST, sizeof(double),
                                cudaMemcpyHostToDevice, st));
   precondition(st);
-  // A batch of `every` iterations is a fixed sequence of some 130 launches
-  // per iteration (most of them small coarse-level kernels) whose scalars
-  // live on the device, so it is captured once as a CUDA graph and
-  // replayed; iterations past convergence return at once (`done` flag), so
-  // a full batch may be replayed where fewer iterations remain (the
-  // residual history is written only below maxit, which the device holds).
-  const int every = tr.check_every > 0 ? tr.check_every : 16;
+  // The iteration loop runs on the device: a graph holding one WHILE node
+  // whose body is one iteration (some 95 launches, most of them small
+  // coarse-level kernels, all reading their scalars from the device) and
+  // k_while_more, which ends the loop once `done` is set (convergence,
+  // maxit or breakdown) -- no host round trip per iteration and no
+  // iterations queued past convergence.
   const void *gk[7] = {xL, rL, w, qL, qE, bL, hist};
-  if (!(H->exec && H->gevery == every && std::equal(gk, gk + 7, H->gkey))) {
+  if (!(H->exec && std::equal(gk, gk + 7, H->gkey))) {
     H->drop_graph();
     if (!H->cs) GF_CUDA(ctx, cudaStreamCreateWithFlags(&H->cs, cudaStreamNonBlocking));
     const uint64_t n0 = level_launches();
-    cudaError_t e = cudaStreamBeginCapture(H->cs, cudaStreamCaptureModeRelaxed);
+    cudaGraph_t g = nullptr, body = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
     if (e == cudaSuccess) {
-      iterations(every, H->cs);
-      e = cudaStreamEndCapture(H->cs, &H->graph);
+      body = np.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(H->cs, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeRelaxed);
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&H->exec, H->graph, 0);
-    H->glaunches = level_launches() - n0;
+    if (e == cudaSuccess) {
+      iterations(1, H->cs);
+      k_while_more<<<1, 1, 0, H->cs>>>(h, scal);
+      e = cudaStreamEndCapture(H->cs, &body);
+    }
+    H->graph = g;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&H->exec, g, 0);
+    H->glaunches = level_launches() - n0 + 1;
     for (size_t l = 1; l < H->lv.size(); l++) H->lv[l]->prob->launches = 0;
     prob->launches = n0;
     if (e != cudaSuccess) {
       H->drop_graph();
-      return gf_fail(ctx, GF_ERR_CUDA, "CG batch capture failed: %s", cudaGetErrorString(e));
+      return gf_fail(ctx, GF_ERR_CUDA, "CG loop capture failed: %s", cudaGetErrorString(e));
     }
-    H->gevery = every;
     std::copy(gk, gk + 7, H->gkey);
   }
-  rc = S.batches(tr, tr.maxit, total, [&](int) {
-    cudaGraphLaunch(H->exec, st);
-    prob->launches += H->glaunches;
-  });
+  GF_CUDA(ctx, cudaGraphLaunch(H->exec, st));
+  GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h, scal, sizeof(double) * S_COUNT,
+                               cudaMemcpyDeviceToHost, st));
+  GF_CUDA(ctx, cudaStreamSynchronize(st));
+  *total = (int)prob->scal_h[S_ITER];
+  prob->launches += H->glaunches * (uint64_t)std::max(1, *total);
   for (size_t l = 1; l < H->lv.size(); l++) {  // the levels' applies count as this problem's
     prob->launches += H->lv[l]->prob->launches;
     H->lv[l]->prob->launches = 0;
   }
-  if (rc) return rc;
+  if (prob->scal_h[S_FLAG] != 0.0)
+    return gf_fail(ctx, GF_ERR_NONFINITE, "CG breakdown: non-finite scalar at iteration %d",
+                   *total);
   *rn = prob->scal_h[S_RNORM];
   return (*total >= tr.maxit && *rn > prob->scal_h[S_RTOL]) ? GF_CG_NOCONVERGE : GF_OK;
 }
