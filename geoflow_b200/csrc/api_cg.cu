@@ -799,6 +799,11 @@ __global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1
                          const uint8_t *__restrict__ mask, int mode, const double *stop) {
   if (stop && *stop != 0.0) return;
   const int R = T.R, pc = T.pc, nc = T.pc + 1, nec = T.nec;
+  // the weights in shared memory: along x the threads of a warp read
+  // different rows, which the constant (parameter) bank would serialise
+  __shared__ float J[MG_XR * GF_MAXN];
+  for (int i = threadIdx.x; i < (R + 1) * nc; i += blockDim.x) J[i] = T.J[i];
+  __syncthreads();
   // lattice sizes are below 2^31 (32-bit index arithmetic)
   const int n32 = (int)nout;
   for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n32; o += gridDim.x * blockDim.x) {
@@ -827,24 +832,24 @@ __global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1
       for (int a = 0; a < nc; a++) {
         int c = ec * pc + a;
         if (c >= T.Mc) c -= T.Mc;
-        s = fmaf(T.J[r * nc + a], in[base + c * stride], s);
+        s = fmaf(J[r * nc + a], in[base + c * stride], s);
       }
     } else {  // coarse point gd = ec pc + a
       const int ec = gd / pc, a = gd - ec * pc;
       if (a != 0) {
         for (int r = 1; r < R; r++)
-          s = fmaf(T.J[r * nc + a], in[base + (ec * R + r) * stride], s);
+          s = fmaf(J[r * nc + a], in[base + (ec * R + r) * stride], s);
       } else {
         s = in[base + (ec * R) * stride];  // the coinciding vertex
         const bool left = ec > 0 || T.per, right = ec < nec;
         if (left) {
           const int el = ec > 0 ? ec - 1 : nec - 1;
           for (int r = 1; r < R; r++)
-            s = fmaf(T.J[r * nc + pc], in[base + (el * R + r) * stride], s);
+            s = fmaf(J[r * nc + pc], in[base + (el * R + r) * stride], s);
         }
         if (right)
           for (int r = 1; r < R; r++)
-            s = fmaf(T.J[r * nc], in[base + (ec * R + r) * stride], s);
+            s = fmaf(J[r * nc], in[base + (ec * R + r) * stride], s);
       }
     }
     if (mode == 2 && mask && !mask[o]) s = 0.0f;
