@@ -5,8 +5,9 @@ the Python host-side mirror of the reference interfaces over that ABI.
 """
 from . import _abi, gio
 from ._abi import GFError, load
-from .sem import (CGTraits, Context, GBurgers, GCG, GGFX, GHelmholtz, GMass, Graph, GridBox,
-                  Problem, gll_basis)
+from .sem import (CGTraits, Context, GBoydFilter, GBurgers, GCG, GGFX, GHelmholtz, GMass,
+                  GProjectionFilter, Graph, GridBox, Problem, filter_matrix, gll_basis)
 
-__all__ = ["GFError", "load", "CGTraits", "Context", "GBurgers", "GCG", "GGFX", "GHelmholtz",
-           "GMass", "Graph", "GridBox", "Problem", "gll_basis", "_abi", "gio"]
+__all__ = ["GFError", "load", "CGTraits", "Context", "GBoydFilter", "GBurgers", "GCG", "GGFX",
+           "GHelmholtz", "GMass", "GProjectionFilter", "Graph", "GridBox", "Problem",
+           "filter_matrix", "gll_basis", "_abi", "gio"]

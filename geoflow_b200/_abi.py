@@ -28,6 +28,7 @@ GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV, GF_PRECOND_PMG = 0, 1,
 GF_CG_FP64, GF_CG_MIXED = 0, 1
 GF_GEOM_AFFINE, GF_GEOM_REGULAR, GF_GEOM_DEFORMED, GF_GEOM_EMBEDDED = 0, 1, 2, 3
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
+GF_FILTER_BOYD, GF_FILTER_PROJECTION = 0, 1
 GF_RK1, GF_RK2, GF_RK3, GF_RK4, GF_SSP22, GF_SSP33, GF_SSP34 = 1, 2, 3, 4, 22, 33, 34
 # gf_integrate_noalloc: fixed scratch of GF_NOALLOC_MAX_BLOCKS blocks of GF_NOALLOC_CHUNK
 GF_NOALLOC_CHUNK, GF_NOALLOC_MAX_BLOCKS = 4096, 32768
@@ -114,6 +115,8 @@ SIGNATURES = {
                                 c_void_p]),
     "gf_rk_graph_create": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
                                    c_int, P_void]),
+    "gf_filter_matrix": (c_int, [c_int, c_int, c_int, c_double, P_double]),
+    "gf_filter_apply": (c_int, [c_void_p, c_int, P_double, P_double, P_double, c_int, P_void]),
     "gf_gio_header_bytes": (c_int64, [c_int, c_int, C.c_uint64, c_int]),
     "gf_gio_write": (c_int, [c_void_p, C.c_char_p, C.POINTER(GioHeader), c_void_p, c_void_p,
                              c_int, c_void_p, C.c_uint64]),

@@ -157,3 +157,26 @@ extern "C" int gf_tensor_apply(gf_problem_t prob, int dtype, const double *A1, c
   GF_CHECK_LAUNCH(ctx);
   return GF_OK;
 }
+
+// Spectral filter in place: the tensor kernel reads each element's values
+// before writing any of them, and no other block reads the element.
+extern "C" int gf_filter_apply(gf_problem_t prob, int dtype, const double *F1, const double *F2,
+                               const double *F3, int ncomp, void *const *u) {
+  if (!prob) return GF_ERR_ARG;
+  gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, F1 && F2 && (prob->dim == 2 || F3) && u && ncomp >= 1, "bad arguments");
+  const double *A[3] = {F1, F2, prob->dim == 3 ? F3 : F1};
+  for (int k = 0; k < ncomp; k++) {
+    GF_REQUIRE(ctx, u[k], "component %d missing", k);
+    int rc = dtype == GF_F64
+                 ? dispatch_n<TensorLaunch<double>::template F>(prob->n, prob, A, (const double *)u[k],
+                                                               (double *)u[k], ctx->stream)
+             : dtype == GF_F32
+                 ? dispatch_n<TensorLaunch<float>::template F>(prob->n, prob, A, (const float *)u[k],
+                                                              (float *)u[k], ctx->stream)
+                 : GF_ERR_ARG;
+    if (rc) return gf_fail(ctx, rc, "filter apply failed");
+  }
+  GF_CHECK_LAUNCH(ctx);
+  return GF_OK;
+}

@@ -256,6 +256,58 @@ def tensor_apply(prob: Problem, A1, A2, A3, u, out):
                    "tensor_apply")
 
 
+def filter_matrix(kind: int, p: int, pdelta: int, strength: float) -> np.ndarray:
+    """The (p+1) x (p+1) 1-d filter matrix of GBoydFilter::init
+    (kind GF_FILTER_BOYD) or GProjectionFilter::init (GF_FILTER_PROJECTION)."""
+    F = np.zeros((p + 1) * (p + 1))
+    rc = _lib().gf_filter_matrix(kind, p, pdelta, strength, A.ptr(F))
+    if rc < 0:
+        raise A.GFError(rc, "gf_filter_matrix")
+    return F.reshape(p + 1, p + 1, order="F")
+
+
+class _Filter:
+    """FilterBase over the library's in-place tensor filter: traits istate
+    (state ids to filter; empty = all), pdelta and strength per direction."""
+    KIND = A.GF_FILTER_BOYD
+
+    def __init__(self, prob: Problem, pdelta, strength, istate=None):
+        dim = prob.dim
+        pd = [int(pdelta)] * dim if np.isscalar(pdelta) else [int(v) for v in pdelta][:dim]
+        st = [float(strength)] * dim if np.isscalar(strength) else [float(v) for v in strength][:dim]
+        if not all(0.0 <= v <= 1.0 for v in st):
+            raise ValueError("filter strength must lie in [0, 1]")
+        self.prob, self.istate = prob, list(istate or [])
+        self.F = [filter_matrix(self.KIND, prob.n - 1, pd[d], st[d]) for d in range(dim)]
+        self._flat = [np.ascontiguousarray(f.ravel(order="F")) for f in self.F]
+
+    def apply(self, u, utmp=None, uo=None):
+        """In place on the state list u (the selected components), or with
+        uo given, out of place (u unchanged)."""
+        ids = self.istate or list(range(len(u)))
+        if uo is not None:
+            for j in ids:
+                uo[j].copy_(u[j])
+            target = uo
+        else:
+            target = u
+        comps = [target[j] for j in ids]
+        f3 = self._flat[2] if self.prob.dim == 3 else None
+        self.prob.ctx.check(_lib().gf_filter_apply(
+            self.prob.handle, _dtype_code(comps[0]), A.ptr(self._flat[0]), A.ptr(self._flat[1]),
+            A.ptr(f3), len(comps), A.ptr_array(comps)), "Filter::apply")
+
+
+class GBoydFilter(_Filter):
+    """GBoydFilter (sem/gboyd_filter.ipp): u <- (F x F x F) u, F = L Lambda L^-1."""
+    KIND = A.GF_FILTER_BOYD
+
+
+class GProjectionFilter(_Filter):
+    """GProjectionFilter (sem/gprojection_filter.ipp): F = a Ihi Ilow + (1-a) I."""
+    KIND = A.GF_FILTER_PROJECTION
+
+
 class GMass:
     """Lumped mass W x W (x W) x Jac; inverse=True uses 1/Smooth(M)."""
 
@@ -374,11 +426,25 @@ class GBurgers:
                                         len(u), A.ptr_array(u), A.ptr_array(c or []),
                                         A.ptr_array(dudt)), "GBurgers::dudt")
 
-    def step(self, u, c=None, dt=1e-4, nsteps=1, t0=0.0):
+    def step(self, u, c=None, dt=1e-4, nsteps=1, t0=0.0, filters=None):
+        """nsteps steps in place; with `filters` (a filter list, as
+        EquationBase::set_filter_list) each filter is applied in place after
+        every step, as GMConv::step_impl does (gmconv.ipp:648-653)."""
         tr = self.traits()
-        self.prob.ctx.check(_lib().gf_rk_advance(self.prob.handle, _dtype_code(u[0]), C.byref(tr),
-                                                 A.ptr_array(u), A.ptr_array(c or []), t0, dt,
-                                                 nsteps), "GBurgers::step")
+        if not filters:
+            self.prob.ctx.check(_lib().gf_rk_advance(self.prob.handle, _dtype_code(u[0]),
+                                                     C.byref(tr), A.ptr_array(u),
+                                                     A.ptr_array(c or []), t0, dt, nsteps),
+                                "GBurgers::step")
+            return
+        for k in range(nsteps):
+            self.prob.ctx.check(_lib().gf_rk_advance(self.prob.handle, _dtype_code(u[0]),
+                                                     C.byref(tr), A.ptr_array(u),
+                                                     A.ptr_array(c or []), t0 + k * dt, dt, 1),
+                                "GBurgers::step")
+            for f in filters:
+                if f is not None:
+                    f.apply(u)
 
     def capture(self, u, c=None, dt=1e-4, nsteps=1):
         """Record `nsteps` steps advancing u in place as a CUDA graph

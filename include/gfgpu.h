@@ -302,6 +302,21 @@ int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
 int gf_integrate_noalloc(int64_t n, const double *mass, const double *u, double *result,
                          void *stream);
 
+/* ---- spectral filters (sem/gboyd_filter.ipp, sem/gprojection_filter.ipp) ----
+ * gf_filter_matrix: the 1-d filter matrix of order p, column-major
+ * F[i + j*(p+1)], as GBoydFilter::init (pdelta: filtered modes above
+ * ifilter = p - pdelta, strength mu in [0, 1]) or GProjectionFilter::init
+ * (projection to order p - pdelta, 1 <= pdelta <= p/2, blended with
+ * strength).  Host only; p = 1 bases are allowed here (the reference's
+ * GLLBasis asserts on them).  gf_filter_apply: u_k <- (F3 (x) F2 (x) F1) u_k
+ * in every element for the ncomp device fields u (FilterBase::apply in
+ * place; the filters' D3_X_D2_X_D1(F, F^T, F^T) with a matrix per direction,
+ * F3 ignored in 2-d; GMConv applies its filter list after each step). */
+enum { GF_FILTER_BOYD = 0, GF_FILTER_PROJECTION = 1 };
+int gf_filter_matrix(int kind, int p, int pdelta, double strength, double *F);
+int gf_filter_apply(gf_problem_t prob, int dtype, const double *F1, const double *F2,
+                    const double *F3, int ncomp, void *const *u);
+
 /* ---- GIO state files (io/gio.ipp POSIX format) ----
  * One field of one rank per file: the GIO header (io/gio.ipp:459-503)
  * followed by the field's values, straight from / into device memory

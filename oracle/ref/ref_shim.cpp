@@ -61,4 +61,48 @@ int gfr_gmtk(int which, const double *A, const double *B, const double *C,
   return 0;
 }
 
+// Boyd filter matrix, column-major, as GBoydFilter::init
+// (sem/gboyd_filter.ipp:150-200) computes it from the basis' Legendre
+// transform: F = L Lambda L^-1 (the compiled Lambda branch).
+int gfr_boyd_filter(int p, int pdelta, double strength, double *F) {
+  GLLBasis<GCTYPE, GFTYPE> b(p);
+  GTMatrix<GFTYPE> *L = b.getLegTransform(), *iL = b.getiLegTransform();
+  const int n = p + 1, ifilter = n - pdelta - 1;
+  if (!(ifilter > 0 && ifilter < n)) return -1;
+  GTMatrix<GFTYPE> Lambda(n, n), tmp(n, n), Fm(n, n);
+  Lambda = 0.0;
+  for (int i = 0; i < n; i++) {
+    Lambda(i, i) = 1.0;
+    if (i >= ifilter)
+      Lambda(i, i) = strength * pow(fabs((GFTYPE)(i - ifilter) / ((GFTYPE)(n - ifilter))), 2.0);
+  }
+  tmp = Lambda * (*iL);
+  Fm = (*L) * tmp;
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++) F[i + j * n] = Fm(i, j);
+  return 0;
+}
+
+// Projection filter matrix, column-major, as GProjectionFilter::init
+// (sem/gprojection_filter.ipp:156-202).
+int gfr_projection_filter(int p, int pdelta, double strength, double *F) {
+  GLLBasis<GCTYPE, GFTYPE> hi(p);
+  const int n = p + 1, nlow = n - pdelta;
+  if (!(pdelta >= 1 && pdelta <= (n - 1) / 2)) return -1;
+  GLLBasis<GCTYPE, GFTYPE> lo(nlow - 1);
+  GTVector<GFTYPE> xihi, xilow;
+  hi.getXiNodes(xihi);
+  lo.getXiNodes(xilow);
+  GTMatrix<GFTYPE> Ilow(nlow, n), Ihi(n, nlow), M(n, n), Fm(n, n), Id(n, n);
+  Id.createIdentity();
+  hi.evalBasis(xilow, Ilow);
+  lo.evalBasis(xihi, Ihi);
+  M = Ihi * Ilow;
+  Fm = M * strength;
+  Fm += (Id * (1.0 - strength));
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++) F[i + j * n] = Fm(i, j);
+  return 0;
+}
+
 }  // extern "C"
