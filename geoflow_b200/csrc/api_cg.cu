@@ -858,6 +858,144 @@ __global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1
   }
 }
 
+// ---- transfers between p-levels (same elements), one element per
+// thread-block slot: with P = J (x) J (x) J element by element (J the
+// NF x NC interpolation of Xfer1D with ratio 1), no 1-d sweeps and no
+// intermediate lattices.  3-d box lattices.
+//
+// lattice index of local point (l0, l1, l2) of the element at (c0, c1, c2)
+__device__ __forceinline__ int elem_lattice(const BoxLattice &L, int c0, int c1, int c2, int l0,
+                                            int l1, int l2) {
+  const int P = L.p, M0 = (int)L.M[0], M1 = (int)L.M[1], M2 = (int)L.M[2];
+  int g0 = c0 * P + l0, g1 = c1 * P + l1, g2 = c2 * P + l2;
+  if (L.per[0] && g0 == M0) g0 = 0;
+  if (L.per[1] && g1 == M1) g1 = 0;
+  if (L.per[2] && g2 == M2) g2 = 0;
+  return g0 + M0 * (g1 + M1 * g2);
+}
+
+// prolongation x_f += P x_c: gather the coarse element, contract along x,
+// y, z in shared memory, add into the fine lattice points the element owns
+// (local index < P, or P on a non-periodic upper face), so each point is
+// written once.
+template <int NF>
+__global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF * NF)))
+    k_pxfer_prolong(BoxLattice Lf, BoxLattice Lc, const __grid_constant__ Xfer1D T,
+                    const float *__restrict__ xc, float *__restrict__ xf, const double *stop) {
+  constexpr int NC = NF / 2 + 1, PF = NF - 1, NT = NF * NF;
+  constexpr int EPB = (256 / NT) < 1 ? 1 : 256 / NT;
+  constexpr int S0 = NC * NC * NC, S1 = NF * NC * NC, S2 = NF * NF * NC;
+  __shared__ float J[NF * NC];
+  __shared__ float sm[EPB][S0 + S1 + S2];
+  if (stop && *stop != 0.0) return;
+  const int t = threadIdx.x, slot = threadIdx.y;
+  for (int i = t + NT * slot; i < NF * NC; i += NT * EPB) J[i] = T.J[i];
+  const int ne0 = Lf.ne[0], ne1 = Lf.ne[1], ne2 = Lf.ne[2];
+  const int nel = ne0 * ne1 * ne2;
+  const int e = blockIdx.x * EPB + slot;
+  const bool active = e < nel;
+  const int c0 = e % ne0, r = e / ne0, c1 = r % ne1, c2 = r / ne1;
+  float *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
+  if (active)
+    for (int i = t; i < S0; i += NT) {
+      const int a = i % NC, b = (i / NC) % NC, c = i / (NC * NC);
+      s0[i] = xc[elem_lattice(Lc, c0, c1, c2, a, b, c)];
+    }
+  __syncthreads();
+  if (active)
+    for (int i = t; i < S1; i += NT) {  // s1[c][b][i0] = sum_a J[i0][a] s0[c][b][a]
+      const int i0 = i % NF, cb = i / NF;
+      float v = 0.0f;
+#pragma unroll
+      for (int a = 0; a < NC; a++) v = fmaf(J[i0 * NC + a], s0[cb * NC + a], v);
+      s1[i] = v;
+    }
+  __syncthreads();
+  if (active)
+    for (int i = t; i < S2; i += NT) {  // s2[c][j][i0] = sum_b J[j][b] s1[c][b][i0]
+      const int i0 = i % NF, j = (i / NF) % NF, c = i / (NF * NF);
+      float v = 0.0f;
+#pragma unroll
+      for (int b = 0; b < NC; b++) v = fmaf(J[j * NC + b], s1[(c * NC + b) * NF + i0], v);
+      s2[i] = v;
+    }
+  __syncthreads();
+  if (!active) return;
+  const int i0 = t % NF, j = t / NF;
+  if (i0 == PF && (Lf.per[0] || c0 != ne0 - 1)) return;
+  if (j == PF && (Lf.per[1] || c1 != ne1 - 1)) return;
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    if (k == PF && (Lf.per[2] || c2 != ne2 - 1)) continue;
+    float v = 0.0f;
+#pragma unroll
+    for (int c = 0; c < NC; c++) v = fmaf(J[k * NC + c], s2[(c * NF + j) * NF + i0], v);
+    xf[elem_lattice(Lf, c0, c1, c2, i0, j, k)] += v;
+  }
+}
+
+// restriction into the coarse E-vector: q_c(e) = (J^T (x) J^T (x) J^T)
+// (w r_f)(e), w = 1/(number of elements sharing the fine point), so that
+// folding q_c's copies over the coarse lattice gives P^T r_f.
+template <int NF>
+__global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF * NF)))
+    k_pxfer_restrict(BoxLattice Lf, const __grid_constant__ Xfer1D T,
+                     const float *__restrict__ rf, float *__restrict__ qc, const double *stop) {
+  constexpr int NC = NF / 2 + 1, PF = NF - 1, NT = NF * NF;
+  constexpr int EPB = (256 / NT) < 1 ? 1 : 256 / NT;
+  constexpr int S0 = NF * NF * NF, S1 = NC * NF * NF, S2 = NC * NC * NF;
+  __shared__ float J[NF * NC];
+  __shared__ float sm[EPB][S0 + S1 + S2];
+  if (stop && *stop != 0.0) return;
+  const int t = threadIdx.x, slot = threadIdx.y;
+  for (int i = t + NT * slot; i < NF * NC; i += NT * EPB) J[i] = T.J[i];
+  const int ne[3] = {Lf.ne[0], Lf.ne[1], Lf.ne[2]};
+  const int nel = ne[0] * ne[1] * ne[2];
+  const int e = blockIdx.x * EPB + slot;
+  const bool active = e < nel;
+  const int cc[3] = {e % ne[0], (e / ne[0]) % ne[1], e / (ne[0] * ne[1])};
+  float *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
+  if (active)
+    for (int i = t; i < S0; i += NT) {
+      const int l[3] = {i % NF, (i / NF) % NF, i / (NF * NF)};
+      float w = 1.0f;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const bool shared = (l[d] == 0 && (Lf.per[d] || cc[d] > 0)) ||
+                            (l[d] == PF && (Lf.per[d] || cc[d] < ne[d] - 1));
+        if (shared) w *= 0.5f;
+      }
+      s0[i] = w * rf[elem_lattice(Lf, cc[0], cc[1], cc[2], l[0], l[1], l[2])];
+    }
+  __syncthreads();
+  if (active)
+    for (int i = t; i < S1; i += NT) {  // s1[k][j][a] = sum_i0 J[i0][a] s0[k][j][i0]
+      const int a = i % NC, kj = i / NC;
+      float v = 0.0f;
+#pragma unroll
+      for (int i0 = 0; i0 < NF; i0++) v = fmaf(J[i0 * NC + a], s0[kj * NF + i0], v);
+      s1[i] = v;
+    }
+  __syncthreads();
+  if (active)
+    for (int i = t; i < S2; i += NT) {  // s2[k][b][a] = sum_j J[j][b] s1[k][j][a]
+      const int a = i % NC, b = (i / NC) % NC, k = i / (NC * NC);
+      float v = 0.0f;
+#pragma unroll
+      for (int j = 0; j < NF; j++) v = fmaf(J[j * NC + b], s1[(k * NF + j) * NC + a], v);
+      s2[i] = v;
+    }
+  __syncthreads();
+  if (!active) return;
+  for (int i = t; i < NC * NC * NC; i += NT) {  // q[c][b][a] = sum_k J[k][c] s2[k][b][a]
+    const int ab = i % (NC * NC), c = i / (NC * NC);
+    float v = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NF; k++) v = fmaf(J[k * NC + c], s2[k * NC * NC + ab], v);
+    qc[(int64_t)e * (NC * NC * NC) + i] = v;
+  }
+}
+
 // Chebyshev smoothing of A x = b from x = 0 (the recurrence of k_cheb_*):
 // res = b, d = c0 Dinv res, x = d.  With r64 the level's b is first taken
 // from the FP64 outer residual.
@@ -883,7 +1021,10 @@ __global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, float *__
 //                          (smoothing of the residual equation from an existing x)
 // DOTS (last pass of the finest level): <b, x> (b = the FP32 copy of the
 // outer residual) for the CG step, finished by fcg_finish_fr.
-enum { MG_STEP = 0, MG_RESID = 1, MG_RESTART = 2 };
+//   MG_START    qE = a coarse E-vector (the element restriction's output):
+//               b = s; res = b; d = c1 Dinv b; x = d  (smoothing from zero)
+//   MG_FOLDB    b = s only (a dense coarsest level)
+enum { MG_STEP = 0, MG_RESID = 1, MG_RESTART = 2, MG_START = 3, MG_FOLDB = 4 };
 
 // The passes run on the box lattice, one thread per lattice point in
 // lattice order: the state vectors stream fully coalesced (a warp reads 128
@@ -940,7 +1081,7 @@ __device__ __forceinline__ int lattice_cands(int g, int ne, int per, int (&ec)[2
 template <int N, int MODE, bool DOTS>
 __global__ void __launch_bounds__(RED_THREADS)
     k_mg_pass_lat(MapBox<N> map, Weights wt, const float *__restrict__ qE,
-                  const float *__restrict__ b, const float *__restrict__ dinv, float c1, float c2,
+                  float *__restrict__ b, const float *__restrict__ dinv, float c1, float c2,
                   float *__restrict__ res, float *__restrict__ d, float *__restrict__ x, int LB,
                   double *scal, double *partials, unsigned int *counter) {
   __shared__ double sh[32];
@@ -980,6 +1121,18 @@ __global__ void __launch_bounds__(RED_THREADS)
     if (wt.maskL && !wt.maskL[c]) s = 0.0f;
     if (MODE == MG_RESID) {
       res[c] = res[c] - s;
+      continue;
+    }
+    if (MODE == MG_FOLDB) {
+      b[c] = s;
+      continue;
+    }
+    if (MODE == MG_START) {
+      const float dc0 = c1 * (dinv[c] * s);
+      b[c] = s;
+      res[c] = s;
+      d[c] = dc0;
+      x[c] = dc0;
       continue;
     }
     float rc, dc;
@@ -1558,6 +1711,11 @@ struct MGLevelBase {
                     cudaStream_t st) = 0;
   virtual int jacobi(double p, double q, int use_mass) = 0;
   virtual int estimate(double p, double q, int use_mass, int64_t nfree) = 0;
+  // element-wise transfers to the next coarser level when it has the same
+  // elements (p-coarsening, 3-d): restriction into C.qE, prolongation into x
+  bool ptransfer = false;
+  virtual void restrict_elem(MGLevelBase &C, gf_problem *outer, cudaStream_t st) = 0;
+  virtual void prolong_elem(const MGLevelBase &C, gf_problem *outer, cudaStream_t st) = 0;
 };
 
 template <int N>
@@ -1591,10 +1749,26 @@ struct MGLevel : MGLevelBase {
             cudaStream_t st) override {
     outer->launches++;
     if (mode == MG_RESID) run_pass<MG_RESID, false>(a1, a2, outer, st);
+    else if (mode == MG_START) run_pass<MG_START, false>(a1, a2, outer, st);
+    else if (mode == MG_FOLDB) run_pass<MG_FOLDB, false>(a1, a2, outer, st);
     else if (mode == MG_STEP && dots) run_pass<MG_STEP, true>(a1, a2, outer, st);
     else if (mode == MG_STEP) run_pass<MG_STEP, false>(a1, a2, outer, st);
     else if (dots) run_pass<MG_RESTART, true>(a1, a2, outer, st);
     else run_pass<MG_RESTART, false>(a1, a2, outer, st);
+  }
+  void restrict_elem(MGLevelBase &C, gf_problem *outer, cudaStream_t st) override {
+    constexpr int NT = N * N, EPB = (256 / NT) < 1 ? 1 : 256 / NT;
+    const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+    outer->launches++;
+    k_pxfer_restrict<N><<<grid, dim3(NT, EPB), 0, st>>>(prob->box, X[0], res, C.qE,
+                                                        outer->scal_d + S_DONE);
+  }
+  void prolong_elem(const MGLevelBase &C, gf_problem *outer, cudaStream_t st) override {
+    constexpr int NT = N * N, EPB = (256 / NT) < 1 ? 1 : 256 / NT;
+    const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+    outer->launches++;
+    k_pxfer_prolong<N><<<grid, dim3(NT, EPB), 0, st>>>(prob->box, C.prob->box, X[0], C.x, x,
+                                                       outer->scal_d + S_DONE);
   }
   int jacobi(double p, double q, int use_mass) override {
     double *d64 = nullptr;
@@ -2075,6 +2249,10 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
         MGLevelBase *F = H->lv[l - 1];
         for (int k = 0; k < dim; k++)
           F->X[k] = build_xfer(ds[l - 1].ne[k], ds[l - 1].p, ds[l].ne[k], ds[l].p, B.per[k] != 0);
+        // same elements, coarse order as the element kernels assume
+        F->ptransfer = dim == 3 && ds[l - 1].ne[0] == ds[l].ne[0] &&
+                       ds[l - 1].ne[1] == ds[l].ne[1] && ds[l - 1].ne[2] == ds[l].ne[2] &&
+                       ds[l].p + 1 == (ds[l - 1].p + 1) / 2 + 1;
         // sweep intermediates: restriction (c, f, f), (c, c, f); prolongation
         // (f, c, c), (f, f, c)
         const int64_t f0 = F->M[0], f1 = F->M[1], f2 = F->M[2];
@@ -2142,15 +2320,22 @@ void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem
   MGLevelBase &L = *H.lv[l];
   const double *stop = outer->scal_d + S_DONE;
   const bool top = l == 0, last = l + 1 == H.lv.size();
+  // b arrives as the element restriction's coarse E-vector in L.qE
+  const bool folded = l > 0 && H.lv[l - 1]->ptransfer;
   if (last && L.ainv) {  // coarsest: dense solve (never the finest level)
+    if (folded) L.pass(MG_FOLDB, false, 0.0f, 0.0f, outer, st);
     k_dense_solve<<<(unsigned)std::min<int64_t>(L.nfree, 148 * 8), 128, 0, st>>>(
         L.nfree, L.ainv, L.free_idx, L.b, L.x, stop);
     outer->launches++;
     return;
   }
-  k_mg_start<<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(L.nL, top ? r64 : nullptr, L.b, L.dinv,
-                                                          L.c0, L.res, L.d, L.x, stop);
-  outer->launches++;
+  if (folded) {
+    L.pass(MG_START, false, L.c0, 0.0f, outer, st);
+  } else {
+    k_mg_start<<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(
+        L.nL, top ? r64 : nullptr, L.b, L.dinv, L.c0, L.res, L.d, L.x, stop);
+    outer->launches++;
+  }
   if (last) {  // coarsest: Chebyshev solve from zero
     for (int j = 1; j <= L.m; j++) {
       L.apply(L.d, p, q, use_mass, stop, st);
@@ -2164,9 +2349,11 @@ void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem
   }
   L.apply(L.d, p, q, use_mass, stop, st);  // res = b - A x
   L.pass(MG_RESID, false, 0.0f, 0.0f, outer, st);
-  mg_restrict(L, *H.lv[l + 1], outer, st);
+  if (L.ptransfer) L.restrict_elem(*H.lv[l + 1], outer, st);
+  else mg_restrict(L, *H.lv[l + 1], outer, st);
   mg_vcycle(H, l + 1, p, q, use_mass, outer, r64, st);
-  mg_prolong(L, *H.lv[l + 1], outer, st);
+  if (L.ptransfer) L.prolong_elem(*H.lv[l + 1], outer, st);
+  else mg_prolong(L, *H.lv[l + 1], outer, st);
   L.apply(L.x, p, q, use_mass, stop, st);  // post-smoothing x += S (b - A x)
   L.pass(MG_RESTART, top && L.m == 0, L.c0, 0.0f, outer, st);
   for (int j = 1; j <= L.m; j++) {
