@@ -518,28 +518,12 @@ __global__ void __launch_bounds__(RED_THREADS)
   }
 }
 
-// 3. x += alpha w; r -= alpha q; rho' = <r, Dinv r>; norm(r); beta; stop test
-template <typename T, class MAP>
-__global__ void __launch_bounds__(RED_THREADS)
-    k_update(int64_t nL, MAP map, Weights wt, T *__restrict__ x, const T *__restrict__ w,
-             T *__restrict__ r, const T *__restrict__ q, const float *__restrict__ dinv,
-             double *__restrict__ hist, double *__restrict__ ab, int nab, double *scal,
-             double *partials, unsigned int *counter) {
-  __shared__ double sh[32];
-  if (scal[S_DONE] != 0.0) return;
-  const int normtype = (int)scal[S_NORMT];
-  const T alpha = (T)scal[S_ALPHA];
-  double rho = 0.0, rn = 0.0;
-  // plain streaming over the unique nodes (no lattice information needed)
-  GRID_STRIDE(c, nL) {
-    x[c] = x[c] + alpha * w[c];
-    const T rc = r[c] + (-alpha) * q[c];
-    r[c] = rc;
-    const T zc = dinv ? (T)dinv[c] * rc : rc;
-    rho += (double)rc * (double)zc;
-    const double t = norm_term_L(normtype, (double)rc, wt, c);
-    rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
-  }
+// grid-wide finish of the x/r update: rho' and norm(r) from the block
+// partials; beta; the residual history; the stop test
+__device__ __forceinline__ void update_finish(double rho, double rn, int normtype,
+                                              double *__restrict__ hist, double *__restrict__ ab,
+                                              int nab, double *scal, double *partials,
+                                              unsigned int *counter, double *sh) {
   rho = block_reduce<false>(rho, sh);
   rn = normtype == GF_NORM_INF ? block_reduce<true>(rn, sh) : block_reduce<false>(rn, sh);
   double pv[2] = {rho, rn};
@@ -566,6 +550,60 @@ __global__ void __launch_bounds__(RED_THREADS)
       *counter = 0;
     }
   }
+}
+
+// 3. x += alpha w; r -= alpha q; rho' = <r, Dinv r>; norm(r); beta; stop test
+template <typename T, class MAP>
+__global__ void __launch_bounds__(RED_THREADS)
+    k_update(int64_t nL, MAP map, Weights wt, T *__restrict__ x, const T *__restrict__ w,
+             T *__restrict__ r, const T *__restrict__ q, const float *__restrict__ dinv,
+             double *__restrict__ hist, double *__restrict__ ab, int nab, double *scal,
+             double *partials, unsigned int *counter) {
+  __shared__ double sh[32];
+  if (scal[S_DONE] != 0.0) return;
+  const int normtype = (int)scal[S_NORMT];
+  const T alpha = (T)scal[S_ALPHA];
+  double rho = 0.0, rn = 0.0;
+  // plain streaming over the unique nodes (no lattice information needed)
+  GRID_STRIDE(c, nL) {
+    x[c] = x[c] + alpha * w[c];
+    const T rc = r[c] + (-alpha) * q[c];
+    r[c] = rc;
+    const T zc = dinv ? (T)dinv[c] * rc : rc;
+    rho += (double)rc * (double)zc;
+    const double t = norm_term_L(normtype, (double)rc, wt, c);
+    rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
+  }
+  update_finish(rho, rn, normtype, hist, ab, nab, scal, partials, counter, sh);
+}
+
+// k_update of the multigrid-preconditioned CG (FP64, no Jacobi weight),
+// which also takes the first smoothing term of the next V-cycle on the new
+// residual (k_mg_start's work: b32 = (float) r, x32 = c0 Dinv32 b32) while r
+// is in registers.  Points written after convergence are never read.
+__global__ void __launch_bounds__(RED_THREADS)
+    k_update_mg(int64_t nL, Weights wt, double *__restrict__ x, const double *__restrict__ w,
+                double *__restrict__ r, const double *__restrict__ q,
+                const float *__restrict__ dinv32, float c0, float *__restrict__ b32,
+                float *__restrict__ x32, double *__restrict__ hist, double *scal,
+                double *partials, unsigned int *counter) {
+  __shared__ double sh[32];
+  if (scal[S_DONE] != 0.0) return;
+  const int normtype = (int)scal[S_NORMT];
+  const double alpha = scal[S_ALPHA];
+  double rho = 0.0, rn = 0.0;
+  GRID_STRIDE(c, nL) {
+    x[c] = x[c] + alpha * w[c];
+    const double rc = r[c] + (-alpha) * q[c];
+    r[c] = rc;
+    rho += rc * rc;
+    const float bc = (float)rc;
+    b32[c] = bc;
+    x32[c] = c0 * (dinv32[c] * bc);
+    const double t = norm_term_L(normtype, rc, wt, c);
+    rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
+  }
+  update_finish(rho, rn, normtype, hist, nullptr, 0, scal, partials, counter, sh);
 }
 
 // 4. w = beta w + Dinv r
@@ -996,94 +1034,107 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
   }
 }
 
-// Chebyshev smoothing of A x = b from x = 0 (the recurrence of k_cheb_*):
-// res = b, d = c0 Dinv res, x = d.  With r64 the level's b is first taken
-// from the FP64 outer residual.
+// Chebyshev smoothing of A x = b from x = 0 (the recurrence of k_cheb_*),
+// first term: x = c0 Dinv b.  With r64 the level's b is first taken from
+// the FP64 outer residual.
 __global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, float *__restrict__ b,
-                           const float *__restrict__ dinv, float c0, float *__restrict__ res,
-                           float *__restrict__ d, float *__restrict__ x, const double *stop) {
+                           const float *__restrict__ dinv, float c0, float *__restrict__ x,
+                           const double *stop) {
   if (stop && *stop != 0.0) return;
   GRID_STRIDE(c, nL) {
     const float bc = r64 ? (float)r64[c] : b[c];
     if (r64) b[c] = bc;
-    res[c] = bc;
-    const float dc = c0 * (dinv[c] * bc);
-    d[c] = dc;
-    x[c] = dc;
+    x[c] = c0 * (dinv[c] * bc);
   }
 }
 
-// Passes that fold the element-local qE into the lattice (s = mask * sum
-// of copies) and update the smoother state:
-//   MG_STEP     qE = A d:  res -= s; d = c1 d + c2 Dinv res; x += d
-//   MG_RESID    qE = A d:  res -= s                (res = b - A x after a smoothing)
-//   MG_RESTART  qE = A x:  res = b - s; d = c1 Dinv res; x += d
-//                          (smoothing of the residual equation from an existing x)
+// Passes that fold the element-local qE = A x into the lattice (s = mask *
+// sum of copies) and advance the smoother state:
+//   MG_STEP   r = b - s; d = a1 dprev + a2 Dinv r; x += d, with dprev
+//             DP_NONE  (none: smoothing of the residual equation from an
+//                       existing x, the first post-smoothing term),
+//             DP_X     (x: the step after a start from zero, where d = x),
+//             DP_D     (the stored d);
+//             d is stored only when a later step reads it (wd)
+//   MG_RESID  res = b - s                  (the residual to restrict)
+//   MG_START  qE = a coarse E-vector (the element restriction's output):
+//             b = s; x = a1 Dinv b         (smoothing from zero)
+//   MG_FOLDB  b = s only (a dense coarsest level)
 // DOTS (last pass of the finest level): <b, x> (b = the FP32 copy of the
 // outer residual) for the CG step, finished by fcg_finish_fr.
-//   MG_START    qE = a coarse E-vector (the element restriction's output):
-//               b = s; res = b; d = c1 Dinv b; x = d  (smoothing from zero)
-//   MG_FOLDB    b = s only (a dense coarsest level)
-enum { MG_STEP = 0, MG_RESID = 1, MG_RESTART = 2, MG_START = 3, MG_FOLDB = 4 };
+// Applying x rather than the step direction keeps the running residual out
+// of the smoother state: a step reads b, dinv, x (and d) and writes x (and
+// d); mathematically the same Chebyshev polynomial.
+enum { MG_STEP = 0, MG_RESID = 1, MG_START = 3, MG_FOLDB = 4 };
+enum { DP_NONE = 0, DP_X = 1, DP_D = 2 };
 
-// The passes run on the box lattice, one thread per lattice point in
-// lattice order: the state vectors stream fully coalesced (a warp reads 128
-// contiguous bytes of each), and a point's element copies are gathered
-// from qE, where the copies of one element row are one aligned 32-byte
-// sector shared by the warp's neighbouring points.  Copies are added in
-// ascending element id.  Lattice and element-local sizes are below 2^31
-// (checked when the problem is created).
+// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, sec. 4):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// q = (mulhi(m, n) + n) >> l  (the add cannot overflow for n < 2^31).
+struct FastDiv {
+  uint32_t m;
+  int l;
+  static FastDiv make(int d) {
+    FastDiv f;
+    f.l = 0;
+    while ((int64_t(1) << f.l) < d) f.l++;
+    f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.l) - (uint64_t)d)) / (uint64_t)d + 1);
+    return f;
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi((uint32_t)n, m) + (uint32_t)n) >> l);
+  }
+};
+
+// The element copies of lattice coordinate g along one direction, as
+// offsets into the E-vector (es = the element stride, ls = the local
+// index stride), in ascending element coordinate; returns their count.
 template <int P>
-__device__ __forceinline__ int lattice_cands(int g, int ne, int per, int (&ec)[2], int (&l)[2]) {
+__device__ __forceinline__ int lattice_offsets(int g, int ne, int per, int es, int ls, int &o0,
+                                               int &o1) {
   const int q = g / P, r = g - q * P;
   if (r != 0) {
-    ec[0] = q;
-    l[0] = r;
+    o0 = o1 = q * es + r * ls;
     return 1;
   }
   if (per) {  // (q-1, P) and (q, 0), wrapping; one element twice when ne == 1
     if (q == 0) {
-      ec[0] = 0;
-      l[0] = 0;
-      ec[1] = ne - 1;
-      l[1] = P;
+      o0 = 0;
+      o1 = (ne - 1) * es + P * ls;
     } else {
-      ec[0] = q - 1;
-      l[0] = P;
-      ec[1] = q;
-      l[1] = 0;
+      o0 = (q - 1) * es + P * ls;
+      o1 = q * es;
     }
     return 2;
   }
-  int k = 0;
-  if (q >= 1) {
-    ec[k] = q - 1;
-    l[k++] = P;
+  if (q == 0) {
+    o0 = o1 = 0;
+    return 1;
   }
-  if (q < ne) {
-    ec[k] = q;
-    l[k++] = 0;
-  }
-  return k;
+  o0 = (q - 1) * es + P * ls;
+  o1 = q == ne ? o0 : q * es;
+  return q == ne ? 1 : 2;
 }
 
-// One thread per lattice point in lattice order.  A 256-thread block walks
-// lattice rows (fixed y, z), 2^LB threads per row (2^LB >= M0, or segments
-// of 256 for longer rows), so a thread's row and x position come from
-// shifts and masks, the y/z element copies are fixed for the row, and only
-// the x copies vary by thread; consecutive threads take consecutive points
-// (coalesced state vectors, a warp's copies of one element row in one
-// sector).  Copies are added in ascending element id.  Lattice and
-// element-local sizes are below 2^31 (checked when the problem is created).
-// (Measured on B200 against this form: element-ordered walks, several
-// points per thread, z-column walks and a lattice-row layout of qE were all
-// slower.)
+// One thread per lattice point, in lattice order (grid-stride over the
+// flat index): the state vectors stream fully coalesced, and a warp's
+// copies of one element row are one 32-byte sector of qE.  The point's
+// coordinates come from two multiply-shift divisions, its copies from
+// scalar offsets (no local arrays), its state loads are issued before the
+// gather (one memory round trip per point), and the copies are added in
+// ascending element id.  Lattice and element-local sizes are below 2^31
+// (checked when the problem is created).
+// (Measured on B200 against this form: element-ordered walks, lattice rows
+// mapped to power-of-two thread groups, several points per thread, z-column
+// walks and a lattice-row layout of qE were all slower.)
 template <int N, int MODE, bool DOTS>
 __global__ void __launch_bounds__(RED_THREADS)
-    k_mg_pass_lat(MapBox<N> map, Weights wt, const float *__restrict__ qE,
-                  float *__restrict__ b, const float *__restrict__ dinv, float c1, float c2,
-                  float *__restrict__ res, float *__restrict__ d, float *__restrict__ x, int LB,
-                  double *scal, double *partials, unsigned int *counter) {
+    k_mg_pass_lat(MapBox<N> map, FastDiv fd0, FastDiv fd1, Weights wt,
+                  const float *__restrict__ qE, float *__restrict__ b,
+                  const float *__restrict__ dinv, float c1, float c2, float *__restrict__ res,
+                  float *__restrict__ d, float *__restrict__ x, int dsrc, int wd, double *scal,
+                  double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
   constexpr int P = N - 1, NN = N * N;
@@ -1091,63 +1142,60 @@ __global__ void __launch_bounds__(RED_THREADS)
   const bool d3 = map.dim > 2;
   const int nn = d3 ? NN * N : NN;
   const int ne0 = map.ne[0], ne1 = map.ne[1];
-  const int M0 = (int)map.M[0], M1 = (int)map.M[1];
-  const int nrows = M1 * (d3 ? (int)map.M[2] : 1);
-  const int W = 1 << LB, nseg = (M0 + W - 1) / W;
-  const int upb = RED_THREADS >> LB;  // row segments per block trip
-  const int tx = threadIdx.x & (W - 1), ty = threadIdx.x >> LB;
-  int ex[2], lx[2], nx = 0;
-  if (nseg == 1 && tx < M0) nx = lattice_cands<P>(tx, ne0, map.per[0], ex, lx);
-  for (int unit = blockIdx.x * upb + ty; unit < nrows * nseg; unit += gridDim.x * upb) {
-    int row = unit, g0 = tx;
-    if (nseg > 1) {
-      row = unit / nseg;
-      g0 = (unit - row * nseg) * W + tx;
-      if (g0 < M0) nx = lattice_cands<P>(g0, ne0, map.per[0], ex, lx);
+  const int M0 = map.M[0], M1 = map.M[1];
+  const int nL = M0 * M1 * (d3 ? map.M[2] : 1);
+  const int sy = ne0 * nn, sz = ne0 * ne1 * nn;
+  const int stride = gridDim.x * blockDim.x;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nL;
+       c = (c < nL - stride) ? c + stride : nL) {
+    const bool keep = !wt.maskL || wt.maskL[c];
+    float bc = 0.0f, xo = 0.0f, dv = 0.0f, dpv = 0.0f;
+    if (MODE == MG_STEP || MODE == MG_RESID) bc = b[c];
+    if (MODE == MG_STEP || MODE == MG_START) dv = dinv[c];
+    if (MODE == MG_STEP) {
+      xo = x[c];
+      if (dsrc == DP_D) dpv = d[c];
     }
-    if (g0 >= M0) continue;
-    const int g1 = row % M1, g2 = row / M1;
-    int ey[2], ly[2], ez[2] = {0, 0}, lz[2] = {0, 0};
-    const int ny = lattice_cands<P>(g1, ne1, map.per[1], ey, ly);
-    const int nz = d3 ? lattice_cands<P>(g2, map.ne[2], map.per[2], ez, lz) : 1;
+    const int row = fd0.div(c), g0 = c - row * M0;
+    const int g2 = fd1.div(row), g1 = row - g2 * M1;
+    int ox0, ox1, oy0, oy1, oz0 = 0, oz1 = 0;
+    const int nx = lattice_offsets<P>(g0, ne0, map.per[0], nn, 1, ox0, ox1);
+    const int ny = lattice_offsets<P>(g1, ne1, map.per[1], sy, N, oy0, oy1);
+    const int nz = d3 ? lattice_offsets<P>(g2, map.ne[2], map.per[2], sz, NN, oz0, oz1) : 1;
     float s = 0.0f;
-    for (int az = 0; az < nz; az++)
-      for (int ay = 0; ay < ny; ay++) {
-        const int base = ne0 * (ey[ay] + ne1 * ez[az]) * nn + N * ly[ay] + NN * lz[az];
-        s = __fadd_rn(s, qE[base + ex[0] * nn + lx[0]]);
-        if (nx > 1) s = __fadd_rn(s, qE[base + ex[1] * nn + lx[1]]);
+#pragma unroll
+    for (int az = 0; az < 2; az++) {
+      if (az >= nz) break;
+      const int oz = az ? oz1 : oz0;
+#pragma unroll
+      for (int ay = 0; ay < 2; ay++) {
+        if (ay >= ny) break;
+        const int o = oz + (ay ? oy1 : oy0);
+        s = __fadd_rn(s, qE[o + ox0]);
+        if (nx > 1) s = __fadd_rn(s, qE[o + ox1]);
       }
-    const int c = g0 + M0 * row;
-    if (wt.maskL && !wt.maskL[c]) s = 0.0f;
-    if (MODE == MG_RESID) {
-      res[c] = res[c] - s;
-      continue;
     }
+    if (!keep) s = 0.0f;
     if (MODE == MG_FOLDB) {
       b[c] = s;
       continue;
     }
     if (MODE == MG_START) {
-      const float dc0 = c1 * (dinv[c] * s);
       b[c] = s;
-      res[c] = s;
-      d[c] = dc0;
-      x[c] = dc0;
+      x[c] = c1 * (dv * s);
       continue;
     }
-    float rc, dc;
-    if (MODE == MG_STEP) {
-      rc = res[c] - s;
-      dc = c1 * d[c] + c2 * (dinv[c] * rc);
-    } else {
-      rc = b[c] - s;
-      dc = c1 * (dinv[c] * rc);
+    const float rc = bc - s;
+    if (MODE == MG_RESID) {
+      res[c] = rc;
+      continue;
     }
-    const float xc = x[c] + dc;
+    const float dp = dsrc == DP_X ? xo : dpv;
+    const float dc = c1 * dp + c2 * (dv * rc);
+    const float xc = xo + dc;
     x[c] = xc;
-    res[c] = rc;
-    d[c] = dc;
-    if (DOTS) rz += (double)b[c] * (double)xc;
+    if (wd) d[c] = dc;
+    if (DOTS) rz += (double)bc * (double)xc;
   }
   if (!DOTS) return;
   rz = block_reduce<false>(rz, sh);
@@ -1707,8 +1755,8 @@ struct MGLevelBase {
   }
   virtual int apply(const float *in, double p, double q, int use_mass, const double *stop,
                     cudaStream_t st) = 0;
-  virtual void pass(int mode, bool dots, float a1, float a2, gf_problem *outer,
-                    cudaStream_t st) = 0;
+  virtual void pass(int mode, bool dots, float a1, float a2, int dsrc, int wd,
+                    gf_problem *outer, cudaStream_t st) = 0;
   virtual int jacobi(double p, double q, int use_mass) = 0;
   virtual int estimate(double p, double q, int use_mass, int64_t nfree) = 0;
   // element-wise transfers to the next coarser level when it has the same
@@ -1729,32 +1777,29 @@ struct MGLevel : MGLevelBase {
     nE = lp->nlocal;
     for (int k = 0; k < 3; k++) M[k] = (int)lp->box.M[k];
     maskL = S.wt.maskL;
-    // lattice row width of the smoother passes: 2^LB >= M0 threads (a
-    // block, 2^8, at most; longer rows in segments)
-    LB = 5;
-    while ((1 << LB) < M[0] && LB < 8) LB++;
+    fd0 = FastDiv::make(M[0]);
+    fd1 = FastDiv::make(M[1]);
   }
-  int LB = 8;
+  FastDiv fd0, fd1;  // divisions by the lattice widths (smoother passes)
   int apply(const float *in, double p, double q, int use_mass, const double *stop,
             cudaStream_t st) override {
     return launch_helm_L<float>(prob, (float)p, (float)q, use_mass, in, qE, st, stop);
   }
   template <int MODE, bool DOTS>
-  void run_pass(float a1, float a2, gf_problem *outer, cudaStream_t st) {
+  void run_pass(float a1, float a2, int dsrc, int wd, gf_problem *outer, cudaStream_t st) {
     auto kern = k_mg_pass_lat<N, MODE, DOTS>;
-    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, S.wt, qE, b, dinv, a1, a2, res, d, x, LB,
-                                                 outer->scal_d, outer->partials, outer->counter);
+    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, fd0, fd1, S.wt, qE, b, dinv, a1, a2, res,
+                                                 d, x, dsrc, wd, outer->scal_d, outer->partials,
+                                                 outer->counter);
   }
-  void pass(int mode, bool dots, float a1, float a2, gf_problem *outer,
+  void pass(int mode, bool dots, float a1, float a2, int dsrc, int wd, gf_problem *outer,
             cudaStream_t st) override {
     outer->launches++;
-    if (mode == MG_RESID) run_pass<MG_RESID, false>(a1, a2, outer, st);
-    else if (mode == MG_START) run_pass<MG_START, false>(a1, a2, outer, st);
-    else if (mode == MG_FOLDB) run_pass<MG_FOLDB, false>(a1, a2, outer, st);
-    else if (mode == MG_STEP && dots) run_pass<MG_STEP, true>(a1, a2, outer, st);
-    else if (mode == MG_STEP) run_pass<MG_STEP, false>(a1, a2, outer, st);
-    else if (dots) run_pass<MG_RESTART, true>(a1, a2, outer, st);
-    else run_pass<MG_RESTART, false>(a1, a2, outer, st);
+    if (mode == MG_RESID) run_pass<MG_RESID, false>(a1, a2, dsrc, wd, outer, st);
+    else if (mode == MG_START) run_pass<MG_START, false>(a1, a2, dsrc, wd, outer, st);
+    else if (mode == MG_FOLDB) run_pass<MG_FOLDB, false>(a1, a2, dsrc, wd, outer, st);
+    else if (dots) run_pass<MG_STEP, true>(a1, a2, dsrc, wd, outer, st);
+    else run_pass<MG_STEP, false>(a1, a2, dsrc, wd, outer, st);
   }
   void restrict_elem(MGLevelBase &C, gf_problem *outer, cudaStream_t st) override {
     constexpr int NT = N * N, EPB = (256 / NT) < 1 ? 1 : 256 / NT;
@@ -2316,49 +2361,47 @@ void mg_prolong(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t 
 // is the FP64 outer residual r64 and the last pass reduces <r, z> for the
 // CG step.
 void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem *outer,
-               const double *r64, cudaStream_t st) {
+               const double *r64, bool started, cudaStream_t st) {
   MGLevelBase &L = *H.lv[l];
   const double *stop = outer->scal_d + S_DONE;
   const bool top = l == 0, last = l + 1 == H.lv.size();
   // b arrives as the element restriction's coarse E-vector in L.qE
   const bool folded = l > 0 && H.lv[l - 1]->ptransfer;
   if (last && L.ainv) {  // coarsest: dense solve (never the finest level)
-    if (folded) L.pass(MG_FOLDB, false, 0.0f, 0.0f, outer, st);
+    if (folded) L.pass(MG_FOLDB, false, 0.0f, 0.0f, DP_NONE, 0, outer, st);
     k_dense_solve<<<(unsigned)std::min<int64_t>(L.nfree, 148 * 8), 128, 0, st>>>(
         L.nfree, L.ainv, L.free_idx, L.b, L.x, stop);
     outer->launches++;
     return;
   }
+  // x = c0 Dinv b (the top level's b and x may come from the outer update)
   if (folded) {
-    L.pass(MG_START, false, L.c0, 0.0f, outer, st);
-  } else {
-    k_mg_start<<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(
-        L.nL, top ? r64 : nullptr, L.b, L.dinv, L.c0, L.res, L.d, L.x, stop);
+    L.pass(MG_START, false, L.c0, 0.0f, DP_NONE, 0, outer, st);
+  } else if (!(top && started)) {
+    k_mg_start<<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(L.nL, top ? r64 : nullptr, L.b,
+                                                               L.dinv, L.c0, L.x, stop);
     outer->launches++;
   }
-  if (last) {  // coarsest: Chebyshev solve from zero
-    for (int j = 1; j <= L.m; j++) {
-      L.apply(L.d, p, q, use_mass, stop, st);
-      L.pass(MG_STEP, top && j == L.m, L.c1[j], L.c2[j], outer, st);
-    }
-    return;
+  // pre-smoothing x = S b (on the coarsest level: the whole Chebyshev solve)
+  for (int j = 1; j <= L.m; j++) {
+    L.apply(L.x, p, q, use_mass, stop, st);
+    L.pass(MG_STEP, last && top && j == L.m, L.c1[j], L.c2[j], j == 1 ? DP_X : DP_D, j < L.m,
+           outer, st);
   }
-  for (int j = 1; j <= L.m; j++) {  // pre-smoothing x = S b
-    L.apply(L.d, p, q, use_mass, stop, st);
-    L.pass(MG_STEP, false, L.c1[j], L.c2[j], outer, st);
-  }
-  L.apply(L.d, p, q, use_mass, stop, st);  // res = b - A x
-  L.pass(MG_RESID, false, 0.0f, 0.0f, outer, st);
+  if (last) return;
+  L.apply(L.x, p, q, use_mass, stop, st);  // res = b - A x
+  L.pass(MG_RESID, false, 0.0f, 0.0f, DP_NONE, 0, outer, st);
   if (L.ptransfer) L.restrict_elem(*H.lv[l + 1], outer, st);
   else mg_restrict(L, *H.lv[l + 1], outer, st);
-  mg_vcycle(H, l + 1, p, q, use_mass, outer, r64, st);
+  mg_vcycle(H, l + 1, p, q, use_mass, outer, r64, false, st);
   if (L.ptransfer) L.prolong_elem(*H.lv[l + 1], outer, st);
   else mg_prolong(L, *H.lv[l + 1], outer, st);
-  L.apply(L.x, p, q, use_mass, stop, st);  // post-smoothing x += S (b - A x)
-  L.pass(MG_RESTART, top && L.m == 0, L.c0, 0.0f, outer, st);
+  // post-smoothing x += S (b - A x): the first term from the residual
+  L.apply(L.x, p, q, use_mass, stop, st);
+  L.pass(MG_STEP, top && L.m == 0, 0.0f, L.c0, DP_NONE, L.m > 0, outer, st);
   for (int j = 1; j <= L.m; j++) {
-    L.apply(L.d, p, q, use_mass, stop, st);
-    L.pass(MG_STEP, top && j == L.m, L.c1[j], L.c2[j], outer, st);
+    L.apply(L.x, p, q, use_mass, stop, st);
+    L.pass(MG_STEP, top && j == L.m, L.c1[j], L.c2[j], DP_D, j < L.m, outer, st);
   }
 }
 
@@ -2383,8 +2426,9 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
   if (rc) return gf_fail(ctx, rc, "residual failed");
   const float *z = H->lv[0]->x;
   double *scal = prob->scal_d;
-  auto precondition = [&](cudaStream_t ls) {
-    mg_vcycle(*H, 0, p, q, use_mass, prob, rL, ls);
+  MGLevelBase &L0 = *H->lv[0];
+  auto precondition = [&](cudaStream_t ls, bool started) {
+    mg_vcycle(*H, 0, p, q, use_mass, prob, rL, started, ls);
     prob->launches++;
     k_fcg_w<<<S.gL, 256, 0, ls>>>(nL, w, z, scal);
   };
@@ -2393,11 +2437,11 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
       launch_helm_L<double>(prob, p, q, use_mass, w, qE, ls, scal + S_DONE);
       k_asm_dot<double, MAP><<<S.rgrid(k_asm_dot<double, MAP>), RED_THREADS, 0, ls>>>(
           nL, S.map, S.wt, qE, w, qL, scal, prob->partials, prob->counter);
-      k_update<double, MAP><<<S.rgrid(k_update<double, MAP>), RED_THREADS, 0, ls>>>(
-          nL, S.map, S.wt, xL, w, rL, qL, nullptr, hist, nullptr, 0, scal, prob->partials,
+      k_update_mg<<<S.rgrid(k_update_mg), RED_THREADS, 0, ls>>>(
+          nL, S.wt, xL, w, rL, qL, L0.dinv, L0.c0, L0.b, L0.x, hist, scal, prob->partials,
           prob->counter);
       prob->launches += 2;
-      precondition(ls);
+      precondition(ls, true);
     }
   };
   auto level_launches = [&]() {
@@ -2408,7 +2452,7 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
   prob->scal_h[S_FIRST] = 1.0;
   GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_d + S_FIRST, prob->scal_h + S_FIRST, sizeof(double),
                                cudaMemcpyHostToDevice, st));
-  precondition(st);
+  precondition(st, false);
   // The iteration loop runs on the device: a graph holding one WHILE node
   // whose body is one iteration (some 95 launches, most of them small
   // coarse-level kernels, all reading their scalars from the device) and
