@@ -69,6 +69,45 @@ enum {
 // and (box only) lattice coordinates g; each(c, g, f) calls f(m) for the
 // members m of the node in ascending local id; mult(c, g) is the count.
 
+// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, sec. 4):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// q = (mulhi(m, n) + n) >> l  (the add cannot overflow for n < 2^31).
+struct FastDiv {
+  uint32_t m;
+  int l;
+  static FastDiv make(int d) {
+    FastDiv f;
+    f.l = 0;
+    while ((int64_t(1) << f.l) < d) f.l++;
+    f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.l) - (uint64_t)d)) / (uint64_t)d + 1);
+    return f;
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi((uint32_t)n, m) + (uint32_t)n) >> l);
+  }
+};
+
+// The element copies of lattice coordinate g along one direction, as
+// offsets into the E-vector (es = the element stride, ls = the local
+// index stride), in ascending element coordinate; returns their count.
+// Off an element face the one copy is (q, r); on a face (r = 0) the copies
+// are (q - 1, P) and (q, 0), the first wrapping to (ne - 1, P) and coming
+// second when periodic and q = 0, and only one of them on a non-periodic
+// boundary.  Branch-free: neighbouring threads of a warp take different
+// cases.
+template <int P>
+__device__ __forceinline__ int lattice_offsets(int g, int ne, int per, int es, int ls, int &o0,
+                                               int &o1) {
+  const int q = g / P, r = g - q * P;
+  const int hi = q * es + r * ls;
+  const int lo = ((q == 0 ? ne : q) - 1) * es + P * ls;
+  const bool face = r == 0;
+  o0 = (face && q != 0) ? lo : hi;
+  o1 = q == 0 ? lo : hi;
+  return !face ? 1 : ((per || (q != 0 && q != ne)) ? 2 : 1);
+}
+
 // Box lattice of order N-1.  Blocks walk lattice rows (fixed gy, gz), so a
 // node's coordinates come from the launch shape, and the order being a
 // compile-time constant turns every % and / by p into a multiply-shift.
@@ -76,6 +115,7 @@ template <int N>
 struct MapBox {
   static constexpr int P = N - 1;
   int dim, ne[3], per[3], M[3];
+  FastDiv fd0, fd1;  // divisions by M[0], M[1]
   static MapBox make(const BoxLattice &L) {
     MapBox m;
     m.dim = L.dim;
@@ -86,6 +126,8 @@ struct MapBox {
       m.M[d] = (int)L.M[d];
       if (d < L.dim && L.per[d] && L.ne[d] == 1) m.sorted = 0;
     }
+    m.fd0 = FastDiv::make(m.M[0]);
+    m.fd1 = FastDiv::make(m.M[1]);
     return m;
   }
   template <class F>
@@ -183,14 +225,13 @@ struct MapBox {
     for (int i = 0; i < k; i++) f((int64_t)m[i]);
   }
   // f(c, s) for every lattice point c, s = sum of its element copies in
-  // ascending local id (added in TS).  Walked by element: every lattice
-  // point is owned by one element, the one holding it at local index < P in
-  // every direction (or P on a non-periodic upper boundary), and the
-  // element's N^2 threads each take one (l0, l1) column of its owned
-  // points.  The other members sit at index P of the lower neighbours, so
-  // each element-local value is read exactly once, by whole element
-  // planes, with all index arithmetic fixed per thread.  Needs blockDim.x
-  // = RED_THREADS.
+  // ascending local id (added in TS).  One thread per lattice point in
+  // lattice order (grid-stride over the flat index): the point's
+  // coordinates from two multiply-shift divisions, its copies from scalar
+  // offsets (lattice_offsets), added in the (z, y, x) nesting, which is
+  // ascending element id when no periodic direction has a single element
+  // (otherwise the explicit sort of each()).  Lattice and element-local
+  // sizes are below 2^31 (checked when the problem is created).
   template <typename TS, typename TV, class F>
   __device__ __forceinline__ void rows_sum(const TV *__restrict__ inE, F f) const {
     if (!sorted) {
@@ -201,64 +242,34 @@ struct MapBox {
       });
       return;
     }
-    constexpr int NN = N * N, EPB = (RED_THREADS / NN) < 1 ? 1 : RED_THREADS / NN;
-    const int slot = threadIdx.x / NN, t = threadIdx.x % NN;
-    if (slot >= EPB) return;
-    const int l0 = t % N, l1 = t / N;
+    constexpr int NN = N * N;
     const bool d3 = dim > 2;
-    const int64_t nn = d3 ? (int64_t)NN * N : NN;
-    const int64_t nel = (int64_t)ne[0] * ne[1] * (d3 ? ne[2] : 1);
-    const int64_t sy = ne[0], sz = (int64_t)ne[0] * ne[1];
-    for (int64_t e = (int64_t)blockIdx.x * EPB + slot; e < nel; e += (int64_t)gridDim.x * EPB) {
-      const int ec0 = (int)(e % ne[0]);
-      const int64_t rr = e / ne[0];
-      const int ec1 = (int)(rr % ne[1]), ec2 = d3 ? (int)(rr / ne[1]) : 0;
-      if (l0 == P && (per[0] || ec0 != ne[0] - 1)) continue;  // owned by the x-neighbour
-      if (l1 == P && (per[1] || ec1 != ne[1] - 1)) continue;
-      // members per direction as (element offset, local index), ascending
-      int64_t dx[2] = {0, 0}, dy[2] = {0, 0};
-      int lx[2] = {l0, l0}, ly[2] = {l1, l1};
-      int nx = 1, ny = 1;
-      if (l0 == 0 && (per[0] || ec0 > 0)) {
-        nx = 2;
-        if (ec0 > 0) { dx[0] = -1; lx[0] = P; }
-        else { dx[1] = ne[0] - 1; lx[1] = P; }
-      }
-      if (l1 == 0 && (per[1] || ec1 > 0)) {
-        ny = 2;
-        if (ec1 > 0) { dy[0] = -sy; ly[0] = P; }
-        else { dy[1] = (ne[1] - 1) * sy; ly[1] = P; }
-      }
-      const int64_t cxy = (int64_t)ec0 * P + l0 + (int64_t)M[0] * ((int64_t)ec1 * P + l1);
-      const int64_t plane = (int64_t)M[0] * M[1];
+    const int nn = d3 ? NN * N : NN;
+    const int sy = ne[0] * nn, sz = ne[0] * ne[1] * nn;
+    const int nL = M[0] * M[1] * (d3 ? M[2] : 1);
+    const int stride = gridDim.x * blockDim.x;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nL;
+         c = (c < nL - stride) ? c + stride : nL) {
+      const int row = fd0.div(c), g0 = c - row * M[0];
+      const int g2 = fd1.div(row), g1 = row - g2 * M[1];
+      int ox0, ox1, oy0, oy1, oz0 = 0, oz1 = 0;
+      const int nx = lattice_offsets<P>(g0, ne[0], per[0], nn, 1, ox0, ox1);
+      const int ny = lattice_offsets<P>(g1, ne[1], per[1], sy, N, oy0, oy1);
+      const int nz = d3 ? lattice_offsets<P>(g2, ne[2], per[2], sz, NN, oz0, oz1) : 1;
+      TS s = TS(0);
 #pragma unroll
-      for (int l2 = 0; l2 < (d3 ? N : 1); l2++) {
-        if (d3 && l2 == P && (per[2] || ec2 != ne[2] - 1)) continue;
-        int64_t dz[2] = {0, 0};
-        int lz[2] = {l2, l2}, nz = 1;
-        if (d3 && l2 == 0 && (per[2] || ec2 > 0)) {
-          nz = 2;
-          if (ec2 > 0) { dz[0] = -sz; lz[0] = P; }
-          else { dz[1] = (ne[2] - 1) * sz; lz[1] = P; }
+      for (int az = 0; az < 2; az++) {
+        if (az >= nz) break;
+        const int oz = az ? oz1 : oz0;
+#pragma unroll
+        for (int ay = 0; ay < 2; ay++) {
+          if (ay >= ny) break;
+          const int o = oz + (ay ? oy1 : oy0);
+          s = __fadd_rn_t(s, (TS)inE[o + ox0]);
+          if (nx > 1) s = __fadd_rn_t(s, (TS)inE[o + ox1]);
         }
-        TS s = TS(0);
-#pragma unroll
-        for (int a = 0; a < 2; a++) {
-          if (a >= nz) break;
-#pragma unroll
-          for (int b = 0; b < 2; b++) {
-            if (b >= ny) break;
-            const int64_t eb = e + dz[a] + dy[b];
-            const int off = NN * lz[a] + N * ly[b];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-              if (i >= nx) break;
-              s = __fadd_rn_t(s, (TS)inE[(eb + dx[i]) * nn + off + lx[i]]);
-            }
-          }
-        }
-        f(cxy + (d3 ? plane * ((int64_t)ec2 * P + l2) : 0), s);
       }
+      f((int64_t)c, s);
     }
   }
   __device__ __forceinline__ double mult(int64_t, const int (&g)[3]) const {
@@ -1068,69 +1079,21 @@ __global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, float *__
 enum { MG_STEP = 0, MG_RESID = 1, MG_START = 3, MG_FOLDB = 4 };
 enum { DP_NONE = 0, DP_X = 1, DP_D = 2 };
 
-// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund & Montgomery,
-// "Division by invariant integers using multiplication", PLDI 1994, sec. 4):
-// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
-// q = (mulhi(m, n) + n) >> l  (the add cannot overflow for n < 2^31).
-struct FastDiv {
-  uint32_t m;
-  int l;
-  static FastDiv make(int d) {
-    FastDiv f;
-    f.l = 0;
-    while ((int64_t(1) << f.l) < d) f.l++;
-    f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.l) - (uint64_t)d)) / (uint64_t)d + 1);
-    return f;
-  }
-  __device__ __forceinline__ int div(int n) const {
-    return (int)((__umulhi((uint32_t)n, m) + (uint32_t)n) >> l);
-  }
-};
-
-// The element copies of lattice coordinate g along one direction, as
-// offsets into the E-vector (es = the element stride, ls = the local
-// index stride), in ascending element coordinate; returns their count.
-template <int P>
-__device__ __forceinline__ int lattice_offsets(int g, int ne, int per, int es, int ls, int &o0,
-                                               int &o1) {
-  const int q = g / P, r = g - q * P;
-  if (r != 0) {
-    o0 = o1 = q * es + r * ls;
-    return 1;
-  }
-  if (per) {  // (q-1, P) and (q, 0), wrapping; one element twice when ne == 1
-    if (q == 0) {
-      o0 = 0;
-      o1 = (ne - 1) * es + P * ls;
-    } else {
-      o0 = (q - 1) * es + P * ls;
-      o1 = q * es;
-    }
-    return 2;
-  }
-  if (q == 0) {
-    o0 = o1 = 0;
-    return 1;
-  }
-  o0 = (q - 1) * es + P * ls;
-  o1 = q == ne ? o0 : q * es;
-  return q == ne ? 1 : 2;
-}
-
 // One thread per lattice point, in lattice order (grid-stride over the
 // flat index): the state vectors stream fully coalesced, and a warp's
 // copies of one element row are one 32-byte sector of qE.  The point's
 // coordinates come from two multiply-shift divisions, its copies from
 // scalar offsets (no local arrays), its state loads are issued before the
-// gather (one memory round trip per point), and the copies are added in
-// ascending element id.  Lattice and element-local sizes are below 2^31
-// (checked when the problem is created).
+// gather (one memory round trip per point), and the copies are added in the
+// (z, y, x) nesting of MapBox::rows_sum (ascending element id unless a
+// periodic direction has a single element).  Lattice and element-local
+// sizes are below 2^31 (checked when the problem is created).
 // (Measured on B200 against this form: element-ordered walks, lattice rows
 // mapped to power-of-two thread groups, several points per thread, z-column
 // walks and a lattice-row layout of qE were all slower.)
 template <int N, int MODE, bool DOTS>
 __global__ void __launch_bounds__(RED_THREADS)
-    k_mg_pass_lat(MapBox<N> map, FastDiv fd0, FastDiv fd1, Weights wt,
+    k_mg_pass_lat(MapBox<N> map, Weights wt,
                   const float *__restrict__ qE, float *__restrict__ b,
                   const float *__restrict__ dinv, float c1, float c2, float *__restrict__ res,
                   float *__restrict__ d, float *__restrict__ x, int dsrc, int wd, double *scal,
@@ -1156,8 +1119,8 @@ __global__ void __launch_bounds__(RED_THREADS)
       xo = x[c];
       if (dsrc == DP_D) dpv = d[c];
     }
-    const int row = fd0.div(c), g0 = c - row * M0;
-    const int g2 = fd1.div(row), g1 = row - g2 * M1;
+    const int row = map.fd0.div(c), g0 = c - row * M0;
+    const int g2 = map.fd1.div(row), g1 = row - g2 * M1;
     int ox0, ox1, oy0, oy1, oz0 = 0, oz1 = 0;
     const int nx = lattice_offsets<P>(g0, ne0, map.per[0], nn, 1, ox0, ox1);
     const int ny = lattice_offsets<P>(g1, ne1, map.per[1], sy, N, oy0, oy1);
@@ -1777,10 +1740,7 @@ struct MGLevel : MGLevelBase {
     nE = lp->nlocal;
     for (int k = 0; k < 3; k++) M[k] = (int)lp->box.M[k];
     maskL = S.wt.maskL;
-    fd0 = FastDiv::make(M[0]);
-    fd1 = FastDiv::make(M[1]);
   }
-  FastDiv fd0, fd1;  // divisions by the lattice widths (smoother passes)
   int apply(const float *in, double p, double q, int use_mass, const double *stop,
             cudaStream_t st) override {
     return launch_helm_L<float>(prob, (float)p, (float)q, use_mass, in, qE, st, stop);
@@ -1788,8 +1748,8 @@ struct MGLevel : MGLevelBase {
   template <int MODE, bool DOTS>
   void run_pass(float a1, float a2, int dsrc, int wd, gf_problem *outer, cudaStream_t st) {
     auto kern = k_mg_pass_lat<N, MODE, DOTS>;
-    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, fd0, fd1, S.wt, qE, b, dinv, a1, a2, res,
-                                                 d, x, dsrc, wd, outer->scal_d, outer->partials,
+    kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, S.wt, qE, b, dinv, a1, a2, res, d, x, dsrc,
+                                                 wd, outer->scal_d, outer->partials,
                                                  outer->counter);
   }
   void pass(int mode, bool dots, float a1, float a2, int dsrc, int wd, gf_problem *outer,
