@@ -259,8 +259,12 @@ def dss_timing(ctx, prob, reps=10):
         torch.cuda.synchronize()
         t = s.elapsed_time(e) / 1e3 / reps
         s_ = 4 if dt == torch.float32 else 8
-        alg = prob.nlocal * (2 * s_ + 4) + prob.grid.nclass * 4
-        out[name] = {"ms": t * 1e3, "gbs": alg / t / 1e9}
+        # box lattice (k_dss_box): every E-node read and written once, no
+        # index arrays; CSR (k_dss_csr): plus members and class_ptr
+        box = getattr(prob, "structured", True)
+        alg = prob.nlocal * 2 * s_ + (0 if box else prob.nlocal * 4 + prob.grid.nclass * 4)
+        out[name] = {"ms": t * 1e3, "alg_bytes": alg, "gbs": alg / t / 1e9,
+                     "kernel": "k_dss_box" if box else "k_dss_csr"}
     return out
 
 

@@ -69,45 +69,6 @@ enum {
 // and (box only) lattice coordinates g; each(c, g, f) calls f(m) for the
 // members m of the node in ascending local id; mult(c, g) is the count.
 
-// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund & Montgomery,
-// "Division by invariant integers using multiplication", PLDI 1994, sec. 4):
-// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
-// q = (mulhi(m, n) + n) >> l  (the add cannot overflow for n < 2^31).
-struct FastDiv {
-  uint32_t m;
-  int l;
-  static FastDiv make(int d) {
-    FastDiv f;
-    f.l = 0;
-    while ((int64_t(1) << f.l) < d) f.l++;
-    f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.l) - (uint64_t)d)) / (uint64_t)d + 1);
-    return f;
-  }
-  __device__ __forceinline__ int div(int n) const {
-    return (int)((__umulhi((uint32_t)n, m) + (uint32_t)n) >> l);
-  }
-};
-
-// The element copies of lattice coordinate g along one direction, as
-// offsets into the E-vector (es = the element stride, ls = the local
-// index stride), in ascending element coordinate; returns their count.
-// Off an element face the one copy is (q, r); on a face (r = 0) the copies
-// are (q - 1, P) and (q, 0), the first wrapping to (ne - 1, P) and coming
-// second when periodic and q = 0, and only one of them on a non-periodic
-// boundary.  Branch-free: neighbouring threads of a warp take different
-// cases.
-template <int P>
-__device__ __forceinline__ int lattice_offsets(int g, int ne, int per, int es, int ls, int &o0,
-                                               int &o1) {
-  const int q = g / P, r = g - q * P;
-  const int hi = q * es + r * ls;
-  const int lo = ((q == 0 ? ne : q) - 1) * es + P * ls;
-  const bool face = r == 0;
-  o0 = (face && q != 0) ? lo : hi;
-  o1 = q == 0 ? lo : hi;
-  return !face ? 1 : ((per || (q != 0 && q != ne)) ? 2 : 1);
-}
-
 // Box lattice of order N-1.  Blocks walk lattice rows (fixed gy, gz), so a
 // node's coordinates come from the launch shape, and the order being a
 // compile-time constant turns every % and / by p into a multiply-shift.

@@ -331,6 +331,18 @@ extern "C" int gf_dudt(gf_problem_t prob, int dtype, int eqn, double nu, int nst
 template <typename T>
 int launch_dss(gf_problem *prob, int op, T *u, cudaStream_t st) {
   unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
+  BoxWalk w;
+  if (dss_box_walk(prob, w)) {  // lattice classes: no index arrays
+    prob->launches++;
+    switch (op) {
+      case GF_DSS_SUM: k_dss_box<T, GF_DSS_SUM><<<grid, 256, 0, st>>>(u, w); break;
+      case GF_DSS_SMOOTH: k_dss_box<T, GF_DSS_SMOOTH><<<grid, 256, 0, st>>>(u, w); break;
+      case GF_DSS_MAX: k_dss_box<T, GF_DSS_MAX><<<grid, 256, 0, st>>>(u, w); break;
+      case GF_DSS_MIN: k_dss_box<T, GF_DSS_MIN><<<grid, 256, 0, st>>>(u, w); break;
+      default: prob->launches--; return GF_ERR_ARG;
+    }
+    return GF_OK;
+  }
   switch (op) {
     case GF_DSS_SUM:
       prob->launches++;

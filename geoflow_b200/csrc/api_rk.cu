@@ -102,32 +102,51 @@ void Stepper<T>::smooth(T *v) {
   launch_dss<T>(prob, GF_DSS_SMOOTH, v, st);
 }
 
-// gather-scatter Smooth fused with the stage update around it (k_dss.cuh)
+// gather-scatter Smooth fused with the stage update around it (k_dss.cuh);
+// box-lattice problems take the index-free kernels
 template <typename T>
 void Stepper<T>::euler_smooth(T *x, T dt, const T *uin, T a, const T *y, T b, T a2, const T *y2,
                               T b2) {
   prob->launches++;
-  k_dss_rk_csr<T, FUSE_EULER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256, 0,
-                                st>>>(x, prob->class_ptr, prob->members, prob->nclass, dt, uin,
-                                      a, y, b, a2, y2, b2, nullptr, nullptr, T(0));
+  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
+  BoxWalk w;
+  if (dss_box_walk(prob, w))
+    k_dss_rk_box<T, FUSE_EULER><<<grid, 256, 0, st>>>(x, w, dt, uin, a, y, b, a2, y2, b2, nullptr,
+                                                      nullptr, T(0));
+  else
+    k_dss_rk_csr<T, FUSE_EULER><<<grid, 256, 0, st>>>(x, prob->class_ptr, prob->members,
+                                                      prob->nclass, dt, uin, a, y, b, a2, y2, b2,
+                                                      nullptr, nullptr, T(0));
 }
 
 template <typename T>
 void Stepper<T>::smooth_accum(T *K, T ch, T *uout) {
   prob->launches++;
-  k_dss_rk_csr<T, FUSE_ACCUM_AFTER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256,
-                                      0, st>>>(K, prob->class_ptr, prob->members, prob->nclass,
-                                               T(0), nullptr, T(0), nullptr, T(0), T(0),
-                                               nullptr, T(0), uout, nullptr, ch);
+  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
+  BoxWalk w;
+  if (dss_box_walk(prob, w))
+    k_dss_rk_box<T, FUSE_ACCUM_AFTER><<<grid, 256, 0, st>>>(K, w, T(0), nullptr, T(0), nullptr,
+                                                            T(0), T(0), nullptr, T(0), uout,
+                                                            nullptr, ch);
+  else
+    k_dss_rk_csr<T, FUSE_ACCUM_AFTER><<<grid, 256, 0, st>>>(
+        K, prob->class_ptr, prob->members, prob->nclass, T(0), nullptr, T(0), nullptr, T(0), T(0),
+        nullptr, T(0), uout, nullptr, ch);
 }
 
 template <typename T>
 void Stepper<T>::accum_smooth(T *uout, const T *K, T ch) {
   prob->launches++;
-  k_dss_rk_csr<T, FUSE_ACCUM_BEFORE><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16),
-                                       256, 0, st>>>(uout, prob->class_ptr, prob->members,
-                                                     prob->nclass, T(0), nullptr, T(0), nullptr,
-                                                     T(0), T(0), nullptr, T(0), nullptr, K, ch);
+  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
+  BoxWalk w;
+  if (dss_box_walk(prob, w))
+    k_dss_rk_box<T, FUSE_ACCUM_BEFORE><<<grid, 256, 0, st>>>(uout, w, T(0), nullptr, T(0),
+                                                             nullptr, T(0), T(0), nullptr, T(0),
+                                                             nullptr, K, ch);
+  else
+    k_dss_rk_csr<T, FUSE_ACCUM_BEFORE><<<grid, 256, 0, st>>>(
+        uout, prob->class_ptr, prob->members, prob->nclass, T(0), nullptr, T(0), nullptr, T(0),
+        T(0), nullptr, T(0), nullptr, K, ch);
 }
 
 template <typename T>

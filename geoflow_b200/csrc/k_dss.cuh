@@ -48,6 +48,57 @@ __device__ __forceinline__ T class_fold(const T *__restrict__ u, const int32_t *
   return acc;
 }
 
+// The box-lattice walk of a problem whose gather-scatter can take the box
+// kernels below: a GGridBox problem (classes = lattice points) with no
+// periodic direction of a single element (members then come in the
+// (z, y, x) nesting in ascending local id).
+inline bool dss_box_walk(const gf_problem *prob, BoxWalk &w) {
+  if (!prob->has_box) return false;
+  w = BoxWalk::make(prob->box);
+  return w.sorted;
+}
+
+// class_fold over the copies of one box-lattice point (ascending local id)
+template <typename T, int OP>
+__device__ __forceinline__ T box_fold(const T *__restrict__ u, const BoxCopies &k) {
+  T acc;
+  if (OP == GF_DSS_SUM || OP == GF_DSS_SMOOTH) {
+    acc = T(0);
+    k.each([&](int m) { acc = __fadd_rn_t(acc, u[m]); });
+    if (OP == GF_DSS_SMOOTH) acc = acc / (T)k.count();
+  } else if (OP == GF_DSS_MAX) {
+    acc = Lim<T>::lowest();
+    k.each([&](int m) {
+      const T v = u[m];
+      acc = (acc < v) ? v : acc;
+    });
+  } else {
+    acc = Lim<T>::highest();
+    k.each([&](int m) {
+      const T v = u[m];
+      acc = (v < acc) ? v : acc;
+    });
+  }
+  return acc;
+}
+
+// Box-lattice form of k_dss_csr (GGridBox problems, whose classes are the
+// lattice points; no periodic direction with a single element): one thread
+// per lattice point in lattice order, the members computed from the
+// point's coordinates (BoxWalk) in ascending local id, so no index arrays
+// are read and a point costs one memory round trip.  Same folds, same
+// order: bit-identical to the CSR form.
+template <typename T, int OP>
+__global__ void __launch_bounds__(256) k_dss_box(T *__restrict__ u, BoxWalk w) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nL;
+       c = (c < w.nL - stride) ? c + stride : w.nL) {
+    const BoxCopies k = w.copies(c);
+    const T acc = box_fold<T, OP>(u, k);
+    k.each([&](int m) { u[m] = acc; });
+  }
+}
+
 template <typename T, int OP>
 __global__ void __launch_bounds__(256)
     k_dss_csr(T *__restrict__ u, const int32_t *__restrict__ ptr,
@@ -110,6 +161,32 @@ __global__ void __launch_bounds__(256)
       x[m] = acc;
       if (MODE == FUSE_ACCUM_AFTER) acc_out[m] = rk_accum_point(acc_out[m], acc, ch);
     }
+  }
+}
+
+// Box-lattice form of k_dss_rk_csr (conditions of k_dss_box): the same
+// per-member stage arithmetic and Smooth fold, bit-identical.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256, 4)
+    k_dss_rk_box(T *__restrict__ x, BoxWalk w, T dt, const T *__restrict__ uin, T a,
+                 const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2,
+                 T *__restrict__ acc_out, const T *__restrict__ K, T ch) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nL;
+       c = (c < w.nL - stride) ? c + stride : w.nL) {
+    const BoxCopies k = w.copies(c);
+    T acc = T(0);
+    k.each([&](int m) {
+      T v = x[m];
+      if (MODE == FUSE_EULER) v = rk_euler_point(v, dt, uin[m], a, y, b, a2, y2, b2, (int64_t)m);
+      if (MODE == FUSE_ACCUM_BEFORE) v = rk_accum_point(v, K[m], ch);
+      acc = __fadd_rn_t(acc, v);
+    });
+    acc = acc / (T)k.count();
+    k.each([&](int m) {
+      x[m] = acc;
+      if (MODE == FUSE_ACCUM_AFTER) acc_out[m] = rk_accum_point(acc_out[m], acc, ch);
+    });
   }
 }
 

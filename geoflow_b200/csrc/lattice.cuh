@@ -114,4 +114,118 @@ struct BoxLattice {
   }
 };
 
+// n / d for 0 <= n < 2^31 by a multiply and a shift (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, sec. 4):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// q = (mulhi(m, n) + n) >> l  (the add cannot overflow for n < 2^31).
+struct FastDiv {
+  uint32_t m;
+  int l;
+  static FastDiv make(int d) {
+    FastDiv f;
+    f.l = 0;
+    while ((int64_t(1) << f.l) < d) f.l++;
+    f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.l) - (uint64_t)d)) / (uint64_t)d + 1);
+    return f;
+  }
+  __device__ __forceinline__ int div(int n) const {
+    return (int)((__umulhi((uint32_t)n, m) + (uint32_t)n) >> l);
+  }
+};
+
+// The element copies of the lattice coordinate g = q P + r along one
+// direction, as offsets into the E-vector (es = the element stride, ls = the
+// local index stride), in ascending element coordinate; returns their
+// count.  Off an element face the one copy is (q, r); on a face (r = 0) the
+// copies are (q - 1, P) and (q, 0), the first wrapping to (ne - 1, P) and
+// coming second when periodic and q = 0, and only one of them on a
+// non-periodic boundary.  Branch-free: neighbouring threads of a warp take
+// different cases.
+__device__ __forceinline__ int lattice_offsets_qr(int q, int r, int P, int ne, int per, int es,
+                                                  int ls, int &o0, int &o1) {
+  const int hi = q * es + r * ls;
+  const int lo = ((q == 0 ? ne : q) - 1) * es + P * ls;
+  const bool face = r == 0;
+  o0 = (face && q != 0) ? lo : hi;
+  o1 = q == 0 ? lo : hi;
+  return !face ? 1 : ((per || (q != 0 && q != ne)) ? 2 : 1);
+}
+template <int P>
+__device__ __forceinline__ int lattice_offsets(int g, int ne, int per, int es, int ls, int &o0,
+                                               int &o1) {
+  const int q = g / P;
+  return lattice_offsets_qr(q, g - q * P, P, ne, per, es, ls, o0, o1);
+}
+
+// The copies of one lattice point: per direction one or two offsets.
+// each() visits them in the (z, y, x) nesting, which is ascending local id
+// when no periodic direction has a single element.
+struct BoxCopies {
+  int ox0, ox1, oy0, oy1, oz0, oz1, nx, ny, nz;
+  __device__ __forceinline__ int count() const { return nx * ny * nz; }
+  template <class F>
+  __device__ __forceinline__ void each(F f) const {
+#pragma unroll
+    for (int az = 0; az < 2; az++) {
+      if (az >= nz) break;
+      const int oz = az ? oz1 : oz0;
+#pragma unroll
+      for (int ay = 0; ay < 2; ay++) {
+        if (ay >= ny) break;
+        const int o = oz + (ay ? oy1 : oy0);
+        f(o + ox0);
+        if (nx > 1) f(o + ox1);
+      }
+    }
+  }
+};
+
+// Flat walk of a box lattice with the order a run-time value: the copies of
+// lattice point c from three multiply-shift divisions, no index arrays.
+// Lattice and element-local sizes below 2^31.
+struct BoxWalk {
+  int dim, P, ne[3], per[3], M[3], nL, es[3];
+  bool sorted;  // no periodic direction with a single element
+  FastDiv f0, f1, fP;
+  static BoxWalk make(const BoxLattice &L) {
+    BoxWalk w;
+    w.dim = L.dim;
+    w.P = L.p;
+    const int n = L.p + 1, nn = L.dim > 2 ? n * n * n : n * n;
+    w.sorted = true;
+    for (int d = 0; d < 3; d++) {
+      w.ne[d] = d < L.dim ? L.ne[d] : 1;
+      w.per[d] = d < L.dim ? L.per[d] : 0;
+      w.M[d] = d < L.dim ? (int)L.M[d] : 1;
+      if (d < L.dim && L.per[d] && L.ne[d] == 1) w.sorted = false;
+    }
+    w.nL = w.M[0] * w.M[1] * w.M[2];
+    w.es[0] = nn;
+    w.es[1] = w.ne[0] * nn;
+    w.es[2] = w.ne[0] * w.ne[1] * nn;
+    w.f0 = FastDiv::make(w.M[0]);
+    w.f1 = FastDiv::make(w.M[1]);
+    w.fP = FastDiv::make(w.P);
+    return w;
+  }
+  __device__ __forceinline__ BoxCopies copies(int c) const {
+    const int row = f0.div(c), g0 = c - row * M[0];
+    const int g2 = f1.div(row), g1 = row - g2 * M[1];
+    BoxCopies k;
+    int q = fP.div(g0);
+    k.nx = lattice_offsets_qr(q, g0 - q * P, P, ne[0], per[0], es[0], 1, k.ox0, k.ox1);
+    q = fP.div(g1);
+    k.ny = lattice_offsets_qr(q, g1 - q * P, P, ne[1], per[1], es[1], P + 1, k.oy0, k.oy1);
+    if (dim > 2) {
+      q = fP.div(g2);
+      k.nz = lattice_offsets_qr(q, g2 - q * P, P, ne[2], per[2], es[2], (P + 1) * (P + 1), k.oz0,
+                                k.oz1);
+    } else {
+      k.oz0 = k.oz1 = 0;
+      k.nz = 1;
+    }
+    return k;
+  }
+};
+
 }  // namespace gfk

@@ -142,6 +142,7 @@ class Problem:
         of (dim*nxy + 1) * ndof values, nxy = dim or 3.  node_xyz (3 * ndof,
         optional) are the node coordinates used by constrain2sphere."""
         self.ctx, self.grid, self.geometry = ctx, grid, geometry
+        self.structured = structured
         self.dim, self.n, self.nlocal = grid.dim, grid.n, grid.ndof()
         # velocity components: one per physical coordinate
         self.nvel = 3 if geometry == "embedded" else grid.dim
