@@ -102,51 +102,107 @@ void Stepper<T>::smooth(T *v) {
   launch_dss<T>(prob, GF_DSS_SMOOTH, v, st);
 }
 
-// gather-scatter Smooth fused with the stage update around it (k_dss.cuh);
-// box-lattice problems take the index-free kernels
+// gather-scatter Smooth fused with the stage update around it, one
+// component, CSR members (k_dss.cuh); box problems take the *_n forms below
 template <typename T>
 void Stepper<T>::euler_smooth(T *x, T dt, const T *uin, T a, const T *y, T b, T a2, const T *y2,
                               T b2) {
   prob->launches++;
-  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
-  BoxWalk w;
-  if (dss_box_walk(prob, w))
-    k_dss_rk_box<T, FUSE_EULER><<<grid, 256, 0, st>>>(x, w, dt, uin, a, y, b, a2, y2, b2, nullptr,
-                                                      nullptr, T(0));
-  else
-    k_dss_rk_csr<T, FUSE_EULER><<<grid, 256, 0, st>>>(x, prob->class_ptr, prob->members,
-                                                      prob->nclass, dt, uin, a, y, b, a2, y2, b2,
-                                                      nullptr, nullptr, T(0));
+  k_dss_rk_csr<T, FUSE_EULER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256, 0,
+                                st>>>(x, prob->class_ptr, prob->members, prob->nclass, dt, uin,
+                                      a, y, b, a2, y2, b2, nullptr, nullptr, T(0));
 }
 
 template <typename T>
 void Stepper<T>::smooth_accum(T *K, T ch, T *uout) {
   prob->launches++;
-  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
-  BoxWalk w;
-  if (dss_box_walk(prob, w))
-    k_dss_rk_box<T, FUSE_ACCUM_AFTER><<<grid, 256, 0, st>>>(K, w, T(0), nullptr, T(0), nullptr,
-                                                            T(0), T(0), nullptr, T(0), uout,
-                                                            nullptr, ch);
-  else
-    k_dss_rk_csr<T, FUSE_ACCUM_AFTER><<<grid, 256, 0, st>>>(
-        K, prob->class_ptr, prob->members, prob->nclass, T(0), nullptr, T(0), nullptr, T(0), T(0),
-        nullptr, T(0), uout, nullptr, ch);
+  k_dss_rk_csr<T, FUSE_ACCUM_AFTER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256,
+                                      0, st>>>(K, prob->class_ptr, prob->members, prob->nclass,
+                                               T(0), nullptr, T(0), nullptr, T(0), T(0),
+                                               nullptr, T(0), uout, nullptr, ch);
 }
 
 template <typename T>
 void Stepper<T>::accum_smooth(T *uout, const T *K, T ch) {
   prob->launches++;
-  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
+  k_dss_rk_csr<T, FUSE_ACCUM_BEFORE><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16),
+                                       256, 0, st>>>(uout, prob->class_ptr, prob->members,
+                                                     prob->nclass, T(0), nullptr, T(0), nullptr,
+                                                     T(0), T(0), nullptr, T(0), nullptr, K, ch);
+}
+
+// Launch k_dss_rk_box_n / k_dss_smooth_box_n for nstate components; false
+// when the problem takes the per-component CSR kernels.
+template <typename T, int MODE>
+static bool launch_rk_n(gf_problem *prob, cudaStream_t st, int nstate, const RKComps<T> &pc,
+                        T dt, T a, T b, T a2, T b2, T ch, bool plain) {
   BoxWalk w;
-  if (dss_box_walk(prob, w))
-    k_dss_rk_box<T, FUSE_ACCUM_BEFORE><<<grid, 256, 0, st>>>(uout, w, T(0), nullptr, T(0),
-                                                             nullptr, T(0), T(0), nullptr, T(0),
-                                                             nullptr, K, ch);
-  else
-    k_dss_rk_csr<T, FUSE_ACCUM_BEFORE><<<grid, 256, 0, st>>>(
-        uout, prob->class_ptr, prob->members, prob->nclass, T(0), nullptr, T(0), nullptr, T(0),
-        T(0), nullptr, T(0), nullptr, K, ch);
+  if (!dss_box_walk(prob, w) || nstate < 1 || nstate > 3) return false;
+  const unsigned grid = grid_for(prob->nclass, 256, prob->ctx->sm_count * 16);
+  prob->launches++;
+  if (plain) {
+    if (nstate == 1) k_dss_smooth_box_n<T, 1><<<grid, 256, 0, st>>>(pc, w);
+    else if (nstate == 2) k_dss_smooth_box_n<T, 2><<<grid, 256, 0, st>>>(pc, w);
+    else k_dss_smooth_box_n<T, 3><<<grid, 256, 0, st>>>(pc, w);
+  } else {
+    if (nstate == 1) k_dss_rk_box_n<T, MODE, 1><<<grid, 256, 0, st>>>(pc, w, dt, a, b, a2, b2, ch);
+    else if (nstate == 2) k_dss_rk_box_n<T, MODE, 2><<<grid, 256, 0, st>>>(pc, w, dt, a, b, a2, b2, ch);
+    else k_dss_rk_box_n<T, MODE, 3><<<grid, 256, 0, st>>>(pc, w, dt, a, b, a2, b2, ch);
+  }
+  return true;
+}
+
+template <typename T>
+static RKComps<T> comps(int nstate, T *const *x, T *const *uin, T *const *y, T *const *y2,
+                        T *const *K, T *const *acc) {
+  RKComps<T> pc{};
+  for (int k = 0; k < nstate && k < 3; k++) {
+    pc.x[k] = x[k];
+    pc.uin[k] = uin ? uin[k] : nullptr;
+    pc.y[k] = y ? y[k] : nullptr;
+    pc.y2[k] = y2 ? y2[k] : nullptr;
+    pc.K[k] = K ? K[k] : nullptr;
+    pc.acc[k] = acc ? acc[k] : nullptr;
+  }
+  return pc;
+}
+
+template <typename T>
+void Stepper<T>::smooth_n(T *const *v) {
+  if (launch_rk_n<T, FUSE_EULER>(prob, st, nstate,
+                                 comps<T>(nstate, v, nullptr, nullptr, nullptr, nullptr, nullptr),
+                                 T(0), T(0), T(0), T(0), T(0), T(0), true))
+    return;
+  for (int k = 0; k < nstate; k++) smooth(v[k]);
+}
+
+template <typename T>
+void Stepper<T>::euler_smooth_n(T *const *x, T dt, T *const *uin, T a, T *const *y, T b, T a2,
+                                T *const *y2, T b2) {
+  if (launch_rk_n<T, FUSE_EULER>(prob, st, nstate,
+                                 comps<T>(nstate, x, uin, y, y2, nullptr, nullptr), dt, a, b, a2,
+                                 b2, T(0), false))
+    return;
+  for (int k = 0; k < nstate; k++)
+    euler_smooth(x[k], dt, uin[k], a, y ? y[k] : nullptr, b, a2, y2 ? y2[k] : nullptr, b2);
+}
+
+template <typename T>
+void Stepper<T>::smooth_accum_n(T *const *Kv, T ch, T *const *uout) {
+  if (launch_rk_n<T, FUSE_ACCUM_AFTER>(
+          prob, st, nstate, comps<T>(nstate, Kv, nullptr, nullptr, nullptr, nullptr, uout), T(0),
+          T(0), T(0), T(0), T(0), ch, false))
+    return;
+  for (int k = 0; k < nstate; k++) smooth_accum(Kv[k], ch, uout[k]);
+}
+
+template <typename T>
+void Stepper<T>::accum_smooth_n(T *const *uout, T *const *Kv, T ch) {
+  if (launch_rk_n<T, FUSE_ACCUM_BEFORE>(
+          prob, st, nstate, comps<T>(nstate, uout, nullptr, nullptr, nullptr, Kv, nullptr), T(0),
+          T(0), T(0), T(0), T(0), ch, false))
+    return;
+  for (int k = 0; k < nstate; k++) accum_smooth(uout[k], Kv[k], ch);
 }
 
 template <typename T>
@@ -195,7 +251,7 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
       }
       constrain(um);
       if ((rc = rhs(um, K[m]))) return rc;
-      for (int k = 0; k < nstate; k++) smooth_accum(K[m][k], (T)cc[m] * h, uout[k]);
+      smooth_accum_n(K[m], (T)cc[m] * h, uout);
       constrain(uout);
     }
     T *const *uf = stage_in(ns - 1);
@@ -204,15 +260,15 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
       k_stage_sum<T><<<g, 256, 0, st>>>(n, uin[k], ns - 1, K[0][k], K[1][k], K[2][k],
                                         (T)beta[ns - 1][0] * h, (T)beta[ns - 1][1] * h,
                                         (T)beta[ns - 1][2] * h, uf[k]);
-      smooth(uf[k]);
     }
+    smooth_n(uf);
     constrain(uf);
     // the final stage result goes to the last K slot (K[0] in the
     // reference, whose earlier content is no longer needed)
     T *const *Kf = K[0];
     if ((rc = rhs(uf, Kf))) return rc;
-    for (int k = 0; k < nstate; k++) smooth(Kf[k]);
-    for (int k = 0; k < nstate; k++) accum_smooth(uout[k], Kf[k], (T)cc[ns - 1] * h);
+    smooth_n(Kf);
+    accum_smooth_n(uout, Kf, (T)cc[ns - 1] * h);
     constrain(uout);
     return GF_OK;
   }
@@ -236,47 +292,29 @@ int Stepper<T>::step_ssp(T *const *uin, T *const *uout, T dt) {
   const T one = T(1);
   if (scheme == GF_SSP22) {
     if ((rc = rhs(uin, K[0]))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
-    }
+    euler_smooth_n(K[0], dt, uin, one, nullptr, T(0), one, nullptr, T(0));
     if ((rc = rhs(K[0], uout))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(uout[k], dt, K[0][k], T(0.5), uin[k], T(0.5), one, nullptr, T(0));
-    }
+    euler_smooth_n(uout, dt, K[0], T(0.5), uin, T(0.5), one, nullptr, T(0));
     return GF_OK;
   }
   if (scheme == GF_SSP33) {
     if ((rc = rhs(uin, K[0]))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(K[0][k], dt, uin[k], one, nullptr, T(0), one, nullptr, T(0));
-    }
+    euler_smooth_n(K[0], dt, uin, one, nullptr, T(0), one, nullptr, T(0));
     if ((rc = rhs(K[0], K[1]))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(K[1][k], dt, K[0][k], T(0.25), uin[k], T(0.75), one, nullptr, T(0));
-    }
+    euler_smooth_n(K[1], dt, K[0], T(0.25), uin, T(0.75), one, nullptr, T(0));
     if ((rc = rhs(K[1], uout))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(uout[k], dt, K[1][k], T(2.0 / 3.0), uin[k], T(1.0 / 3.0), one, nullptr, T(0));
-    }
+    euler_smooth_n(uout, dt, K[1], T(2.0 / 3.0), uin, T(1.0 / 3.0), one, nullptr, T(0));
     return GF_OK;
   }
   if (scheme == GF_SSP34) {
     if ((rc = rhs(uin, K[0]))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(K[0][k], dt, uin[k], T(0.5), uin[k], T(0.5), one, nullptr, T(0));
-    }
+    euler_smooth_n(K[0], dt, uin, T(0.5), uin, T(0.5), one, nullptr, T(0));
     if ((rc = rhs(K[0], K[1]))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(K[1][k], dt, K[0][k], T(0.5), K[0][k], T(0.5), one, nullptr, T(0));
-    }
+    euler_smooth_n(K[1], dt, K[0], T(0.5), K[0], T(0.5), one, nullptr, T(0));
     if ((rc = rhs(K[1], K[2]))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(K[2][k], dt, K[1][k], T(1.0 / 6.0), K[1][k], T(1.0 / 6.0), one, uin[k], T(2.0 / 3.0));
-    }
+    euler_smooth_n(K[2], dt, K[1], T(1.0 / 6.0), K[1], T(1.0 / 6.0), one, uin, T(2.0 / 3.0));
     if ((rc = rhs(K[2], uout))) return rc;
-    for (int k = 0; k < nstate; k++) {
-      euler_smooth(uout[k], dt, K[2][k], T(0.5), K[2][k], T(0.5), one, nullptr, T(0));
-    }
+    euler_smooth_n(uout, dt, K[2], T(0.5), K[2], T(0.5), one, nullptr, T(0));
     return GF_OK;
   }
   return GF_ERR_ARG;

@@ -164,29 +164,70 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Box-lattice form of k_dss_rk_csr (conditions of k_dss_box): the same
-// per-member stage arithmetic and Smooth fold, bit-identical.
-template <typename T, int MODE>
+// The state components of one fused stage update (pointers per component;
+// y, y2, uin, K, acc may be null as in k_dss_rk_csr).
+template <typename T>
+struct RKComps {
+  T *x[3];
+  const T *uin[3], *y[3], *y2[3], *K[3];
+  T *acc[3];
+};
+
+// Box-lattice form of k_dss_rk_csr (conditions of k_dss_box) on every
+// state component in one pass: the copies of a lattice point are computed
+// once, and every component's members are read before any is written (all
+// loads of a point in one memory round trip).  Per component the same
+// stage arithmetic, Smooth fold and order as k_dss_rk_csr: bit-identical.
+template <typename T, int MODE, int NC>
 __global__ void __launch_bounds__(256, 4)
-    k_dss_rk_box(T *__restrict__ x, BoxWalk w, T dt, const T *__restrict__ uin, T a,
-                 const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2,
-                 T *__restrict__ acc_out, const T *__restrict__ K, T ch) {
+    k_dss_rk_box_n(RKComps<T> p, BoxWalk w, T dt, T a, T b, T a2, T b2, T ch) {
   const int stride = gridDim.x * blockDim.x;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nL;
        c = (c < w.nL - stride) ? c + stride : w.nL) {
     const BoxCopies k = w.copies(c);
-    T acc = T(0);
-    k.each([&](int m) {
-      T v = x[m];
-      if (MODE == FUSE_EULER) v = rk_euler_point(v, dt, uin[m], a, y, b, a2, y2, b2, (int64_t)m);
-      if (MODE == FUSE_ACCUM_BEFORE) v = rk_accum_point(v, K[m], ch);
-      acc = __fadd_rn_t(acc, v);
-    });
-    acc = acc / (T)k.count();
-    k.each([&](int m) {
-      x[m] = acc;
-      if (MODE == FUSE_ACCUM_AFTER) acc_out[m] = rk_accum_point(acc_out[m], acc, ch);
-    });
+    T acc[NC];
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      const T *__restrict__ x = p.x[j];
+      const T *__restrict__ uin = p.uin[j];
+      const T *__restrict__ Kj = p.K[j];
+      T s = T(0);
+      k.each([&](int m) {
+        T v = x[m];
+        if (MODE == FUSE_EULER)
+          v = rk_euler_point(v, dt, uin[m], a, p.y[j], b, a2, p.y2[j], b2, (int64_t)m);
+        if (MODE == FUSE_ACCUM_BEFORE) v = rk_accum_point(v, Kj[m], ch);
+        s = __fadd_rn_t(s, v);
+      });
+      acc[j] = s / (T)k.count();
+    }
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      T *__restrict__ x = p.x[j];
+      T *__restrict__ ao = p.acc[j];
+      k.each([&](int m) {
+        x[m] = acc[j];
+        if (MODE == FUSE_ACCUM_AFTER) ao[m] = rk_accum_point(ao[m], acc[j], ch);
+      });
+    }
+  }
+}
+
+// k_dss_box Smooth on every state component in one pass
+template <typename T, int NC>
+__global__ void __launch_bounds__(256) k_dss_smooth_box_n(RKComps<T> p, BoxWalk w) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nL;
+       c = (c < w.nL - stride) ? c + stride : w.nL) {
+    const BoxCopies k = w.copies(c);
+    T acc[NC];
+#pragma unroll
+    for (int j = 0; j < NC; j++) acc[j] = box_fold<T, GF_DSS_SMOOTH>(p.x[j], k);
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      T *__restrict__ x = p.x[j];
+      k.each([&](int m) { x[m] = acc[j]; });
+    }
   }
 }
 

@@ -37,6 +37,13 @@ struct Stepper {
   void euler_smooth(T *x, T dt, const T *uin, T a, const T *y, T b, T a2, const T *y2, T b2);
   void smooth_accum(T *K, T ch, T *uout);
   void accum_smooth(T *uout, const T *K, T ch);
+  // the same on every state component (arrays of nstate pointers; y and y2
+  // may be null): one pass over the lattice on box problems
+  void smooth_n(T *const *v);
+  void euler_smooth_n(T *const *x, T dt, T *const *uin, T a, T *const *y, T b, T a2,
+                      T *const *y2, T b2);
+  void smooth_accum_n(T *const *K, T ch, T *const *uout);
+  void accum_smooth_n(T *const *uout, T *const *K, T ch);
   // One step uin -> uout.  With a tape (pointers tape[3*m + k], m = 0 ..
   // stages-1), stage m's input state (the argument of its RHS call) is left
   // in tape[3*m + k] for the adjoint sweep.

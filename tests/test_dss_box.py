@@ -1,4 +1,4 @@
-"""Box-lattice gather-scatter (k_dss_box, k_dss_rk_box: members computed from
+"""Box-lattice gather-scatter (k_dss_box, k_dss_rk_box_n: members computed from
 the lattice point's coordinates) against the CSR kernels (k_dss_csr,
 k_dss_rk_csr: members read from class_ptr/members) on the same grid built
 without its box description (Problem(structured=False)).  Both fold the
@@ -69,3 +69,17 @@ def test_rk_stages_box_equal_csr(ctx, scheme, dim, ne, p, per):
         GBurgers(pc, GBurgers.BURGERS, 1e-2, scheme=scheme).step(uc, None, dt=1e-3, nsteps=3)
         for a, b in zip(ub, uc):
             assert bits_equal(a, b), (dt, scheme)
+
+
+@pytest.mark.parametrize("scheme", [A.GF_RK4, A.GF_SSP33, A.GF_SSP34])
+def test_rk_stages_box_equal_csr_one_component(ctx, scheme):
+    import torch
+    from geoflow_b200 import GBurgers
+    g, pb, pc = pair(ctx, *SHAPES[0])
+    u0 = np.random.default_rng(scheme + 7).standard_normal(g.ndof())
+    for dt in (torch.float64, torch.float32):
+        ub = [torch.from_numpy(u0).to(device="cuda", dtype=dt)]
+        uc = [ub[0].clone()]
+        GBurgers(pb, GBurgers.HEAT, 5e-2, scheme=scheme).step(ub, None, dt=1e-3, nsteps=3)
+        GBurgers(pc, GBurgers.HEAT, 5e-2, scheme=scheme).step(uc, None, dt=1e-3, nsteps=3)
+        assert bits_equal(ub[0], uc[0]), (dt, scheme)
