@@ -179,7 +179,7 @@ struct RKComps {
 // loads of a point in one memory round trip).  Per component the same
 // stage arithmetic, Smooth fold and order as k_dss_rk_csr: bit-identical.
 template <typename T, int MODE, int NC>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 5)
     k_dss_rk_box_n(RKComps<T> p, BoxWalk w, T dt, T a, T b, T a2, T b2, T ch) {
   const int stride = gridDim.x * blockDim.x;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nL;
