@@ -121,6 +121,15 @@ __global__ void __launch_bounds__(N *N *EPB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *su = reinterpret_cast<T *>(smem_raw) + threadIdx.y * 2 * VOL;
   T *sr = su + VOL;
+  // FP32 at N = 8: rows of 8 at stride 8 in planes of 72 words, the two
+  // 16-byte halves of rows 4..7 swapped (an XOR swizzle), so that an x-line
+  // moves as two 128-bit accesses and both these and the scalar y-/z-line
+  // accesses are free of bank conflicts; otherwise rows at stride P.
+  constexpr bool VX = sizeof(T) == 4 && N == 8;
+  constexpr int RS = VX ? N : P;
+  auto at = [](int k, int r, int c) {
+    return k * PLANE + r * RS + (VX ? (c ^ (r & 4)) : c);
+  };
   const int t = threadIdx.x;
   const int64_t e = (int64_t)blockIdx.x * EPB + threadIdx.y;
   const bool active = e < ne;
@@ -150,22 +159,39 @@ __global__ void __launch_bounds__(N *N *EPB)
     for (int k = 0; k < N; k++) ru[k] = T(0);
   }
 #pragma unroll
-  for (int k = 0; k < N; k++) su[k * PLANE + a1 * P + a0] = ru[k];
+  for (int k = 0; k < N; k++) su[at(k, a1, a0)] = ru[k];
   __syncthreads();
   T ax[N], ay[N];
+  if constexpr (VX) {
+    // logical half h of row a0 is physical half h ^ sw; each thread takes
+    // its own first half first, which keeps each quarter warp on 32 banks
+    const int sw = (a0 >> 2) & 1;
+    const float4 *row = reinterpret_cast<const float4 *>(su + a1 * PLANE + a0 * RS);
+    const float4 h0 = row[sw], h1 = row[sw ^ 1];
+    ax[0] = h0.x, ax[1] = h0.y, ax[2] = h0.z, ax[3] = h0.w;
+    ax[4] = h1.x, ax[5] = h1.y, ax[6] = h1.z, ax[7] = h1.w;
+  } else {
 #pragma unroll
-  for (int m = 0; m < N; m++) ax[m] = su[a1 * PLANE + a0 * P + m];
+    for (int m = 0; m < N; m++) ax[m] = su[at(a1, a0, m)];
+  }
 #pragma unroll
-  for (int m = 0; m < N; m++) ay[m] = su[a1 * PLANE + m * P + a0];
+  for (int m = 0; m < N; m++) ay[m] = su[at(a1, m, a0)];
   __syncthreads();
   {
     T y[N];
     line_K1<T, N>(B, ax, cx, y);
+    if constexpr (VX) {
+      const int sw = (a0 >> 2) & 1;
+      float4 *row = reinterpret_cast<float4 *>(su + a1 * PLANE + a0 * RS);
+      row[sw] = make_float4(y[0], y[1], y[2], y[3]);
+      row[sw ^ 1] = make_float4(y[4], y[5], y[6], y[7]);
+    } else {
 #pragma unroll
-    for (int i = 0; i < N; i++) su[a1 * PLANE + a0 * P + i] = y[i];
+      for (int i = 0; i < N; i++) su[at(a1, a0, i)] = y[i];
+    }
     line_K1<T, N>(B, ay, cy, y);
 #pragma unroll
-    for (int j = 0; j < N; j++) sr[a1 * PLANE + j * P + a0] = y[j];
+    for (int j = 0; j < N; j++) sr[at(a1, j, a0)] = y[j];
   }
   T yz[N];
   line_K1<T, N>(B, ru, cz, yz);
@@ -173,7 +199,7 @@ __global__ void __launch_bounds__(N *N *EPB)
   if (active) {
 #pragma unroll
     for (int k = 0; k < N; k++) {
-      const int s = k * PLANE + a1 * P + a0;
+      const int s = at(k, a1, a0);
       T o = (su[s] + sr[s]) + yz[k];
       if (use_mass) {
         const int64_t node = base + k * NN + a1 * N + a0;
