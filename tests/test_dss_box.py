@@ -17,7 +17,9 @@ pytestmark = pytest.mark.gpu
 
 SHAPES = [(3, [3, 2, 4], 4, [1, 0, 1]), (3, [2, 2, 2], 7, None), (2, [5, 3], 6, [0, 1]),
           (3, [4, 3, 2], 1, [1, 1, 0]), (3, [2, 3, 2], 5, [1, 1, 1]),
-          (2, [1, 4], 3, [1, 0])]  # the last: a single-element periodic direction (CSR both)
+          (2, [1, 4], 3, [1, 0]),  # a single-element periodic direction (CSR both)
+          # lattice rows longer than a block (281 and 601 points), and p = 11
+          (3, [40, 2, 2], 7, [0, 1, 0]), (2, [300, 2], 2, None), (3, [2, 2, 3], 11, [1, 0, 1])]
 
 
 def pair(ctx, dim, ne, p, per):
