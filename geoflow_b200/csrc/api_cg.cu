@@ -69,9 +69,11 @@ enum {
 // and (box only) lattice coordinates g; each(c, g, f) calls f(m) for the
 // members m of the node in ascending local id; mult(c, g) is the count.
 
-// Box lattice of order N-1.  Blocks walk lattice rows (fixed gy, gz), so a
-// node's coordinates come from the launch shape, and the order being a
-// compile-time constant turns every % and / by p into a multiply-shift.
+// Box lattice of order N-1.  rows() walks lattice rows (fixed gy, gz) by
+// block, so a node's coordinates come from the launch shape; rows_sum() walks
+// the flat lattice index with multiply-shift divisions by the lattice
+// widths (FastDiv); the order being a compile-time constant turns every %
+// and / by p into a multiply-shift.
 template <int N>
 struct MapBox {
   static constexpr int P = N - 1;
