@@ -22,7 +22,9 @@ template <int N, int NF> constexpr int epb_dudt3() {
 
 // fields[0..NF): ADVECT: {p, c0, c1, c2}; BURGERS: {u0, u1, u2}; HEAT: {u}.
 // Evolved components: ADVECT/HEAT: field 0; BURGERS: fields 0..2.
-template <typename T, int N, int EPB, int EQN, int MODE>
+// AFF: affine elements (g.egeom), known at compile time, so the per-node
+// geometry path (node indices and loads) is not compiled in.
+template <typename T, int N, int EPB, int EQN, int MODE, bool AFF>
 __global__ void __launch_bounds__(N *N *EPB)
     k_dudt3d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T nu,
              const T *__restrict__ f0, const T *__restrict__ f1, const T *__restrict__ f2,
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(N *N *EPB)
       for (int k = 0; k < N; k++) {
         const int sidx = k * PLANE + j * P + i;
         NodeGeom<T, 3> ng = eg;
-        if (active) node_geom<T, 3>(g, base + k * NN + j * N + i, ng);
+        if (!AFF && active) node_geom<T, 3>(g, base + k * NN + j * N + i, ng);
         const T mass = B.W[k] * B.W[j] * B.W[i] * ng.J;
         if (EQN != GF_EQN_HEAT) {
           const int cb = EQN == GF_EQN_ADVECT ? 1 : 0;
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(N *N *EPB)
 #pragma unroll
       for (int m = 0; m < N; m++) {
         NodeGeom<T, 3> ng = eg;
-        if (active) node_geom<T, 3>(g, base + k * NN + j * N + m, ng);
+        if (!AFF && active) node_geom<T, 3>(g, base + k * NN + j * N + m, ng);
         const T mass = B.W[k] * B.W[j] * B.W[m] * ng.J;
         a[m] = mass * (sdx[k * PLANE + j * P + m] * (ng.X[0] * ng.X[0]));
       }
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(N *N *EPB)
 #pragma unroll
       for (int m = 0; m < N; m++) {
         NodeGeom<T, 3> ng = eg;
-        if (active) node_geom<T, 3>(g, base + k * NN + m * N + i, ng);
+        if (!AFF && active) node_geom<T, 3>(g, base + k * NN + m * N + i, ng);
         const T mass = B.W[k] * B.W[m] * B.W[i] * ng.J;
         a[m] = mass * (sdy[k * PLANE + m * P + i] * (ng.X[1] * ng.X[1]));
       }
