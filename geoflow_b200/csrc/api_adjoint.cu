@@ -130,7 +130,9 @@ __global__ void __launch_bounds__(256)
 // of direction-m lines.
 template <int N> constexpr int epb_vjp3() { return (160 / (N * N)) < 1 ? 1 : 160 / (N * N); }
 
-template <int N, int EPB, int EQN>
+// AFF: affine elements (g.egeom) known at compile time, so the per-node
+// geometry path is not compiled in.
+template <int N, int EPB, int EQN, bool AFF>
 __global__ void __launch_bounds__(N *N *EPB)
     k_dudt_vjp3d(const __grid_constant__ Basis<double, N> B, const Geom<double> g, int64_t ne,
                  double nu, const double *__restrict__ c0, const double *__restrict__ c1,
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(N *N *EPB)
   // geometry and mass at local node (i, j, k)
   auto geo = [&](int i, int j, int k, NodeGeom<double, 3> &ng) {
     ng = eg;
-    if (active) node_geom<double, 3>(g, base + k * NN + j * N + i, ng);
+    if (!AFF && active) node_geom<double, 3>(g, base + k * NN + j * N + i, ng);
     return B.W[k] * B.W[j] * B.W[i] * ng.J;
   };
 #pragma unroll 1
@@ -254,7 +256,7 @@ int launch_vjp_n(gf_problem *prob, double nu, const double *const *c, const doub
     constexpr int EPB = epb_vjp3<N>();
     constexpr int NF = (EQN == GF_EQN_HEAT ? 0 : 3) + (EQN == GF_EQN_BURGERS ? 3 : 1) + 2;
     const size_t smem = sizeof(double) * NF * N * N * Pad<N>::P * EPB;
-    auto kern = k_dudt_vjp3d<N, EPB, EQN>;
+    auto kern = g.egeom ? k_dudt_vjp3d<N, EPB, EQN, true> : k_dudt_vjp3d<N, EPB, EQN, false>;
     set_smem(kern, smem);
     prob->launches++;
     kern<<<(unsigned)((prob->ne + EPB - 1) / EPB), dim3(N * N, EPB), smem, st>>>(
