@@ -407,7 +407,9 @@ struct Reverse {
     }
   }
   static int slots(int nstate) { return nstate * 6; }
-  void smooth(double *v) { launch_dss<double>(prob, GF_DSS_SMOOTH, v, st); }
+  // Smooth (its own transpose) on every state component: one lattice pass
+  // on box problems (the stepper's multi-component kernel), CSR otherwise
+  void smooth_n(double *const *v) { S.smooth_n(v); }
 
   // lam <- (d step/d uin)^T lam; tape[3*m + k] = input of stage m
   int run(double *const *tape, double *const *lam, double dt) {
@@ -420,8 +422,8 @@ struct Reverse {
   int butcher(double *const *tape, double *const *lam, double h) {
     double alpha[4], beta[4][4], cc[4];
     gfrk::butcher(S.scheme, alpha, beta, cc);
+    smooth_n(lam);
     for (int k = 0; k < nstate; k++) {
-      smooth(lam[k]);
       prob->launches++;
       k_adj_start<<<g, 256, 0, st>>>(n, lam[k], acc[k], lamK[0][k], ns > 1 ? lamK[1][k] : nullptr,
                                      ns > 2 ? lamK[2][k] : nullptr, ns > 3 ? lamK[3][k] : nullptr,
@@ -429,12 +431,12 @@ struct Reverse {
     }
     for (int m = ns - 1; m >= 0; m--) {
       double *mu[3] = {lamK[m][0], lamK[m][1], lamK[m][2]};
-      for (int k = 0; k < nstate; k++) smooth(mu[k]);
+      smooth_n(mu);
       const double *um[3] = {tape[3 * m], tape[3 * m + 1], tape[3 * m + 2]};
       int rc = vjp(prob, S.eqn, (double)S.nu, nstate, um, S.c, (const double *const *)mu, tmp);
       if (rc) return rc;
+      if (m == ns - 1) smooth_n(tmp);
       for (int k = 0; k < nstate; k++) {
-        if (m == ns - 1) smooth(tmp[k]);
         prob->launches++;
         k_adj_fan<<<g, 256, 0, st>>>(n, tmp[k], acc[k], m > 0 ? lamK[0][k] : nullptr,
                                      m > 1 ? lamK[1][k] : nullptr, m > 2 ? lamK[2][k] : nullptr,
@@ -476,7 +478,7 @@ struct Reverse {
         cudaMemsetAsync(lamK[m][k], 0, sizeof(double) * n, st);
     double *lout[3] = {lam[0], lam[1], lam[2]};  // cotangent of out_m
     for (int m = ns - 1; m >= 0; m--) {
-      for (int k = 0; k < nstate; k++) smooth(lout[k]);
+      smooth_n(lout);
       const double *um[3] = {tape[3 * m], tape[3 * m + 1], tape[3 * m + 2]};
       int rc = vjp(prob, S.eqn, (double)S.nu, nstate, um, S.c, (const double *const *)lout, tmp);
       if (rc) return rc;
