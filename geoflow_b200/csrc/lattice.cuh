@@ -128,8 +128,13 @@ struct FastDiv {
     f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.l) - (uint64_t)d)) / (uint64_t)d + 1);
     return f;
   }
-  __device__ __forceinline__ int div(int n) const {
-    return (int)((__umulhi((uint32_t)n, m) + (uint32_t)n) >> l);
+  __host__ __device__ __forceinline__ int div(int n) const {
+#ifdef __CUDA_ARCH__
+    const uint32_t hi = __umulhi((uint32_t)n, m);
+#else
+    const uint32_t hi = (uint32_t)(((uint64_t)(uint32_t)n * m) >> 32);
+#endif
+    return (int)((hi + (uint32_t)n) >> l);
   }
 };
 
@@ -141,7 +146,7 @@ struct FastDiv {
 // wrapping to (ne - 1, P) and coming second when periodic and q = 0, and
 // only one of them on a non-periodic boundary.  (A branch-free form with
 // selects executed 5-10 % more instructions per point on B200.)
-__device__ __forceinline__ int lattice_offsets_qr(int q, int r, int P, int ne, int per, int es,
+__host__ __device__ __forceinline__ int lattice_offsets_qr(int q, int r, int P, int ne, int per, int es,
                                                   int ls, int &o0, int &o1) {
   if (r != 0) {
     o0 = o1 = q * es + r * ls;
@@ -177,7 +182,7 @@ __device__ __forceinline__ int lattice_offsets(int g, int ne, int per, int es, i
 // when no periodic direction has a single element.
 struct BoxCopies {
   int ox0, ox1, oy0, oy1, oz0, oz1, nx, ny, nz;
-  __device__ __forceinline__ int count() const { return nx * ny * nz; }
+  __host__ __device__ __forceinline__ int count() const { return nx * ny * nz; }
   template <class F>
   __device__ __forceinline__ void each(F f) const {
 #pragma unroll
@@ -223,7 +228,7 @@ struct BoxWalk {
     w.fP = FastDiv::make(w.P);
     return w;
   }
-  __device__ __forceinline__ BoxCopies copies(int c) const {
+  __host__ __device__ __forceinline__ BoxCopies copies(int c) const {
     const int row = f0.div(c), g0 = c - row * M[0];
     const int g2 = f1.div(row), g1 = row - g2 * M[1];
     BoxCopies k;
