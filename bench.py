@@ -189,7 +189,7 @@ def time_solves(ctx, prob, H, b, traits, steps, warmup):
         e.record()
         torch.cuda.synchronize()
         times.append(s.elapsed_time(e) / 1e3)
-        iters.append(cg.get_iteration_count())
+        iters.append(cg.iter_)
     return times, iters, rc, x
 
 

@@ -3,9 +3,8 @@
 Compiles every CUDA translation unit under geoflow_b200/csrc with nvcc for
 sm_100a, in parallel, and links them into geoflow_b200/libgfgpu.so (in the
 source tree, so it travels with the repository).  `build_oracle()` builds
-the C oracle (oracle/_build) and, when the reference sources are present,
-the reference's own GLLBasis/GMTK subset (oracle/_ref); those are test
-infrastructure only.
+the C oracle (oracle/_build) and, given a reference checkout, the
+reference's own code (oracle/_ref); those are test infrastructure only.
 """
 from __future__ import annotations
 
@@ -77,20 +76,28 @@ def build_lib(force: bool = False, jobs: int | None = None, verbose: bool = Fals
 
 
 def build_oracle(reference: str | None = None) -> None:
-    """Build the C oracle and, if the reference sources exist, oracle/_ref."""
+    """Build the C oracle and, given a reference checkout, oracle/_ref.
+
+    `reference` (or the GEOFLOW_REFERENCE environment variable) is the root of
+    a NOAA-GSL/GeoFLOW checkout; without one only the C oracle is built.
+    """
     od = ROOT / "oracle"
     r = subprocess.run(["make", "-C", str(od)], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stderr[-4000:])
-    ref = reference or os.environ.get("GEOFLOW_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src", "cdg")):
-        r = subprocess.run(["make", "-C", str(od), "ref", f"REF={ref}"], capture_output=True,
-                           text=True)
-        if r.returncode != 0:
-            raise RuntimeError("oracle/_ref build failed:\n" + r.stderr[-4000:])
+    ref = reference or os.environ.get("GEOFLOW_REFERENCE")
+    if not ref:
+        return
+    if not os.path.isdir(os.path.join(ref, "src", "cdg")):
+        raise RuntimeError(f"no reference sources under {ref}")
+    r = subprocess.run(["make", "-C", str(od), "-j", "4", "ref", f"REF={ref}"],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle/_ref build failed:\n" + r.stderr[-4000:])
 
 
 if __name__ == "__main__":
     build_lib(force="--force" in sys.argv, verbose=True)
-    build_oracle()
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    build_oracle(args[0] if args else None)
     print(LIB)

@@ -402,7 +402,10 @@ class GCG:
         return rc
 
     def get_iteration_count(self) -> int:
-        return self.iter_
+        """As the reference's GCG::get_iteration_count (solvers/gcg.hpp:75):
+        the number of iterations taken plus one.  `iter_` holds the number
+        of iterations."""
+        return self.iter_ + 1
 
     def get_residuals(self):
         return self.residuals_[: self.iter_]

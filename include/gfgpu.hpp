@@ -181,7 +181,9 @@ class CG {
   CG(const gf_cg_traits &tr, Problem &p) : tr_(tr), p_(p) {}
   int solve(Helmholtz &A, const double *b, double *x) { return run(A, b, nullptr, x); }
   int solve(Helmholtz &A, const double *b, const double *xb, double *x) { return run(A, b, xb, x); }
-  int get_iteration_count() const { return iters_; }
+  // As GCG::get_iteration_count (solvers/gcg.hpp:75): iterations taken + 1.
+  int get_iteration_count() const { return iters_ + 1; }
+  int iterations() const { return iters_; }
   double get_resid() const { return rnorm_; }
   const std::vector<double> &get_residuals() const { return res_; }
 

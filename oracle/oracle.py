@@ -320,3 +320,126 @@ def constrain2sphere(xyz, v):
     va = (P_double * 3)(*[dp(a) for a in v])
     load().gfo_constrain2sphere(c_size_t(len(v[0])), xa, va)
     return v
+
+
+# ---- the reference's own path code (oracle/_ref/libgfref{2,3}.so) ----
+REFPATH = {2: HERE / "_ref" / "libgfref2.so", 3: HERE / "_ref" / "libgfref3.so"}
+_refpath = {}
+P_void = C.c_void_p
+
+
+def load_refpath(dim):
+    """The reference's GGridBox/GGFX/GHelmholtz/GAdvect/GCG/GBurgers compiled
+    from its sources for GDIM = dim (oracle/ref/ref_path.cpp), or None."""
+    if dim not in _refpath:
+        if not REFPATH[dim].exists():
+            return None
+        lib = C.CDLL(str(REFPATH[dim]))
+        lib.gfr_box_create.restype = P_void
+        lib.gfr_box_create.argtypes = [C.POINTER(C.c_int), C.c_int, P_double, P_double, C.c_int,
+                                       C.c_double]
+        lib.gfr_ndof.restype = c_size_t
+        lib.gfr_ndof.argtypes = [P_void]
+        lib.gfr_path_error.restype = C.c_char_p
+        for f in ("gfr_coords", "gfr_mass", "gfr_mask", "gfr_imult"):
+            getattr(lib, f).argtypes = [P_void, P_double]
+        lib.gfr_dss.argtypes = [P_void, P_double, C.c_int]
+        lib.gfr_helmholtz.argtypes = [P_void, P_double, P_double, P_double, c_size_t, P_double]
+        lib.gfr_advect.argtypes = [P_void, P_double, P_double, P_double]
+        lib.gfr_cg_solve.argtypes = [P_void, C.c_double, P_double, P_double, P_double, P_double,
+                                     C.c_int, C.c_double, C.c_int, P_double,
+                                     C.POINTER(C.c_int), P_double]
+        lib.gfr_burgers_run.argtypes = [P_void, C.c_int, C.c_double, C.c_int, C.c_int,
+                                        C.c_double, C.c_int, P_double]
+        lib.gfr_box_destroy.argtypes = [P_void]
+        assert lib.gfr_path_dim() == dim
+        _refpath[dim] = lib
+    return _refpath[dim]
+
+
+class RefBox:
+    """A box grid run by the reference's own code (see load_refpath); the
+    same layout as OracleBox (element-major, x fastest)."""
+
+    def __init__(self, dim, ne, p, periodic=None, x0=None, length=None, tol_frac=0.001):
+        self.lib = lib = load_refpath(dim)
+        if lib is None:
+            raise FileNotFoundError(f"{REFPATH[dim]} not built")
+        self.dim, self.p = dim, p
+        per = list(periodic if periodic is not None else [0] * dim)
+        mask = sum(1 << d for d in range(dim) if per[d])
+        ne3 = (C.c_int * 3)(*(list(ne)[:dim] + [1] * (3 - dim)))
+        x0 = np.array(list(x0 if x0 is not None else [0.0] * dim) + [0.0] * (3 - dim))
+        ln = np.array(list(length if length is not None else [1.0] * dim) + [1.0] * (3 - dim))
+        self.h = lib.gfr_box_create(ne3, p, dp(x0), dp(ln), mask, tol_frac)
+        if not self.h:
+            raise RuntimeError(lib.gfr_path_error().decode())
+        self.N = int(lib.gfr_ndof(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.gfr_box_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _vec(self, fn, nvec=1):
+        a = np.zeros(self.N * nvec)
+        getattr(self.lib, fn)(self.h, dp(a))
+        return a
+
+    def coords(self):
+        return self._vec("gfr_coords", self.dim).reshape(self.dim, self.N)
+
+    def mass(self):
+        return self._vec("gfr_mass")
+
+    def mask(self):
+        return self._vec("gfr_mask")
+
+    def imult(self):
+        return self._vec("gfr_imult")
+
+    def dss(self, u, op):
+        rc = self.lib.gfr_dss(self.h, dp(u), op)
+        assert rc == 0
+        return u
+
+    def helmholtz(self, u, p=1.0, p_vec=None, q_vec=None):
+        pv = np.ascontiguousarray(p_vec if p_vec is not None else np.array([p], dtype=np.float64))
+        out = np.zeros(self.N)
+        self.lib.gfr_helmholtz(self.h, dp(u), dp(out), dp(pv), c_size_t(len(pv)), dp(q_vec))
+        return out
+
+    def advect(self, u, c):
+        cc = np.ascontiguousarray(np.concatenate(c))
+        out = np.zeros(self.N)
+        self.lib.gfr_advect(self.h, dp(u), dp(cc), dp(out))
+        return out
+
+    def cg_solve(self, b, x, p=1.0, q_vec=None, xb=None, maxit=512, normtype=NORM_INF,
+                 tol=1e-6, dinv=None):
+        """GCG::solve(A, b, xb, x); returns (rc, iterations, residuals).  The
+        reference's get_iteration_count() is iterations + 1 (gcg.hpp:75)."""
+        q = q_vec if q_vec is not None else np.ones(self.N)
+        xbv = xb if xb is not None else np.zeros(self.N)
+        it = C.c_int(0)
+        res = np.zeros(max(1, maxit))
+        rc = self.lib.gfr_cg_solve(self.h, p, dp(q), dp(b), dp(xbv), dp(x), maxit, tol,
+                                   normtype, dp(dinv), C.byref(it), dp(res))
+        iters = it.value - 1
+        return rc, iters, res[:iters]
+
+    def burgers_run(self, kind, nu, order, ssp, state, dt, nsteps):
+        """GBurgers stepped by its GExRKStepper; state: list of component
+        arrays (kind 0: [u, c_1..c_dim]; 1: dim velocities; 2: [u]); the
+        evolved components are updated in place."""
+        st = np.ascontiguousarray(np.concatenate(state))
+        rc = self.lib.gfr_burgers_run(self.h, kind, nu, order, 1 if ssp else 0, dt, nsteps,
+                                      dp(st))
+        if rc != 0:
+            raise RuntimeError(self.lib.gfr_path_error().decode())
+        for k, a in enumerate(state):
+            a[:] = st[k * self.N:(k + 1) * self.N]
+        return state

@@ -44,3 +44,12 @@ def ctx():
     from geoflow_b200 import Context
     # problems keep a reference to their context; it is released after them
     return Context(0)
+
+
+@pytest.fixture(scope="session")
+def refpath():
+    """Inputs and outputs of the reference's own grid, GGFX, GHelmholtz,
+    GAdvect, GCG and GBurgers/GExRKStepper code
+    (tests/golden/make_path_golden.py)."""
+    import numpy as np
+    return np.load(ROOT / "tests" / "golden" / "ref_path.npz")

@@ -65,7 +65,7 @@ int main() {
     vol += mass[i];
   }
   const double err = num / vol;
-  std::printf("cdg_cg: rc=%d iterations=%d err=%.3e\n", rc, cg.get_iteration_count(), err);
+  std::printf("cdg_cg: rc=%d iterations=%d err=%.3e\n", rc, cg.iterations(), err);
   if (rc != CG::GCGERR_NONE || !(err < 1e-12)) return 1;
 
   // GGFX Smooth of a continuous field leaves it bit-identical

@@ -201,7 +201,7 @@ def test_cdg_cg_poisson_on_gpu(ctx, structured):
     # the oracle's restatement stops after the same number of iterations
     xo = np.zeros(g.ndof())
     rc_o, it_o, res_o = o.cg_solve(b, xo, xb=ub, maxit=256, tol=1e-7)
-    assert abs(cg.get_iteration_count() - it_o) <= 1
+    assert abs(cg.iter_ - it_o) <= 1
     # CG amplifies rounding differences between iterate sequences, so the
     # 1e-10 solution parity is checked with both solves run to 1e-13
     xo = np.zeros(g.ndof())
@@ -229,7 +229,7 @@ def test_cg_helmholtz_3d_matches_oracle(ctx, precond, structured):
     x = prob.zeros()
     rc = cg.solve(H, dev(b), dev(np.zeros(g.ndof())), x)
     assert rc == 0 and rc_o == 0
-    assert abs(cg.get_iteration_count() - it_o) <= 2
+    assert abs(cg.iter_ - it_o) <= 2
     assert relerr(host(x), xo) < 1e-10
 
 
@@ -258,7 +258,7 @@ def test_cg_mixed_precision_reaches_fp64_solution(ctx, structured, inner):
     # reliable updates never restart the FP32 Krylov run: about the FP64
     # count; restarts rebuild the Krylov space once per refinement sweep
     bound = 1.5 if inner == 0.0 else 3.0
-    assert cgm.get_iteration_count() <= bound * cg64.get_iteration_count() + 32
+    assert cgm.iter_ <= bound * cg64.iter_ + 32
 
 
 @pytest.mark.parametrize("degree", [0, 3, 8])
@@ -283,7 +283,7 @@ def test_cg_chebyshev_preconditioned_reaches_fp64_solution(ctx, structured, p, d
     assert cgc.solve(H, dev(b), dev(0 * b), xc) == 0
     assert relerr(host(xc), host(x64)) < 1e-9
     if degree >= 3:
-        assert cgc.get_iteration_count() < cg64.get_iteration_count()
+        assert cgc.iter_ < cg64.iter_
 
 
 def test_cg_chebyshev_rejects_bad_degree(ctx):
@@ -351,7 +351,7 @@ def test_cg_norm_types_periodic_unmasked(ctx, structured, normtype):
     x = prob.zeros()
     rc = cg.solve(H, dev(b), x)
     assert rc == rc_o == 0
-    assert abs(cg.get_iteration_count() - it_o) <= 1
+    assert abs(cg.iter_ - it_o) <= 1
     assert relerr(host(x), xo) < 1e-9
 
 

@@ -60,9 +60,9 @@ def test_pmg_reaches_fp64_solution(ctx, dim, ne, p, per, m):
     cgm = GCG(CGTraits(precond=A.GF_PRECOND_PMG, poly_degree=m, **COMMON), prob)
     assert cgm.solve(H, dev(b), dev(0 * b), xm) == 0
     assert relerr(host(xm), host(xj)) < 1e-9
-    assert cgm.get_iteration_count() <= 40
+    assert cgm.iter_ <= 40
     if g.nelems * p ** dim >= 512:
-        assert cgm.get_iteration_count() < cgj.get_iteration_count()
+        assert cgm.iter_ < cgj.iter_
 
 
 @pytest.mark.parametrize("per", [[1, 0, 0], [0, 0, 0]])
@@ -81,7 +81,7 @@ def test_pmg_long_lattice_rows(ctx, per):
     cgm = GCG(CGTraits(precond=A.GF_PRECOND_PMG, **COMMON), prob)
     assert cgm.solve(H, dev(b), dev(0 * b), xm) == 0
     assert relerr(host(xm), host(xj)) < 1e-9
-    assert cgm.get_iteration_count() <= 30
+    assert cgm.iter_ <= 30
 
 
 def test_pmg_iterations_independent_of_element_count(ctx):
@@ -95,7 +95,7 @@ def test_pmg_iterations_independent_of_element_count(ctx):
         x = prob.zeros()
         cg = GCG(CGTraits(precond=A.GF_PRECOND_PMG, **COMMON), prob)
         assert cg.solve(H, dev(b), dev(0 * b), x) == 0
-        its.append(cg.get_iteration_count())
+        its.append(cg.iter_)
     assert max(its) <= min(its) + 6, its
 
 
@@ -134,7 +134,7 @@ def test_pmg_residual_history_is_recorded(ctx):
     x = prob.zeros()
     assert cg.solve(H, b, 0 * b, x) == 0
     res = cg.get_residuals()
-    assert len(res) == cg.get_iteration_count() and res[-1] == cg.rnorm_
+    assert len(res) == cg.iter_ and res[-1] == cg.rnorm_
     assert res[-1] < 1e-6 * res[0] and np.all(res > 0)
 
 
