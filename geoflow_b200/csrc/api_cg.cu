@@ -454,8 +454,13 @@ __global__ void __launch_bounds__(RED_THREADS)
         scal[S_RTOL] = scal[S_INNER] > 0.0 ? fmax(scal[S_INNER] * rnorm, rtol) : rtol;
         scal[S_RNORM] = 10.0 * scal[S_RTOL];
         scal[S_ITER] = 0.0;
-        scal[S_FLAG] = 0.0;
-        scal[S_DONE] = (scal[S_MAXIT] <= 0.0 || !(10.0 * rtol > rtol)) ? 1.0 : 0.0;
+        // A non-finite right-hand side or initial residual stops the solve
+        // before its first iteration and is reported as GF_ERR_NONFINITE
+        // (the reference's loop test rnorm > rtol is false for NaN, so it
+        // would return GCGERR_NONE without iterating).
+        const bool bad = !isfinite(bnorm) || !isfinite(rnorm) || !isfinite(rho_t);
+        scal[S_FLAG] = bad ? 1.0 : 0.0;
+        scal[S_DONE] = (scal[S_MAXIT] <= 0.0 || !(10.0 * rtol > rtol) || bad) ? 1.0 : 0.0;
       }
       *counter = 0;
     }
@@ -1813,7 +1818,8 @@ struct MGHier {
   cudaStream_t cs = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  const void *gkey[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // buffers the recorded loop reads, and the FP32 apply kernel it launches
+  const void *gkey[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   uint64_t glaunches = 0;  // launches per iteration
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -2382,8 +2388,8 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
   // k_while_more, which ends the loop once `done` is set (convergence,
   // maxit or breakdown) -- no host round trip per iteration and no
   // iterations queued past convergence.
-  const void *gk[7] = {xL, rL, w, qL, qE, bL, hist};
-  if (!(H->exec && std::equal(gk, gk + 7, H->gkey))) {
+  const void *gk[8] = {xL, rL, w, qL, qE, bL, hist, (const void *)(intptr_t)g_fp32_apply_mode};
+  if (!(H->exec && std::equal(gk, gk + 8, H->gkey))) {
     H->drop_graph();
     if (!H->cs) GF_CUDA(ctx, cudaStreamCreateWithFlags(&H->cs, cudaStreamNonBlocking));
     const uint64_t n0 = level_launches();
@@ -2417,7 +2423,7 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
       H->drop_graph();
       return gf_fail(ctx, GF_ERR_CUDA, "CG loop capture failed: %s", cudaGetErrorString(e));
     }
-    std::copy(gk, gk + 7, H->gkey);
+    std::copy(gk, gk + 8, H->gkey);
   }
   GF_CUDA(ctx, cudaGraphLaunch(H->exec, st));
   GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h, scal, sizeof(double) * S_COUNT,

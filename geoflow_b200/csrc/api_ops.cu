@@ -9,6 +9,17 @@
 
 using namespace gfk;
 
+namespace gfk {
+int g_fp32_apply_mode = GF_FP32_APPLY_FMA;
+}
+
+extern "C" int gf_set_fp32_apply(int mode) {
+  if (mode != GF_FP32_APPLY_FMA && mode != GF_FP32_APPLY_TF32) return GF_ERR_ARG;
+  const int prev = g_fp32_apply_mode;
+  g_fp32_apply_mode = mode;
+  return prev;
+}
+
 // ---------------------------------------------------------------------
 // Helmholtz
 // ---------------------------------------------------------------------

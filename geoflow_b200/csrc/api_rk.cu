@@ -22,6 +22,9 @@ using namespace gfk;
 
 namespace gfrk {
 
+// slot of the problem's scalar block holding the RK non-finite flag
+constexpr int RK_FLAG_SLOT = 62;
+
 void butcher(int order, double *alpha, double beta[4][4], double *c) {
   std::memset(beta, 0, sizeof(double) * 16);
   for (int i = 0; i < 4; i++) alpha[i] = c[i] = 0.0;
@@ -69,6 +72,23 @@ __global__ void k_stage_sum(int64_t n, const T *__restrict__ uin, int nk, const 
     v += s;
     y[i] = v;
   }
+}
+
+// flag[0] = 1 when any of the nstate fields holds a non-finite value
+// (GBurgers::step_impl asserts isfinite on the evolved state after every
+// step, gburgers.ipp:325-331).  Only a bad value writes the flag.
+template <typename T>
+__global__ void k_nonfinite(int64_t n, int nstate, const T *__restrict__ u0,
+                            const T *__restrict__ u1, const T *__restrict__ u2,
+                            double *__restrict__ flag) {
+  bool bad = false;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    bad |= !isfinite(u0[i]);
+    if (nstate > 1) bad |= !isfinite(u1[i]);
+    if (nstate > 2) bad |= !isfinite(u2[i]);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) flag[0] = 1.0;
 }
 
 template <typename T>
@@ -359,6 +379,26 @@ int advance(gf_problem *prob, const gf_rk_traits *tr, void *const *u, const void
     if (rc) return gf_fail(ctx, rc, "RK step failed");
   }
   GF_CHECK_LAUNCH(ctx);
+  // The reference asserts a finite state after every step; a NaN or Inf
+  // stays in the state once made, so one check of the result after the
+  // last step finds the same failures.  It reads the state once and waits
+  // for the stream; inside a stream capture (a recorded step graph) it is
+  // skipped, since the capture cannot wait.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  GF_CUDA(ctx, cudaStreamIsCapturing(S.st, &cs));
+  if (nsteps > 0 && cs == cudaStreamCaptureStatusNone) {
+    double *flag = prob->scal_d + RK_FLAG_SLOT;
+    GF_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(double), S.st));
+    prob->launches++;
+    k_nonfinite<T><<<grid_for(S.n, 256, ctx->sm_count * 8), 256, 0, S.st>>>(
+        S.n, tr->nstate, uu[0], uu[tr->nstate > 1 ? 1 : 0], uu[tr->nstate > 2 ? 2 : 0], flag);
+    GF_CHECK_LAUNCH(ctx);
+    GF_CUDA(ctx, cudaMemcpyAsync(prob->scal_h + RK_FLAG_SLOT, flag, sizeof(double),
+                                 cudaMemcpyDeviceToHost, S.st));
+    GF_CUDA(ctx, cudaStreamSynchronize(S.st));
+    if (prob->scal_h[RK_FLAG_SLOT] != 0.0)
+      return gf_fail(ctx, GF_ERR_NONFINITE, "solution not finite after %d RK steps", nsteps);
+  }
   return GF_OK;
 }
 

@@ -8,9 +8,13 @@
 #include "k_def.cuh"
 #include "k_dudt.cuh"
 #include "k_helm_k1.cuh"
+#include "k_helm_tf32.cuh"
 #include "k_tensor.cuh"
 
 namespace gfk {
+
+// Library-wide choice of the FP32 3-d affine apply at p = 7 (gf_set_fp32_apply).
+extern int g_fp32_apply_mode;
 
 // Raises a kernel's dynamic shared-memory limit once per kernel (several
 // kernels share one function type, so the record is keyed by address).
@@ -74,6 +78,19 @@ struct HelmLaunch {
       }
       const Geom<T> g = geom_of<T>(prob);
       constexpr int P = Pad<N>::P;
+      if constexpr (std::is_same<T, float>::value && N == 8) {
+        if (prob->dim == 3 && g.egeom && !pvec && g_fp32_apply_mode == GF_FP32_APPLY_TF32) {
+          // affine elements, scalar p, p = 7: the K1 contractions as 3xTF32
+          // tensor-core products (k_helm_tf32.cuh)
+          constexpr int EPB = 4;
+          const Tf32Basis TB = make_tf32basis(prob);
+          const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
+          prob->launches++;
+          k_helm3d_tf32<EPB, LD, TO><<<grid, dim3(64, EPB), 0, st>>>(TB, g.egeom, prob->ne, p, q,
+                                                                    qvec, use_mass, ld, uo, stop);
+          return GF_OK;
+        }
+      }
       if (prob->dim == 3 && g.egeom && !pvec) {
         // affine elements, scalar p: one K1 contraction per direction
         constexpr int EPB = epb_k1<N>();

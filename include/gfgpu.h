@@ -173,6 +173,16 @@ int gf_problem_sizes(gf_problem_t prob, int64_t *nlocal, int64_t *nclass);
  * (instrumentation, in the spirit of the reference's tracer ranges). */
 int gf_problem_stats(gf_problem_t prob, int64_t *kernel_launches);
 
+/* ---- library options ---- */
+/* The FP32 3-d apply on affine elements at p = 7 (gf_helmholtz_apply and
+ * the FP32 applies inside the CG solvers): GF_FP32_APPLY_FMA contracts the
+ * lines with packed FP32x2 FMAs; GF_FP32_APPLY_TF32 as 3xTF32 tensor-core
+ * products (mma.sync m16n8k8: TF32 head and tail of each operand, FP32
+ * accumulation; FP32-level accuracy).  Process-wide; returns the previous
+ * mode, or GF_ERR_ARG for an unknown one.  No reference counterpart. */
+enum { GF_FP32_APPLY_FMA = 0, GF_FP32_APPLY_TF32 = 1 };
+int gf_set_fp32_apply(int mode);
+
 /* ---- operators (device pointers) ---- */
 /* GHelmholtz::opVec_prod (sem/ghelmholtz.ipp:77-93, reg_prod 309-378):
  * uo = p L u + q M u with L the weak Laplacian sum_k Dk^T (Gk M) Dk u.
@@ -277,7 +287,11 @@ typedef struct {
 } gf_rk_traits;
 /* Advances u[nstate] (device, dtype) in place by nsteps steps of size dt,
  * with the DSS Smooth calls where GExRKStepper::step_b / step_ssp* place
- * them.  c[dim] are prescribed velocities for GF_EQN_ADVECT (else NULL). */
+ * them.  c[dim] are prescribed velocities for GF_EQN_ADVECT (else NULL).
+ * Returns GF_ERR_NONFINITE when the state holds a NaN or Inf after the last
+ * step (GBurgers::step_impl asserts a finite state, gburgers.ipp:325-331);
+ * that check waits for the stream, and is skipped while the stream is
+ * being captured into a graph. */
 int gf_rk_advance(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
                   void *const *u, const void *const *c, double t0, double dt, int nsteps);
 /* Host-buffer variant: copies u and c in, advances, copies u out. */

@@ -16,6 +16,21 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* The oracle is serial.  Built with -fopenmp (libgforacle_omp.so, the
+ * bench's all-core CPU baseline only) the element, class and node loops
+ * below run on every host core; dot products and norms then sum in thread
+ * order, so that build is not bit-identical to the serial checker. */
+#if defined(_OPENMP)
+#define GFO_PRAGMA(x) _Pragma(#x)
+#define GFO_PAR GFO_PRAGMA(omp parallel for schedule(static))
+#define GFO_PAR_SUM(v) GFO_PRAGMA(omp parallel for schedule(static) reduction(+ : v))
+#define GFO_PAR_MAX(v) GFO_PRAGMA(omp parallel for schedule(static) reduction(max : v))
+#else
+#define GFO_PAR
+#define GFO_PAR_SUM(v)
+#define GFO_PAR_MAX(v)
+#endif
+
 /* ===================================================================== */
 /* GLL basis: GLLBasis<long double,double> (sem/gllbasis.ipp)            */
 /* ===================================================================== */
@@ -148,6 +163,7 @@ int gfo_gll(int p, double *xi_out, double *w_out, double *D_out) {
 /* ===================================================================== */
 void gfo_dmxm(double *C, const double *A, size_t nai, const double *B,
               size_t nbi, size_t nbj) {
+  GFO_PAR
   for (size_t j = 0; j < nbj; j++)
     for (size_t i = 0; i < nai; i++) {
       double s = A[i] * B[j * nbi];
@@ -180,6 +196,7 @@ void gfo_I2_X_D1(const double *D1, const double *u, size_t N1, size_t N2,
 void gfo_D2_X_I1(const double *D2T, const double *u, size_t N1, size_t N2,
                  size_t Ne, double *y) {
   size_t Nu = N1 * N2;
+  GFO_PAR
   for (size_t e = 0; e < Ne; e++) gfo_dmxm(y + e * Nu, u + e * Nu, N1, D2T, N2, N2);
 }
 
@@ -193,6 +210,7 @@ void gfo_I3_X_I2_X_D1(const double *D1, const double *u, size_t N1,
 void gfo_I3_X_D2_X_I1(const double *D2T, const double *u, size_t N1,
                       size_t N2, size_t N3, size_t Ne, double *y) {
   size_t NXY = N1 * N2, Nu = N1 * N2 * N3;
+  GFO_PAR
   for (size_t e = 0; e < Ne; e++)
     for (size_t k = 0; k < N3; k++)
       gfo_dmxm(y + k * NXY + e * Nu, u + k * NXY + e * Nu, N1, D2T, N2, N2);
@@ -202,6 +220,7 @@ void gfo_I3_X_D2_X_I1(const double *D2T, const double *u, size_t N1,
 void gfo_D3_X_I2_X_I1(const double *D3T, const double *u, size_t N1,
                       size_t N2, size_t N3, size_t Ne, double *y) {
   size_t NXY = N1 * N2, Nu = NXY * N3;
+  GFO_PAR
   for (size_t e = 0; e < Ne; e++) gfo_dmxm(y + e * Nu, u + e * Nu, NXY, D3T, N3, N3);
 }
 
@@ -477,6 +496,7 @@ long gfo_ggfx_init(size_t N, int dim, const double *x, const double *y,
  * written. */
 void gfo_ggfx_doop(double *u, size_t nclass, const int32_t *class_ptr,
                    const int32_t *members, int op) {
+  GFO_PAR
   for (size_t c = 0; c < nclass; c++) {
     int32_t b = class_ptr[c], e = class_ptr[c + 1];
     double acc;
@@ -580,11 +600,13 @@ void gfo_grefdiv(const gfo_grid *g, const double *const *u, int dotrans,
                  double *divu) {
   size_t nd = g->Ne * elem_nodes(g);
   double *etmp = (double *)malloc(nd * sizeof(double));
+  GFO_PAR
   for (size_t i = 0; i < nd; i++) divu[i] = 0.0;
   for (int k = 0; k < g->dim; k++) {
     if (!u[k]) continue;
     int src = (g->dim == 3 && k == 2) ? 1 : k;
     apply_dir(g, g->D[src], g->n[src], u[k], k + 1, dotrans, etmp);
+    GFO_PAR
     for (size_t i = 0; i < nd; i++) divu[i] += etmp[i];
   }
   free(etmp);
@@ -609,6 +631,7 @@ void gfo_helmholtz(const gfo_grid *g, const double *u, double p_scalar,
     gfo_grefderiv(g, u, k + 1, 0, gdu[k]);
   }
   for (int k = 0; k < g->dim; k++) {
+    GFO_PAR
     for (size_t i = 0; i < nd; i++) {
       double G = g->dXidX[k][i] * g->dXidX[k][i];
       gdu[k][i] *= G;
@@ -618,14 +641,18 @@ void gfo_helmholtz(const gfo_grid *g, const double *u, double p_scalar,
     }
   }
   gfo_grefdiv(g, (const double *const *)gdu, 1, uo);
-  if (!p_vec && p_scalar != 1.0)
+  if (!p_vec && p_scalar != 1.0) {
+    GFO_PAR
     for (size_t i = 0; i < nd; i++) uo[i] *= p_scalar;
-  if (q_vec)
+  }
+  if (q_vec) {
+    GFO_PAR
     for (size_t i = 0; i < nd; i++) {
       double t = g->mass[i] * u[i];
       t *= q_vec[i];
       uo[i] += t;
     }
+  }
   for (int k = 0; k < g->dim; k++) free(gdu[k]);
 }
 
@@ -970,6 +997,7 @@ void gfo_rk_advance(const gfo_burgers *b, int scheme, int nstate,
 static double cg_norm(const gfo_grid *g, int normtype, const double *x, size_t nd, double ivol) {
   if (normtype == GFO_NORM_INF) {
     double m = 0.0;
+    GFO_PAR_MAX(m)
     for (size_t i = 0; i < nd; i++) {
       double a = fabs(x[i]);
       m = m > a ? m : a;
@@ -980,6 +1008,7 @@ static double cg_norm(const gfo_grid *g, int normtype, const double *x, size_t n
   double r;
   if (normtype == GFO_NORM_EUC) {
     double s = 0.0;
+    GFO_PAR_SUM(s)
     for (size_t i = 0; i < nd; i++) s += x[i] * x[i];
     r = sqrt(s / (double)nd);
   } else if (normtype == GFO_NORM_L2) {
@@ -1034,18 +1063,26 @@ int gfo_cg_solve(const gfo_grid *g, double p_scalar, const double *q_vec,
   while (iret == GFO_CG_NONE && iter < tr->maxit && rnorm > rtol) {
     gfo_helmholtz(g, w, p_scalar, NULL, q_vec, q);
     gfo_ggfx_doop(q, nclass, class_ptr, members, GFO_SUM);
-    if (bbv) for (size_t i = 0; i < nd; i++) q[i] *= mask[i];
+    if (bbv) {
+      GFO_PAR
+      for (size_t i = 0; i < nd; i++) q[i] *= mask[i];
+    }
     double wq = 0.0;
+    GFO_PAR_SUM(wq)
     for (size_t i = 0; i < nd; i++) wq += w[i] * q[i] * imult[i];
     alpha = rho / wq;
-    for (size_t i = 0; i < nd; i++) x[i] = 1.0 * x[i] + alpha * w[i];
-    for (size_t i = 0; i < nd; i++) r[i] = 1.0 * r[i] + (-alpha) * q[i];
-    if (dinv) for (size_t i = 0; i < nd; i++) z[i] = dinv[i] * r[i];
-    else memcpy(z, r, nd * sizeof(double));
+    GFO_PAR
+    for (size_t i = 0; i < nd; i++) {
+      x[i] = 1.0 * x[i] + alpha * w[i];
+      r[i] = 1.0 * r[i] + (-alpha) * q[i];
+      z[i] = dinv ? dinv[i] * r[i] : r[i];
+    }
     rhom = rho;
     rho = 0.0;
+    GFO_PAR_SUM(rho)
     for (size_t i = 0; i < nd; i++) rho += r[i] * z[i] * imult[i];
     beta = rho / rhom;
+    GFO_PAR
     for (size_t i = 0; i < nd; i++) w[i] = beta * w[i] + 1.0 * z[i];
     rnorm = cg_norm(g, tr->normtype, r, nd, ivol);
     if (residuals) residuals[iter] = rnorm;

@@ -16,6 +16,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "libgforacle.so"
+# GFO_OPENMP=1 selects the OpenMP build of the same sources (every host
+# core; dot products sum in thread order): the bench's CPU baseline only.
+if os.environ.get("GFO_OPENMP") == "1":
+    LIB = HERE / "_build" / "libgforacle_omp.so"
 REFLIB = HERE / "_ref" / "libgfref.so"
 
 P_double = C.POINTER(C.c_double)

@@ -1,19 +1,21 @@
 """Generates tests/golden/gio_g2vtk.json from the reference's own GIO reader
 in Python (analysis/python/g2vtk, read_header at lines 158-195).
 
-Runs in the build container only (it loads the g2vtk script from the
-reference tree).  For a few small GIO files written by the oracle's
+Runs where a reference checkout is available (it loads the g2vtk script
+from the reference tree): pass the checkout's root as the first argument or
+in GEOFLOW_REFERENCE.  For a few small GIO files written by the oracle's
 restatement (oracle/gio_oracle.py) it records the file bytes (hex) and the
 header fields that g2vtk parses from them: version, dim, nelems, porder,
 gtype, cycle, time and `skip`, the byte where g2vtk starts the field data.
 g2vtk predates the multivar flag and the element keys at the end of the
 header (io/gio.ipp:489-496), so its `skip` is the offset of the multivar
 field; the test records that difference instead of hiding it.
-Usage: python tests/golden/make_gio_golden.py
+Usage: python tests/golden/make_gio_golden.py <reference checkout>
 """
 import importlib.machinery
 import importlib.util
 import json
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -24,7 +26,6 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT / "oracle"))
 import gio_oracle as GO  # noqa: E402
 
-G2VTK = Path("/root/reference/analysis/python/g2vtk")
 CASES = [  # (dim, nelems, p, float bytes, gtype, cycle, time)
     (3, 4, 2, 8, 0, 12, 0.375),
     (2, 6, 3, 8, 2, 7, 1.5),
@@ -33,7 +34,14 @@ CASES = [  # (dim, nelems, p, float bytes, gtype, cycle, time)
 
 
 def load_g2vtk():
-    loader = importlib.machinery.SourceFileLoader("g2vtk", str(G2VTK))
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GEOFLOW_REFERENCE")
+    if not ref:
+        raise SystemExit("usage: make_gio_golden.py <reference checkout> "
+                         "(or set GEOFLOW_REFERENCE)")
+    g2vtk = Path(ref) / "analysis" / "python" / "g2vtk"
+    if not g2vtk.exists():
+        raise SystemExit(f"{g2vtk} not found")
+    loader = importlib.machinery.SourceFileLoader("g2vtk", str(g2vtk))
     spec = importlib.util.spec_from_loader("g2vtk", loader)
     mod = importlib.util.module_from_spec(spec)
     loader.exec_module(mod)
