@@ -239,14 +239,19 @@ static int launch_def_dudt(gf_problem *prob, int eqn, int mode, T nu, const T *c
 
 template <typename T>
 int launch_dudt(gf_problem *prob, int eqn, int mode, T nu, const T *const *f, T *const *o,
-                cudaStream_t st) {
-  if (prob->geom >= GF_GEOM_DEFORMED) return launch_def_dudt<T>(prob, eqn, mode, nu, f, o, st);
-  return dispatch_n<DudtLaunch<T>::template F>(prob->n, prob, eqn, mode, nu, f, o, st);
+                cudaStream_t st, const gfk::RKEpi<T> *epi) {
+  if (prob->geom >= GF_GEOM_DEFORMED) {
+    if (mode == MODE_EULER) return GF_ERR_UNSUPPORTED;
+    return launch_def_dudt<T>(prob, eqn, mode, nu, f, o, st);
+  }
+  const RKEpi<T> none{};
+  return dispatch_n<DudtLaunch<T>::template F>(prob->n, prob, eqn, mode, nu, f, o, st,
+                                               epi ? *epi : none);
 }
 template int launch_dudt<double>(gf_problem *, int, int, double, const double *const *,
-                                 double *const *, cudaStream_t);
+                                 double *const *, cudaStream_t, const gfk::RKEpi<double> *);
 template int launch_dudt<float>(gf_problem *, int, int, float, const float *const *,
-                                float *const *, cudaStream_t);
+                                float *const *, cudaStream_t, const gfk::RKEpi<float> *);
 
 extern "C" int gf_advect_apply(gf_problem_t prob, int dtype, const void *p, int ncomp,
                                const void *const *c, void *po) {

@@ -118,6 +118,59 @@ int Stepper<T>::rhs(T *const *u, T *const *K) {
 }
 
 template <typename T>
+bool Stepper<T>::rhs_euler_smooth(T *const *u, T *const *x, T dt, T *const *uin, T a,
+                                  T *const *y, T b, T a2, T *const *y2, T b2, int *rc) {
+  // FP32 only: measured on B200 (64^3 p=5 SSP-RK3 Burgers), the fused
+  // epilogue takes an FP32 stage from 1.96 to 1.75 ms but an FP64 one from
+  // 3.28 to 3.59 ms (the FP64 RHS kernel, at 104-109 registers and 3 blocks
+  // per SM, absorbs the extra loads badly)
+  if (sizeof(T) != 4 || prob->dim != 3 || prob->geom >= GF_GEOM_DEFORMED) return false;
+  auto epi_for = [&](int k0, int nk) {
+    RKEpi<T> e{};
+    for (int j = 0; j < nk; j++) {
+      e.uin[j] = uin[k0 + j];
+      e.y[j] = y ? y[k0 + j] : nullptr;
+      e.y2[j] = y2 ? y2[k0 + j] : nullptr;
+    }
+    e.dt = dt;
+    e.a = a;
+    e.b = b;
+    e.a2 = a2;
+    e.b2 = b2;
+    e.uin_is_u = 1;
+    for (int j = 0; j < nk; j++)
+      if (uin[k0 + j] != u[k0 + j]) e.uin_is_u = 0;
+    return e;
+  };
+  const T *f[4] = {nullptr, nullptr, nullptr, nullptr};
+  T *o[3] = {nullptr, nullptr, nullptr};
+  if (eqn == GF_EQN_HEAT) {
+    for (int k = 0; k < nstate; k++) {
+      const T *fk[4] = {u[k], nullptr, nullptr, nullptr};
+      T *ok[3] = {x[k], nullptr, nullptr};
+      const RKEpi<T> e = epi_for(k, 1);
+      if ((*rc = launch_dudt<T>(prob, eqn, MODE_EULER, nu, fk, ok, st, &e))) return true;
+    }
+  } else {
+    if (eqn == GF_EQN_ADVECT) {
+      f[0] = u[0];
+      for (int k = 0; k < gf_nvel(prob); k++) f[1 + k] = c[k];
+      o[0] = x[0];
+    } else {
+      for (int k = 0; k < gf_nvel(prob); k++) {
+        f[k] = u[k];
+        o[k] = x[k];
+      }
+    }
+    const RKEpi<T> e = epi_for(0, nstate);
+    if ((*rc = launch_dudt<T>(prob, eqn, MODE_EULER, nu, f, o, st, &e))) return true;
+  }
+  smooth_n(x);
+  *rc = GF_OK;
+  return true;
+}
+
+template <typename T>
 void Stepper<T>::smooth(T *v) {
   launch_dss<T>(prob, GF_DSS_SMOOTH, v, st);
 }
@@ -305,37 +358,47 @@ int Stepper<T>::step(T *const *uin, T *const *uout, T dt, T *const *tape) {
   return step_ssp(uin, uout, dt);
 }
 
+// One SSP substep: x = Smooth(update(dudt(u))), as the RHS call followed by
+// euler_smooth_n, or in two passes (the RHS kernel writing the update,
+// then the Smooth) where the RHS kernel has the fused epilogue.
+template <typename T>
+static int ssp_substep(Stepper<T> &S, T *const *u, T *const *x, T dt, T *const *uin, T a,
+                       T *const *y, T b, T a2, T *const *y2, T b2) {
+  int rc = GF_OK;
+  if (S.rhs_euler_smooth(u, x, dt, uin, a, y, b, a2, y2, b2, &rc)) return rc;
+  if ((rc = S.rhs(u, x))) return rc;
+  S.euler_smooth_n(x, dt, uin, a, y, b, a2, y2, b2);
+  return GF_OK;
+}
+
 template <typename T>
 int Stepper<T>::step_ssp(T *const *uin, T *const *uout, T dt) {
-  const unsigned g = grid_for(n, 256, prob->ctx->sm_count * 8);
   int rc;
   const T one = T(1);
   if (scheme == GF_SSP22) {
-    if ((rc = rhs(uin, K[0]))) return rc;
-    euler_smooth_n(K[0], dt, uin, one, nullptr, T(0), one, nullptr, T(0));
-    if ((rc = rhs(K[0], uout))) return rc;
-    euler_smooth_n(uout, dt, K[0], T(0.5), uin, T(0.5), one, nullptr, T(0));
-    return GF_OK;
+    if ((rc = ssp_substep<T>(*this, uin, K[0], dt, uin, one, nullptr, T(0), one, nullptr, T(0))))
+      return rc;
+    return ssp_substep<T>(*this, K[0], uout, dt, K[0], T(0.5), uin, T(0.5), one, nullptr, T(0));
   }
   if (scheme == GF_SSP33) {
-    if ((rc = rhs(uin, K[0]))) return rc;
-    euler_smooth_n(K[0], dt, uin, one, nullptr, T(0), one, nullptr, T(0));
-    if ((rc = rhs(K[0], K[1]))) return rc;
-    euler_smooth_n(K[1], dt, K[0], T(0.25), uin, T(0.75), one, nullptr, T(0));
-    if ((rc = rhs(K[1], uout))) return rc;
-    euler_smooth_n(uout, dt, K[1], T(2.0 / 3.0), uin, T(1.0 / 3.0), one, nullptr, T(0));
-    return GF_OK;
+    if ((rc = ssp_substep<T>(*this, uin, K[0], dt, uin, one, nullptr, T(0), one, nullptr, T(0))))
+      return rc;
+    if ((rc = ssp_substep<T>(*this, K[0], K[1], dt, K[0], T(0.25), uin, T(0.75), one, nullptr,
+                             T(0))))
+      return rc;
+    return ssp_substep<T>(*this, K[1], uout, dt, K[1], T(2.0 / 3.0), uin, T(1.0 / 3.0), one,
+                          nullptr, T(0));
   }
   if (scheme == GF_SSP34) {
-    if ((rc = rhs(uin, K[0]))) return rc;
-    euler_smooth_n(K[0], dt, uin, T(0.5), uin, T(0.5), one, nullptr, T(0));
-    if ((rc = rhs(K[0], K[1]))) return rc;
-    euler_smooth_n(K[1], dt, K[0], T(0.5), K[0], T(0.5), one, nullptr, T(0));
-    if ((rc = rhs(K[1], K[2]))) return rc;
-    euler_smooth_n(K[2], dt, K[1], T(1.0 / 6.0), K[1], T(1.0 / 6.0), one, uin, T(2.0 / 3.0));
-    if ((rc = rhs(K[2], uout))) return rc;
-    euler_smooth_n(uout, dt, K[2], T(0.5), K[2], T(0.5), one, nullptr, T(0));
-    return GF_OK;
+    if ((rc = ssp_substep<T>(*this, uin, K[0], dt, uin, T(0.5), uin, T(0.5), one, nullptr, T(0))))
+      return rc;
+    if ((rc = ssp_substep<T>(*this, K[0], K[1], dt, K[0], T(0.5), K[0], T(0.5), one, nullptr,
+                             T(0))))
+      return rc;
+    if ((rc = ssp_substep<T>(*this, K[1], K[2], dt, K[1], T(1.0 / 6.0), K[1], T(1.0 / 6.0), one,
+                             uin, T(2.0 / 3.0))))
+      return rc;
+    return ssp_substep<T>(*this, K[2], uout, dt, K[2], T(0.5), K[2], T(0.5), one, nullptr, T(0));
   }
   return GF_ERR_ARG;
 }

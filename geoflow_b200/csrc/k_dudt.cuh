@@ -10,11 +10,27 @@
 // shared by the advection and the diffusion terms.  Fields are staged in
 // shared memory and contracted line by line as in k_tensor.cuh.
 #pragma once
+#include "k_dss.cuh"
 #include "k_tensor.cuh"
 
 namespace gfk {
 
-enum { MODE_DUDT = 0, MODE_ADVECT = 1 };
+enum { MODE_DUDT = 0, MODE_ADVECT = 1, MODE_EULER = 2 };
+
+// MODE_EULER: the right-hand side K = dudt of each evolved component is
+// not stored; the kernel stores the SSP substep's update before its Smooth
+// instead, with the stage arithmetic of k_dss_rk_box_n (FUSE_EULER):
+//   x = dt K + 1 uin;  x = a x + b y (if y);  x = a2 x + b2 y2 (if y2)
+// (gexrk_stepper.ipp:533-780, 809-819), K rounded to T first, so the
+// following Smooth gives the same bits as the fused update-and-Smooth pass.
+template <typename T>
+struct RKEpi {
+  const T *uin[3];
+  const T *y[3];
+  const T *y2[3];
+  T dt, a, b, a2, b2;
+  int uin_is_u;  // uin[c] is the RHS input u[c]: read it from the staged copy
+};
 
 template <int N, int NF> constexpr int epb_dudt3() {
   return (160 / (N * N)) < 1 ? 1 : (160 / (N * N));
@@ -29,7 +45,7 @@ __global__ void __launch_bounds__(N *N *EPB)
     k_dudt3d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T nu,
              const T *__restrict__ f0, const T *__restrict__ f1, const T *__restrict__ f2,
              const T *__restrict__ f3, const T *__restrict__ imass, T *__restrict__ o0,
-             T *__restrict__ o1, T *__restrict__ o2) {
+             T *__restrict__ o1, T *__restrict__ o2, const RKEpi<T> epi) {
   constexpr int NF = EQN == GF_EQN_ADVECT ? 4 : (EQN == GF_EQN_BURGERS ? 3 : 1);
   constexpr int NC = EQN == GF_EQN_BURGERS ? 3 : 1;  // evolved components
   constexpr int P = Pad<N>::P, PLANE = N * P, VOL = N * PLANE, NN = N * N, NNN = N * N * N;
@@ -154,7 +170,18 @@ __global__ void __launch_bounds__(N *N *EPB)
           T L = (sdx[sidx] + sdy[sidx]) + d[k];
           if (nu != T(1)) L *= nu;
           T rhs = T(-1) * L + T(-1) * radv[k];
-          fout[c][node] = imass[node] * rhs;
+          const T K = imass[node] * rhs;
+          if (MODE == MODE_EULER) {
+            // component pointers by selection (no local-memory copy of epi)
+            const T *ui = c == 0 ? epi.uin[0] : (c == 1 ? epi.uin[1] : epi.uin[2]);
+            const T *yc = c == 0 ? epi.y[0] : (c == 1 ? epi.y[1] : epi.y[2]);
+            const T *y2c = c == 0 ? epi.y2[0] : (c == 1 ? epi.y2[1] : epi.y2[2]);
+            const T uv = epi.uin_is_u ? su[sidx] : ui[node];
+            fout[c][node] = rk_euler_point(K, epi.dt, uv, epi.a, yc, epi.b, epi.a2, y2c, epi.b2,
+                                           node);
+          } else {
+            fout[c][node] = K;
+          }
         }
       }
     }
@@ -168,7 +195,8 @@ __global__ void __launch_bounds__(N *N *EPB)
     k_dudt2d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T nu,
              const T *__restrict__ f0, const T *__restrict__ f1, const T *__restrict__ f2,
              const T *__restrict__ f3, const T *__restrict__ imass, T *__restrict__ o0,
-             T *__restrict__ o1, T *__restrict__ o2) {
+             T *__restrict__ o1, T *__restrict__ o2, const RKEpi<T> epi) {
+  (void)epi;  // the 2-d kernel has no fused update (MODE_EULER is 3-d only)
   constexpr int NF = EQN == GF_EQN_ADVECT ? 3 : (EQN == GF_EQN_BURGERS ? 2 : 1);
   constexpr int NC = EQN == GF_EQN_BURGERS ? 2 : 1;
   constexpr int P = Pad<N>::P, AREA = N * P, NN = N * N;

@@ -162,7 +162,7 @@ struct DerivLaunch {
 
 template <typename T, int N, int EQN, int MODE>
 inline void launch_dudt_kernel(gf_problem *prob, T nu, const T *const *f, T *const *o,
-                               const T *imass, cudaStream_t st) {
+                               const T *imass, cudaStream_t st, const RKEpi<T> &epi) {
   const Basis<T, N> B = make_basis<T, N>(prob);
   const Geom<T> g = geom_of<T>(prob);
   constexpr int P = Pad<N>::P;
@@ -175,7 +175,7 @@ inline void launch_dudt_kernel(gf_problem *prob, T nu, const T *const *f, T *con
     const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
     prob->launches++;
     kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, nu, f[0], f[1], f[2], f[3], imass,
-                                                o[0], o[1], o[2]);
+                                                o[0], o[1], o[2], epi);
   } else {
     constexpr int NF = EQN == GF_EQN_ADVECT ? 3 : (EQN == GF_EQN_BURGERS ? 2 : 1);
     constexpr int EPB = epb2<N>();
@@ -185,7 +185,7 @@ inline void launch_dudt_kernel(gf_problem *prob, T nu, const T *const *f, T *con
     const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
     prob->launches++;
     kern<<<grid, dim3(N * N, EPB), smem, st>>>(B, g, prob->ne, nu, f[0], f[1], f[2], f[3], imass,
-                                                o[0], o[1], o[2]);
+                                                o[0], o[1], o[2], epi);
   }
 }
 
@@ -194,16 +194,24 @@ struct DudtLaunch {
   template <int N>
   struct F {
     static int run(gf_problem *prob, int eqn, int mode, T nu, const T *const *f, T *const *o,
-                   cudaStream_t st) {
+                   cudaStream_t st, const RKEpi<T> &epi) {
       const T *im = imass_of<T>(prob);
-      if (eqn == GF_EQN_ADVECT && mode == MODE_ADVECT)
-        launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_ADVECT>(prob, nu, f, o, im, st);
+      if (mode == MODE_EULER) {
+        if (prob->dim != 3) return GF_ERR_UNSUPPORTED;
+        if (eqn == GF_EQN_ADVECT)
+          launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_EULER>(prob, nu, f, o, im, st, epi);
+        else if (eqn == GF_EQN_BURGERS)
+          launch_dudt_kernel<T, N, GF_EQN_BURGERS, MODE_EULER>(prob, nu, f, o, im, st, epi);
+        else
+          launch_dudt_kernel<T, N, GF_EQN_HEAT, MODE_EULER>(prob, nu, f, o, im, st, epi);
+      } else if (eqn == GF_EQN_ADVECT && mode == MODE_ADVECT)
+        launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_ADVECT>(prob, nu, f, o, im, st, epi);
       else if (eqn == GF_EQN_ADVECT)
-        launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_DUDT>(prob, nu, f, o, im, st);
+        launch_dudt_kernel<T, N, GF_EQN_ADVECT, MODE_DUDT>(prob, nu, f, o, im, st, epi);
       else if (eqn == GF_EQN_BURGERS)
-        launch_dudt_kernel<T, N, GF_EQN_BURGERS, MODE_DUDT>(prob, nu, f, o, im, st);
+        launch_dudt_kernel<T, N, GF_EQN_BURGERS, MODE_DUDT>(prob, nu, f, o, im, st, epi);
       else
-        launch_dudt_kernel<T, N, GF_EQN_HEAT, MODE_DUDT>(prob, nu, f, o, im, st);
+        launch_dudt_kernel<T, N, GF_EQN_HEAT, MODE_DUDT>(prob, nu, f, o, im, st, epi);
       return GF_OK;
     }
   };
@@ -227,4 +235,4 @@ template <typename T>
 int launch_dss(gf_problem *prob, int op, T *u, cudaStream_t st);
 template <typename T>
 int launch_dudt(gf_problem *prob, int eqn, int mode, T nu, const T *const *f, T *const *o,
-                cudaStream_t st);
+                cudaStream_t st, const gfk::RKEpi<T> *epi = nullptr);

@@ -29,6 +29,11 @@ struct Stepper {
   }
   bool alloc();
   int rhs(T *const *u, T *const *Kout);
+  // x = the SSP substep update of dudt(u) before its Smooth (the RHS
+  // kernel's MODE_EULER epilogue; 3-d non-deformed problems), then Smooth;
+  // false when the problem takes the separate RHS and update passes
+  bool rhs_euler_smooth(T *const *u, T *const *x, T dt, T *const *uin, T a, T *const *y, T b,
+                        T a2, T *const *y2, T b2, int *rc);
   void smooth(T *v);
   // GMTK::constrain2sphere on the state where step_b calls it, on embedded
   // surfaces with node coordinates and a state of >= 3 components
