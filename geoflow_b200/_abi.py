@@ -30,6 +30,7 @@ GF_GEOM_AFFINE, GF_GEOM_REGULAR, GF_GEOM_DEFORMED, GF_GEOM_EMBEDDED = 0, 1, 2, 3
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
 GF_FILTER_BOYD, GF_FILTER_PROJECTION = 0, 1
 GF_FP32_APPLY_FMA, GF_FP32_APPLY_TF32 = 0, 1
+GF_ICOS_BISECTION, GF_ICOS_LAGRANGIAN = 0, 1
 GF_RK1, GF_RK2, GF_RK3, GF_RK4, GF_SSP22, GF_SSP33, GF_SSP34 = 1, 2, 3, 4, 22, 33, 34
 # gf_integrate_noalloc: fixed scratch of GF_NOALLOC_MAX_BLOCKS blocks of GF_NOALLOC_CHUNK
 GF_NOALLOC_CHUNK, GF_NOALLOC_MAX_BLOCKS = 4096, 32768
@@ -90,6 +91,8 @@ SIGNATURES = {
     "gf_problem_sizes": (c_int, [c_void_p, C.POINTER(c_int64), C.POINTER(c_int64)]),
     "gf_problem_stats": (c_int, [c_void_p, C.POINTER(c_int64)]),
     "gf_set_fp32_apply": (c_int, [c_int]),
+    "gf_icos_sizes": (c_int, [c_int, c_int, c_int, C.POINTER(c_int64), C.POINTER(c_int64)]),
+    "gf_icos_grid": (c_int, [c_int, c_int, c_double, c_int, C.POINTER(P_double), P_double]),
     "gf_helmholtz_apply": (c_int, [c_void_p, c_int, c_double, c_void_p, c_double, c_void_p, c_int,
                                    c_void_p, c_void_p]),
     "gf_helmholtz_apply_T": (c_int, [c_void_p, c_int, c_double, c_double, c_int, c_void_p,

@@ -128,6 +128,64 @@ class GridBox:
         return cnt[self.node_class].astype(np.float64)
 
 
+class IcosGrid:
+    """The 2-d icosahedral sphere of GGridIcos (GE_2DEMBEDDED): gf_icos_grid
+    builds the node coordinates and the embedded metric, and the gather-
+    scatter classes come from coordinate matching (gf_classes_from_coords,
+    tolerance tol_frac times the smallest node spacing, as GGFX::init).
+    refine: GF_ICOS_BISECTION or GF_ICOS_LAGRANGIAN."""
+
+    def __init__(self, level, p, radius=1.0, refine=A.GF_ICOS_BISECTION, tol_frac=0.001):
+        lib = _lib()
+        self.dim, self.p, self.n, self.level, self.radius = 2, int(p), int(p) + 1, level, radius
+        ne, nl = C.c_int64(), C.c_int64()
+        rc = lib.gf_icos_sizes(level, p, refine, C.byref(ne), C.byref(nl))
+        if rc:
+            raise A.GFError(rc, "gf_icos_sizes")
+        self.nelems, N = int(ne.value), int(nl.value)
+        self.ne = [self.nelems]
+        self.nn = self.n * self.n
+        self.xi, self.W, self.D = gll_basis(self.p)
+        self.xyz = [np.zeros(N) for _ in range(3)]
+        self.node_geom = np.zeros(7 * N)
+        xyz_c = (A.P_double * 3)(*[A.ptr(a) for a in self.xyz])
+        rc = lib.gf_icos_grid(level, p, float(radius), refine, xyz_c, A.ptr(self.node_geom))
+        if rc:
+            raise A.GFError(rc, "gf_icos_grid")
+        self.mask = np.ones(N)
+        self.elem_geom = np.zeros(self.nelems * 3)
+        self.periodic = [0, 0]
+        # smallest distance between neighbouring nodes of an element
+        X = np.stack(self.xyz).reshape(3, self.nelems, self.n, self.n)
+        dx = np.sqrt(((X[:, :, :, 1:] - X[:, :, :, :-1]) ** 2).sum(0)).min()
+        dy = np.sqrt(((X[:, :, 1:, :] - X[:, :, :-1, :]) ** 2).sum(0)).min()
+        self.minnodedist = float(min(dx, dy))
+        self.node_class = np.zeros(N, dtype=np.int32)
+        self.class_ptr = np.zeros(N + 1, dtype=np.int32)
+        self.members = np.zeros(N, dtype=np.int32)
+        nc = lib.gf_classes_from_coords(3, N, xyz_c, tol_frac * self.minnodedist,
+                                        A.ptr(self.node_class), A.ptr(self.class_ptr),
+                                        A.ptr(self.members))
+        if nc < 0:
+            raise A.GFError(nc, "gf_classes_from_coords")
+        self.nclass = int(nc)
+        self.class_ptr = self.class_ptr[: nc + 1].copy()
+
+    def ndof(self) -> int:
+        return self.nelems * self.nn
+
+    def xNodes(self):
+        return self.xyz
+
+    def mult(self):
+        return np.diff(self.class_ptr)[self.node_class].astype(np.float64)
+
+    def problem(self, ctx):
+        """The device problem (GF_GEOM_EMBEDDED, no Dirichlet mask)."""
+        return Problem(ctx, self, dirichlet_mask=False, structured=False, geometry="embedded",
+                       node_geom=self.node_geom, node_xyz=np.concatenate(self.xyz))
+
+
 class Problem:
     """Device-resident grid, operators and gather-scatter map (gf_problem)."""
 

@@ -131,6 +131,23 @@ int64_t gf_classes_from_coords_device(gf_ctx_t ctx, int dim, int64_t n,
                                       const double *const *xyz, double tol, int32_t *node_class,
                                       int32_t *class_ptr, int32_t *members);
 
+/* The 2-d icosahedral sphere of GGridIcos (GE_2DEMBEDDED surface):
+ * the base icosahedron (grid/ggrid_icos.ipp:134-225) refined by
+ * GICOS_BISECTION (2^level - 1 rows of sub-triangles per face) or
+ * GICOS_LAGRANGIAN (level rows) (lagrefine, 252-320), each triangle cut
+ * into 3 quadrilateral elements of order p on the sphere of `radius`
+ * (do_elems2d, 378-515).  gf_icos_sizes gives the element and node
+ * counts; gf_icos_grid fills the node coordinates xyz[0..2] (3 host arrays
+ * of nlocal) and, when node_geom != NULL, the embedded metric as
+ * gf_problem_desc.node_geom takes it for GF_GEOM_EMBEDDED: planes
+ * i*3 + k = dXi_i/dX_k (i < 2, k < 3) and plane 6 = Jac, each nlocal long
+ * (GElem_base::dogeom2d, sem/gelem_base.cpp:877-970).  Host only.
+ * Elements come in the reference's order (one rank). */
+enum { GF_ICOS_BISECTION = 0, GF_ICOS_LAGRANGIAN = 1 };
+int gf_icos_sizes(int level, int p, int refine, int64_t *nelems, int64_t *nlocal);
+int gf_icos_grid(int level, int p, double radius, int refine, double *const *xyz,
+                 double *node_geom);
+
 /* ---- problem (grid + operators + gather-scatter map) ---- */
 typedef struct {
   int dim;                 /* 2 or 3 */

@@ -356,6 +356,11 @@ def load_refpath(dim):
         lib.gfr_burgers_run.argtypes = [P_void, C.c_int, C.c_double, C.c_int, C.c_int,
                                         C.c_double, C.c_int, P_double]
         lib.gfr_box_destroy.argtypes = [P_void]
+        lib.gfr_nxyz.argtypes = [P_void]
+        lib.gfr_metric.argtypes = [P_void, P_double, P_double]
+        if dim == 2:
+            lib.gfr_icos_create.restype = P_void
+            lib.gfr_icos_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]
         assert lib.gfr_path_dim() == dim
         _refpath[dim] = lib
     return _refpath[dim]
@@ -363,7 +368,34 @@ def load_refpath(dim):
 
 class RefBox:
     """A box grid run by the reference's own code (see load_refpath); the
-    same layout as OracleBox (element-major, x fastest)."""
+    same layout as OracleBox (element-major, x fastest).  RefBox.icos(...)
+    builds the reference's 2-d icosahedral sphere instead."""
+
+    @classmethod
+    def icos(cls, level, p, radius=1.0, refine=0, tol_frac=0.001):
+        """GGridIcos (GE_2DEMBEDDED) of the 2-d build: refine 0
+        GICOS_BISECTION, 1 GICOS_LAGRANGIAN."""
+        self = cls.__new__(cls)
+        self.lib = lib = load_refpath(2)
+        if lib is None:
+            raise FileNotFoundError(f"{REFPATH[2]} not built")
+        self.dim, self.p = 2, p
+        self.h = lib.gfr_icos_create(level, p, radius, refine, tol_frac)
+        if not self.h:
+            raise RuntimeError(lib.gfr_path_error().decode())
+        self.N = int(lib.gfr_ndof(self.h))
+        return self
+
+    def nxyz(self):
+        return int(self.lib.gfr_nxyz(self.h))
+
+    def metric(self):
+        """(dXi_i/dX_k planes, i < dim, k < nxyz; Jacobian)."""
+        nx = self.nxyz()
+        m = np.zeros(self.dim * nx * self.N)
+        j = np.zeros(self.N)
+        self.lib.gfr_metric(self.h, dp(m), dp(j))
+        return m.reshape(self.dim * nx, self.N), j
 
     def __init__(self, dim, ne, p, periodic=None, x0=None, length=None, tol_frac=0.001):
         self.lib = lib = load_refpath(dim)
@@ -394,7 +426,8 @@ class RefBox:
         return a
 
     def coords(self):
-        return self._vec("gfr_coords", self.dim).reshape(self.dim, self.N)
+        nx = self.nxyz()
+        return self._vec("gfr_coords", nx).reshape(nx, self.N)
 
     def mass(self):
         return self._vec("gfr_mass")

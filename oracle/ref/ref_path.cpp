@@ -285,6 +285,69 @@ void *gfr_box_create(const int *ne, int p, const double *x0, const double *dx, i
   }
 }
 
+#if defined(_G_IS2D)
+// The 2-d icosahedral sphere of the reference's GGridIcos (GE_2DEMBEDDED):
+// base icosahedron refined by refine_type (0: GICOS_BISECTION, 1:
+// GICOS_LAGRANGIAN) at level `level`, each triangle split into 3 quads,
+// order p, radius r; then GGFX::init on the node coordinates
+// (tolerance tol_frac * minnodedist, max_duplicates of the grid).
+void *gfr_icos_create(int level, int p, double radius, int refine_type, double tol_frac) {
+  try {
+    auto *b = new RefBox;
+    std::ostringstream js;
+    js.precision(17);
+    js << "{\"grid_type\": \"grid_icos\", \"terrain_type\": \"none\", "
+          "\"exp_order_type\": \"constant\", \"exp_order\": [" << p << ", " << p
+       << "], \"grid_icos\": {\"grid_name\": \"grid_icos\", \"ilevel\": " << level
+       << ", \"radius\": " << radius << ", \"refine_type\": \""
+       << (refine_type == 0 ? "GICOS_BISECTION" : "GICOS_LAGRANGIAN")
+       << "\", \"maxit\": 128, \"tol\": 1e-8, \"norm_type\": \"GCG_NORM_INF\"}}";
+    b->ptree.load_string(js.str());
+    b->gbasis.resize(GDIM);
+    for (int d = 0; d < GDIM; d++) b->gbasis[d] = new GLLBasis<GCTYPE, GFTYPE>(p);
+    GC_COMM comm = GC_COMM_WORLD;
+    auto *gi = new GGridIcos<RefTypes>(b->ptree, b->gbasis, comm);
+    b->grid = gi;
+    b->grid->grid_init();
+    b->ndof = b->grid->ndof();
+    const auto nxyz = b->grid->xNodes().size();
+    std::vector<std::array<GFTYPE, GGFX<GFTYPE>::NDIM>> xyz(b->ndof);
+    for (size_t i = 0; i < b->ndof; i++)
+      for (size_t d = 0; d < GGFX<GFTYPE>::NDIM; d++)
+        xyz[i][d] = d < nxyz ? b->grid->xNodes()[d][i] : 0.0;
+    b->ggfx = new GGFX<GFTYPE>;
+    b->ggfx->init(gi->max_duplicates(), tol_frac * b->grid->minnodedist(), xyz);
+    b->grid->set_ggfx(*b->ggfx);
+    b->utmp.resize(24);
+    for (size_t j = 0; j < b->utmp.size(); j++) b->utmp[j] = new GTVector<GFTYPE>(b->ndof);
+    return b;
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+#endif
+
+// Number of coordinate components (GDIM, or 3 on an embedded surface).
+int gfr_nxyz(void *h) { return (int)static_cast<RefBox *>(h)->grid->xNodes().size(); }
+
+// dXi_i/dX_k per node into out[(i * nxy + k) * ndof + n] (i < GDIM,
+// k < nxy) and the Jacobian into jac (GGrid::dXidX(), GGrid::Jac()).
+// Regular grids store only the diagonal (k = i) planes, the rest are 0.
+void gfr_metric(void *h, double *out, double *jac) {
+  auto *b = static_cast<RefBox *>(h);
+  auto &M = b->grid->dXidX();
+  const size_t nxy = b->grid->xNodes().size();
+  for (size_t i = 0; i < (size_t)GDIM; i++)
+    for (size_t k = 0; k < nxy; k++) {
+      double *o = out + (i * nxy + k) * b->ndof;
+      const bool have = i < M.size(1) && k < M.size(2);
+      for (size_t n = 0; n < b->ndof; n++) o[n] = have && M(i, k).size() ? M(i, k)[n] : 0.0;
+    }
+  auto &J = b->grid->Jac();
+  for (size_t n = 0; n < b->ndof; n++) jac[n] = J[n];
+}
+
 size_t gfr_ndof(void *h) { return static_cast<RefBox *>(h)->ndof; }
 
 // Node coordinates, xyz[d*ndof + i].
@@ -352,14 +415,16 @@ int gfr_helmholtz(void *h, const double *u, double *out, const double *p, size_t
   return 0;
 }
 
-// GAdvect::apply: out = M * sum_j c_j d/dx_j u, c given as GDIM vectors.
+// GAdvect::apply: out = M * sum_j c_j d/dx_j u, c given as one vector per
+// physical coordinate (GDIM, or 3 on an embedded surface).
 int gfr_advect(void *h, const double *u, const double *c, double *out) {
   auto *b = static_cast<RefBox *>(h);
+  const int nc = (int)b->grid->xNodes().size();
   GTVector<GFTYPE> vu(b->ndof), vo(b->ndof);
-  std::vector<GTVector<GFTYPE>> cv(GDIM, GTVector<GFTYPE>(b->ndof));
-  RefTypes::State cs(GDIM);
+  std::vector<GTVector<GFTYPE>> cv(nc, GTVector<GFTYPE>(b->ndof));
+  RefTypes::State cs(nc);
   for (size_t i = 0; i < b->ndof; i++) vu[i] = u[i];
-  for (int d = 0; d < GDIM; d++) {
+  for (int d = 0; d < nc; d++) {
     for (size_t i = 0; i < b->ndof; i++) cv[d][i] = c[d * b->ndof + i];
     cs[d] = &cv[d];
   }
@@ -440,7 +505,10 @@ int gfr_burgers_run(void *h, int kind, double nu, int order, int ssp, double dt,
     // GBurgers keeps a shared_ptr to itself (gburgers.ipp:94), so it owns
     // its own lifetime; it is created once per run and left to the process.
     auto *eq = new GBurgers<RefTypes>(*b->grid, tr);
-    const int nstate = tr.nstate;
+    // the equation sets its own state size (one velocity per physical
+    // coordinate: 3 on an embedded surface); the heat equation reads only
+    // its evolved component
+    const int nstate = kind == 2 ? 1 : eq->get_traits().nstate;
     const int ntmp = eq->tmp_size() + 4;
     RefTypes::State us(nstate), uf(nstate), tmp(ntmp);
     std::vector<GTVector<GFTYPE> *> owned;

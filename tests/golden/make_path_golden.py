@@ -18,6 +18,12 @@ is an input handed to the reference or an output it produced:
                                      full length (16^2 elements, p = 4,
                                      c = (1, 0.5), nu = 0.01, RK4,
                                      dt = 1e-4, 200 steps)
+  icos_{tag}_{xyz,metric,jac,mass}   GGridIcos (GE_2DEMBEDDED) nodes, dXi/dX
+                                     (2 x 3 planes), Jacobian, mass
+  icos_{tag}_{u,dss*,q,helm,c,adv}   GGFX, GHelmholtz (embed_prod), GAdvect on it
+  icosadv_{u0,u,c,dt}                the cosine bell in the solid-body wind
+                                     advected by GBurgers (RK4, nu = 1e-3) on
+                                     the level-1 p = 3 sphere
   cfg3s_{u0,u100,dt}                 the 3-d Burgers case (its initial
                                      velocity, nu = 1e-3, SSP-RK3, CFL 0.3,
                                      100 steps) on a 3^3-element p = 5
@@ -153,6 +159,31 @@ def main():
         assert rc == 0
         out[k + "b"], out[k + "x"] = b, x
         out[k + "info"] = np.array([rc, it], dtype=np.int64)
+    # the icosahedral sphere (GE_2DEMBEDDED)
+    for tag, level, p, refine in (("l0p4", 0, 4, 0), ("l1p2lag", 1, 2, 1)):
+        r = O.RefBox.icos(level, p, 1.0, refine)
+        k = f"icos_{tag}_"
+        out[k + "xyz"] = r.coords()
+        m, j = r.metric()
+        out[k + "metric"], out[k + "jac"], out[k + "mass"] = m, j, r.mass()
+        u = rng.standard_normal(r.N)
+        out[k + "u"] = u
+        for op in range(4):
+            out[k + f"dss{op}"] = r.dss(u.copy(), op)
+        q = 0.5 + rng.random(r.N)
+        out[k + "q"] = q
+        out[k + "helm"] = r.helmholtz(u, p=0.7, q_vec=q)
+        c = W.icos_solid_body_wind(list(r.coords()), u0=1.0, alpha=0.3)
+        out[k + "c"] = np.stack(c)
+        out[k + "adv"] = r.advect(u, c)
+    r = O.RefBox.icos(1, 3, 1.0, 0)
+    xyz = list(r.coords())
+    u0 = W.icos_cosine_bell(xyz, 0.3, 4.0)
+    c = W.icos_solid_body_wind(xyz, u0=1.0, alpha=0.3)
+    st = [u0.copy()] + [a.copy() for a in c]
+    r.burgers_run(0, 1e-3, 4, False, st, 2e-3, 20)
+    out["icosadv_u0"], out["icosadv_u"], out["icosadv_c"] = u0, st[0], np.stack(c)
+    out["icosadv_dt"] = np.array([2e-3])
     # 3-d Burgers, SSP-RK3, 100 steps, on 3^3 elements at p = 5
     ne3, p3 = 3, 5
     r = O.RefBox(3, [ne3] * 3, p3, periodic=[1] * 3, length=[2 * np.pi] * 3)
