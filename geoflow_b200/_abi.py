@@ -91,6 +91,15 @@ SIGNATURES = {
     "gf_problem_sizes": (c_int, [c_void_p, C.POINTER(c_int64), C.POINTER(c_int64)]),
     "gf_problem_stats": (c_int, [c_void_p, C.POINTER(c_int64)]),
     "gf_set_fp32_apply": (c_int, [c_int]),
+    "gf_gather": (c_int, [c_void_p, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
+    "gf_dss_fold_copies": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int64,
+                                   c_void_p, c_void_p, c_void_p]),
+    "gf_rk_stage_sum": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                c_double, c_double, c_double, c_void_p]),
+    "gf_rk_update": (c_int, [c_void_p, c_int, c_void_p, c_double, c_void_p, c_double, c_void_p,
+                             c_double, c_double, c_void_p, c_double]),
+    "gf_rk_accum": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_double]),
+    "gf_problem_set_imass": (c_int, [c_void_p, P_double]),
     "gf_icos_sizes": (c_int, [c_int, c_int, c_int, C.POINTER(c_int64), C.POINTER(c_int64)]),
     "gf_icos_grid": (c_int, [c_int, c_int, c_double, c_int, C.POINTER(P_double), P_double]),
     "gf_helmholtz_apply": (c_int, [c_void_p, c_int, c_double, c_void_p, c_double, c_void_p, c_int,

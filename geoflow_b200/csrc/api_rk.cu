@@ -481,6 +481,33 @@ extern "C" int gf_rk_advance(gf_problem_t prob, int dtype, const gf_rk_traits *t
   return gf_fail(prob->ctx, GF_ERR_ARG, "unknown dtype %d", dtype);
 }
 
+// y = uin + ((0 + b0 K0) + b1 K1 + ...) on the problem's nlocal nodes: the
+// stage input of step_b, as the stepper forms it (k_stage_sum); used by the
+// partitioned stepper (geoflow_b200/dist.py).
+extern "C" int gf_rk_stage_sum(gf_problem_t prob, int dtype, const void *uin, int nk,
+                               const void *K0, const void *K1, const void *K2, double b0,
+                               double b1, double b2, void *y) {
+  if (!prob) return GF_ERR_ARG;
+  gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, uin && y && nk >= 0 && nk <= 3, "stage sum needs uin, y and 0..3 terms");
+  GF_REQUIRE(ctx, (nk < 1 || K0) && (nk < 2 || K1) && (nk < 3 || K2), "missing stage vector");
+  const int64_t n = prob->nlocal;
+  const unsigned g = grid_for(n, 256, ctx->sm_count * 8);
+  prob->launches++;
+  if (dtype == GF_F64)
+    k_stage_sum<double><<<g, 256, 0, ctx->stream>>>(n, (const double *)uin, nk,
+                                                    (const double *)K0, (const double *)K1,
+                                                    (const double *)K2, b0, b1, b2, (double *)y);
+  else if (dtype == GF_F32)
+    k_stage_sum<float><<<g, 256, 0, ctx->stream>>>(n, (const float *)uin, nk, (const float *)K0,
+                                                   (const float *)K1, (const float *)K2,
+                                                   (float)b0, (float)b1, (float)b2, (float *)y);
+  else
+    return gf_fail(ctx, GF_ERR_ARG, "unknown dtype %d", dtype);
+  GF_CHECK_LAUNCH(ctx);
+  return GF_OK;
+}
+
 extern "C" int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *tr,
                                   void *const *u, const void *const *c, double t0, double dt,
                                   int nsteps) {

@@ -688,3 +688,18 @@ extern "C" int gf_problem_stats(gf_problem_t prob, int64_t *kernel_launches) {
   if (kernel_launches) *kernel_launches = (int64_t)prob->launches;
   return GF_OK;
 }
+
+// The inverse mass 1/Smooth(M) of a problem that is one rank's part of a
+// partitioned grid: its own classes miss the copies on other ranks, so the
+// caller supplies the assembled values (host, nlocal).
+extern "C" int gf_problem_set_imass(gf_problem_t prob, const double *imass) {
+  if (!prob) return GF_ERR_ARG;
+  gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, imass, "imass is required");
+  const int64_t n = prob->nlocal;
+  std::vector<float> f(n);
+  for (int64_t i = 0; i < n; i++) f[i] = (float)imass[i];
+  GF_CUDA(ctx, cudaMemcpy(prob->imass_d, imass, sizeof(double) * n, cudaMemcpyHostToDevice));
+  GF_CUDA(ctx, cudaMemcpy(prob->imass_f, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  return GF_OK;
+}

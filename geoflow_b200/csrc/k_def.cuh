@@ -50,21 +50,21 @@ enum { DEF_HELM = 0, DEF_DUDT = 1, DEF_ADVECT = 2, DEF_DERIV = 3 };
 // mode DEF_HELM: uo = p L u (+ q M u); DEF_DUDT: uo = Minv(-nu L u - adv)
 // (heat when nv == 0); DEF_ADVECT: uo = adv = M sum_k c_k du/dx_k;
 // DEF_DERIV: uo = du/dx_{idir}.  nv velocity components c0..c2.
-template <typename T, int N, int DIM, class LD, typename TO>
-__global__ void __launch_bounds__(256)
-    k_def(const __grid_constant__ Basis<T, N> B, const DefGeom<T> g, int64_t ne, int mode, T p,
-          const T *__restrict__ pvec, T q, const T *__restrict__ qvec, int use_mass, const LD ld,
-          int nv, const T *__restrict__ c0, const T *__restrict__ c1, const T *__restrict__ c2,
-          int idir, const T *__restrict__ imass, TO *__restrict__ uo,
-          const double *__restrict__ stop) {
-  if (stop && stop[0] != 0.0) return;
+// One element e of k_def, by the threads of the block (the body shared by
+// k_def and the ensemble kernels, api_ensemble.cu).  BB is a basis with
+// members D[N*N] and W[N]; smem holds (1 + 2 DIM) N^DIM values of T.
+template <typename T, int N, int DIM, class LD, typename TO, class BB>
+__device__ __forceinline__ void def_element(const BB &B, const DefGeom<T> &g, int64_t e, int mode,
+                                            T p, const T *__restrict__ pvec, T q,
+                                            const T *__restrict__ qvec, int use_mass, const LD &ld,
+                                            int nv, const T *__restrict__ c0,
+                                            const T *__restrict__ c1, const T *__restrict__ c2,
+                                            int idir, const T *__restrict__ imass,
+                                            TO *__restrict__ uo, T *smem) {
   constexpr int NN = N * N, NE = DIM == 3 ? NN * N : NN;
-  extern __shared__ __align__(16) unsigned char smem_def[];
-  T *su = reinterpret_cast<T *>(smem_def);
+  T *su = smem;
   T *sd = su + NE;        // DIM planes: D_j u
   T *sg = sd + DIM * NE;  // DIM planes: sum_i G_ij D_i u
-  const int64_t e = blockIdx.x;
-  if (e >= ne) return;
   const int64_t base = e * NE;
   const T *cv[3] = {c0, c1, c2};
   const int64_t nl = g.nlocal;
@@ -165,6 +165,21 @@ __global__ void __launch_bounds__(256)
       uo[node] = (TO)(imass[node] * r);
     }
   }
+}
+
+template <typename T, int N, int DIM, class LD, typename TO>
+__global__ void __launch_bounds__(256)
+    k_def(const __grid_constant__ Basis<T, N> B, const DefGeom<T> g, int64_t ne, int mode, T p,
+          const T *__restrict__ pvec, T q, const T *__restrict__ qvec, int use_mass, const LD ld,
+          int nv, const T *__restrict__ c0, const T *__restrict__ c1, const T *__restrict__ c2,
+          int idir, const T *__restrict__ imass, TO *__restrict__ uo,
+          const double *__restrict__ stop) {
+  if (stop && stop[0] != 0.0) return;
+  extern __shared__ __align__(16) unsigned char smem_def[];
+  const int64_t e = blockIdx.x;
+  if (e >= ne) return;
+  def_element<T, N, DIM, LD, TO>(B, g, e, mode, p, pvec, q, qvec, use_mass, ld, nv, c0, c1, c2,
+                                 idir, imass, uo, reinterpret_cast<T *>(smem_def));
 }
 
 }  // namespace gfk

@@ -315,6 +315,37 @@ int gf_rk_advance(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
 int gf_rk_advance_host(gf_problem_t prob, int dtype, const gf_rk_traits *traits,
                        void *const *u, const void *const *c, double t0, double dt, int nsteps);
 
+/* ---- building blocks of the element-partitioned (multi-GPU) path ----
+ * (geoflow_b200/dist.py; no single reference counterpart: GGFX::doOp's
+ * send/recv exchange, comm/ggfx.hpp:346-443, and GExRKStepper's stage
+ * arithmetic, pdes/gexrk_stepper.ipp:252-341, 533-819, split at the
+ * exchange.)  All arrays are device arrays on the problem's stream.
+ * gf_gather: dst[k] = src[idx[k]], k < n.
+ * gf_dss_fold_copies: for k < nout, u[out_local[k]] = the GGFX fold (op)
+ *   of point out_point[k]'s copies pool[table[point*maxc + j]], j in order
+ *   while table[...] >= 0 (Sum/Smooth from 0, Smooth divided by the copy
+ *   count, Max/Min as std::max/min folds): the reference's fold order when
+ *   the table lists the copies in ascending global local id.
+ * gf_rk_stage_sum: y = uin + ((0 + b0 K0) + b1 K1 + b2 K2) (nk terms).
+ * gf_rk_update: x = dt x + uin; x = a x + b y (if y); x = a2 x + b2 y2
+ *   (if y2): the SSP substep update before its Smooth.
+ * gf_rk_accum: uout = uout + K ch.
+ * The last three run on the problem's nlocal nodes. */
+int gf_gather(gf_problem_t prob, int dtype, int64_t n, const int32_t *idx, const void *src,
+              void *dst);
+int gf_dss_fold_copies(gf_problem_t prob, int dtype, int op, int maxc, const int32_t *table,
+                       const void *pool, int64_t nout, const int32_t *out_local,
+                       const int32_t *out_point, void *u);
+int gf_rk_stage_sum(gf_problem_t prob, int dtype, const void *uin, int nk, const void *K0,
+                    const void *K1, const void *K2, double b0, double b1, double b2, void *y);
+int gf_rk_update(gf_problem_t prob, int dtype, void *x, double dt, const void *uin, double a,
+                 const void *y, double b, double a2, const void *y2, double b2);
+int gf_rk_accum(gf_problem_t prob, int dtype, void *uout, const void *K, double ch);
+/* Replaces the problem's inverse mass 1/Smooth(M) (used by gf_dudt and the
+ * RK stepper) with the caller's host values (nlocal): the assembled values
+ * when the problem is one rank's part of a partitioned grid. */
+int gf_problem_set_imass(gf_problem_t prob, const double *imass);
+
 /* ---- allocation-free integral (no counterpart in the reference) ----
  * sum_i mass[i]*u[i] over n nodes into *result, all three device pointers;
  * with mass = the local mass W (x) W (x) W Jac this is GGrid::integrate.
