@@ -32,6 +32,7 @@ GF_FILTER_BOYD, GF_FILTER_PROJECTION = 0, 1
 GF_FP32_APPLY_FMA, GF_FP32_APPLY_TF32 = 0, 1
 GF_ICOS_BISECTION, GF_ICOS_LAGRANGIAN = 0, 1
 GF_RK1, GF_RK2, GF_RK3, GF_RK4, GF_SSP22, GF_SSP33, GF_SSP34 = 1, 2, 3, 4, 22, 33, 34
+GF_ENS_RK, GF_ENS_CG = 0, 1
 # gf_integrate_noalloc: fixed scratch of GF_NOALLOC_MAX_BLOCKS blocks of GF_NOALLOC_CHUNK
 GF_NOALLOC_CHUNK, GF_NOALLOC_MAX_BLOCKS = 4096, 32768
 GF_NOALLOC_MAX_N = GF_NOALLOC_CHUNK * GF_NOALLOC_MAX_BLOCKS
@@ -155,6 +156,17 @@ SIGNATURES = {
                                P_void]),
     "gf_adjoint_gradient": (c_int, [c_void_p, C.POINTER(RKTraits), P_void, P_void, P_void,
                                     c_double, c_int, c_int, P_double, P_void]),
+    "gf_ensemble_create": (c_int, [c_void_p, c_int, P_void, P_void]),
+    "gf_ensemble_destroy": (c_int, [c_void_p]),
+    "gf_ensemble_kind": (c_int, [c_void_p]),
+    "gf_ensemble_launches": (C.c_uint64, [c_void_p]),
+    "gf_ensemble_rk_advance": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void,
+                                       P_double, c_int]),
+    "gf_ensemble_cg_solve": (c_int, [c_void_p, C.POINTER(CGTraits), c_double, c_double, P_void,
+                                     P_void, P_int, P_double, P_int]),
+    "gf_ensemble_tune": (c_int, [c_void_p, c_int, c_int]),
+    "gf_ensemble_shape": (c_int, [c_void_p, c_int, P_int, P_int, P_int, P_int]),
+    "gf_ensemble_set_shape": (c_int, [c_void_p, c_int, c_int, c_int, P_int]),
 }
 
 _lib = None

@@ -1,0 +1,1601 @@
+// api_ensemble.cu -- ensembles of independent problems advanced together:
+// one persistent launch per RK stage (2-d deformed and embedded members,
+// e.g. icosahedral-sphere advection cases) or per CG iteration (2-d box
+// Helmholtz members: FP32 iterations, FP64 residuals and refinement).  The
+// reference runs one problem per process; nothing here has a reference
+// counterpart beyond the per-member arithmetic named below.
+//
+// Work lists.  Element work is cut into chunks of one warp: the warp splits
+// into teams of `team` lanes (8, 16 or 32), one element per team, so a
+// chunk holds 32/team elements of one member.  The chunks of all members
+// are numbered consecutively and the warps of the grid take them round
+// robin, which spreads every member evenly over the GPU whatever its size
+// and order.  Node work is numbered the same way over the members'
+// gather-scatter classes (RK) or, for the CG, cut into one contiguous slice
+// of every member per block, so a block owns the same nodes in every phase
+// and its partial dot products come out in a fixed order.
+//
+// Phases inside one launch are separated by a grid barrier (an arrival
+// count and a generation word; the spin is bounded and records a timeout
+// instead of waiting for ever).  The kernels are launched cooperatively,
+// so all blocks are resident.  The last block to reach a reducing barrier
+// folds the blocks' partials per member in block order and forms the
+// member's CG scalars before it releases the others: for a given launch
+// shape the scalars are deterministic.
+//
+// Arithmetic.  An RK member's element body is def_element (k_def.cuh), its
+// folds are those of k_dss_rk_csr / k_dss_csr and its stage sums those of
+// step_b (rk_stage_point), so each member advances bit for bit as
+// gf_rk_advance advances it alone.  A CG member runs GCG::solve_impl's DFM
+// iteration (solvers/gcg.ipp:239-382) with a Jacobi preconditioner on the
+// unique lattice nodes: FP32 vectors and applies, FP64 dot products, and
+// restarted refinement, x += d and r = mask DSS_Sum(b - A x) in FP64 each
+// time an FP32 run has reduced its residual by inner_tol.
+//
+// Tile shapes (threads per block, blocks per SM, team width per order) are
+// chosen by gf_ensemble_tune, which times the element phase of candidate
+// shapes on the ensemble's own data.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gf_common.cuh"
+#include "k_def.cuh"
+#include "k_dss.cuh"
+#include "k_vec.cuh"
+#include "rk_common.cuh"
+
+using namespace gfk;
+
+namespace {
+
+constexpr int EN_MINN = 3, EN_MAXN = 10;  // members of order 2..9
+constexpr int EN_MAXMEM = 64;
+constexpr int EN_MAXWARPS = 16;           // threads per block <= 512
+constexpr unsigned EN_SPIN_LIMIT = 1u << 21;
+
+enum { EN_REFINE = 0, EN_INNER = 1, EN_DONE = 2 };
+
+struct EnMember {
+  int N, nxy, team, epw;
+  int64_t ne, nlocal, nclass, nL;
+  int64_t chunk0, nchunk, class0;
+  double D[EN_MAXN * EN_MAXN], W[EN_MAXN], K1d[EN_MAXN];
+  // deformed / embedded geometry, [0] FP64 and [1] FP32
+  const void *X[2], *G[2], *J[2], *imass[2];
+  const int32_t *class_ptr, *members;
+  // RK state: u[0] the caller's, u[1] scratch; slopes; final-stage input
+  void *u[2], *K[3], *uf;
+  const void *c[3];
+  double coef[4][3], ch[4];
+  // box lattice (CG)
+  BoxWalk walk;
+  int ne0;
+  const uint8_t *maskL8;
+  const double *egeom64;
+  const float *egeom32;
+  const double *bE;
+  double *xE, *bL, *xL, *r64, *dinv64, *aE;
+  float *dL, *r32, *w32, *q32, *dinv32;
+};
+
+struct EnCG {
+  double rho, alpha, beta, rnorm, rnorm64, rtol, itol, bnorm, nd;
+  int next, iters, sweeps, status;
+};
+
+struct EnCtl {
+  unsigned count, gen, err, launches;
+  int any_active;
+  int nonfinite[EN_MAXMEM];
+};
+
+struct EnArgs {
+  EnMember *mem;
+  int nmem;
+  const int64_t *chunk_pref, *class_pref;  // nmem + 1 each
+  int64_t nchunk, nclass;
+  EnCtl *ctl;
+  EnCG *cg;
+  double *partials;  // [nmem][2][gridDim.x]
+  int wbytes;        // dynamic shared bytes per warp
+  // RK
+  int ns, par, eqn;
+  double nu;
+  // CG
+  double p, q, tol, inner_tol;
+  int normtype, maxit, max_refine, relative, all_inner;
+  unsigned launch_cap;
+  cudaGraphConditionalHandle cond;
+  int has_cond;
+};
+
+// ---- grid barrier -------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Every block calls it; `last` runs in the last block to arrive, with the
+// whole block, before the others are released.
+template <class F>
+__device__ __forceinline__ void en_barrier(EnCtl *ctl, F last) {
+  __shared__ unsigned s_last, s_gen;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = ld_acquire(&ctl->gen);
+    __threadfence();
+    const unsigned t = atomicAdd(&ctl->count, 1u);
+    s_last = (t == gridDim.x - 1);
+    s_gen = g;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    last();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicExch(&ctl->count, 0u);
+      __threadfence();
+      atomicAdd(&ctl->gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    unsigned it = 0;
+    while (ld_acquire(&ctl->gen) == s_gen) {
+      if (++it > EN_SPIN_LIMIT || ld_acquire(&ctl->err)) {
+        atomicExch(&ctl->err, 1u);
+        break;
+      }
+      if (it > 64) __nanosleep(32);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+struct NoWork {
+  __device__ void operator()() const {}
+};
+
+// largest m with pref[m] <= x
+__device__ __forceinline__ int en_find(const int64_t *pref, int n, int64_t x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pref[mid] <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void en_load_pref(const int64_t *g, int64_t *s, int n) {
+  for (int i = threadIdx.x; i <= n; i += blockDim.x) s[i] = g[i];
+}
+
+__device__ __forceinline__ unsigned team_mask(int team, int tid) {
+  return team == 32 ? 0xffffffffu : (((1u << team) - 1u) << (tid * team));
+}
+
+// words of a warp's basis region (D then W), rounded to 16 bytes
+template <typename T>
+__host__ __device__ __forceinline__ int en_basis_words(int N) {
+  const int w = N * N + N, per16 = 16 / (int)sizeof(T);
+  return (w + per16 - 1) / per16 * per16;
+}
+
+template <typename T>
+struct SBasis {
+  const T *D, *W;
+};
+
+// ---- RK members -----------------------------------------------------------
+template <typename T>
+struct LoadStage {  // the step_b stage input at the element's nodes
+  using value_type = T;
+  const T *uin, *K0, *K1, *K2;
+  T b0, b1, b2;
+  int nk;
+  template <int N>
+  __device__ __forceinline__ void zline(int64_t e, int i, int j, T (&out)[N]) const {
+#pragma unroll
+    for (int k = 0; k < N; k++) out[k] = pt(e * (N * N * N) + (int64_t)k * N * N + j * N + i);
+  }
+  __device__ __forceinline__ T pt(int64_t i) const {
+    return rk_stage_point(uin[i], nk, K0, K1, K2, b0, b1, b2, i);
+  }
+  template <int N>
+  __device__ __forceinline__ T point2(int64_t e, int i, int j) const {
+    return pt(e * (N * N) + j * N + i);
+  }
+};
+
+template <typename T>
+struct LoadL2 {  // an element-local vector written earlier in this launch
+  using value_type = T;
+  const T *u;
+  template <int N>
+  __device__ __forceinline__ void zline(int64_t e, int i, int j, T (&out)[N]) const {
+#pragma unroll
+    for (int k = 0; k < N; k++) out[k] = __ldcg(u + e * (N * N * N) + (int64_t)k * N * N + j * N + i);
+  }
+  template <int N>
+  __device__ __forceinline__ T point2(int64_t e, int i, int j) const {
+    return __ldcg(u + e * (N * N) + j * N + i);
+  }
+};
+
+template <typename T, int N>
+__device__ void en_rhs_elem(const LaneTeam &tm, const EnMember &M, int64_t e, const SBasis<T> &B,
+                            T *slice, bool from_uf, int stage, int par, int eqn, T nu) {
+  constexpr int pr = sizeof(T) == 4 ? 1 : 0;
+  const DefGeom<T> g{(const T *)M.X[pr], (const T *)M.G[pr], (const T *)M.J[pr], M.nxy,
+                     M.nlocal};
+  const T *imass = (const T *)M.imass[pr];
+  const int nv = eqn == GF_EQN_ADVECT ? M.nxy : 0;
+  const T *c0 = (const T *)M.c[0], *c1 = (const T *)M.c[1], *c2 = (const T *)M.c[2];
+  if (from_uf) {
+    def_element<T, N, 2, LoadL2<T>, T>(tm, B, g, e, DEF_DUDT, nu, nullptr, T(0), nullptr, 0,
+                                       LoadL2<T>{(const T *)M.uf}, nv, c0, c1, c2, 0, imass,
+                                       (T *)M.K[0], slice);
+  } else {
+    const LoadStage<T> ld{(const T *)M.u[par], (const T *)M.K[0], (const T *)M.K[1],
+                          (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
+                          (T)M.coef[stage][2], stage};
+    def_element<T, N, 2, LoadStage<T>, T>(tm, B, g, e, DEF_DUDT, nu, nullptr, T(0), nullptr, 0,
+                                          ld, nv, c0, c1, c2, 0, imass, (T *)M.K[stage], slice);
+  }
+}
+
+// Element phase of an RK stage: K_stage = dudt(stage input), or for the
+// final stage K_0 = dudt(uf).
+template <typename T>
+__device__ void en_rk_elements(const EnArgs &a, const int64_t *cpref, bool from_uf, int stage) {
+  extern __shared__ __align__(16) unsigned char en_smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  T *ws = reinterpret_cast<T *>(en_smem + (size_t)wib * a.wbytes);
+  const int64_t nw = (int64_t)gridDim.x * wpb;
+  const T nu = (T)a.nu;
+  int cur = -1;
+  for (int64_t ch = (int64_t)blockIdx.x * wpb + wib; ch < a.nchunk; ch += nw) {
+    const int mi = en_find(cpref, a.nmem, ch);
+    const EnMember &M = a.mem[mi];
+    const int N = M.N;
+    if (mi != cur) {
+      for (int i = lane; i < N * N; i += 32) ws[i] = (T)M.D[i];
+      for (int i = lane; i < N; i += 32) ws[N * N + i] = (T)M.W[i];
+      __syncwarp();
+      cur = mi;
+    }
+    const int team = M.team, tid = lane / team;
+    const int64_t e = (ch - M.chunk0) * M.epw + tid;
+    if (e < M.ne) {
+      const LaneTeam tm{lane - tid * team, team, team_mask(team, tid)};
+      const SBasis<T> B{ws, ws + N * N};
+      T *slice = ws + en_basis_words<T>(N) + tid * 5 * N * N;
+      switch (N) {
+        case 3: en_rhs_elem<T, 3>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 4: en_rhs_elem<T, 4>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 5: en_rhs_elem<T, 5>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 6: en_rhs_elem<T, 6>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 7: en_rhs_elem<T, 7>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 8: en_rhs_elem<T, 8>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 9: en_rhs_elem<T, 9>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        default: en_rhs_elem<T, 10>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Final-stage input: uf = Smooth(stage sum over the ns-1 earlier slopes).
+template <typename T>
+__device__ void en_rk_stage_input(const EnArgs &a, const int64_t *kpref, int stage) {
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.nclass; c += nt) {
+    const int mi = en_find(kpref, a.nmem, c);
+    const EnMember &M = a.mem[mi];
+    const int64_t cl = c - M.class0;
+    const int32_t b0 = M.class_ptr[cl], e0 = M.class_ptr[cl + 1];
+    const T *uin = (const T *)M.u[a.par];
+    const T *K0 = (const T *)M.K[0], *K1 = (const T *)M.K[1], *K2 = (const T *)M.K[2];
+    const T c0 = (T)M.coef[stage][0], c1 = (T)M.coef[stage][1], c2 = (T)M.coef[stage][2];
+    T acc = T(0);
+    for (int32_t k = b0; k < e0; k++) {
+      const int64_t m = M.members[k];
+      acc = __fadd_rn_t(acc, rk_stage_point(uin[m], stage, K0, K1, K2, c0, c1, c2, m));
+    }
+    acc = acc / (T)(e0 - b0);
+    T *uf = (T *)M.uf;
+    for (int32_t k = b0; k < e0; k++) uf[M.members[k]] = acc;
+  }
+}
+
+// Fold of a stage: Smooth K_stage and uout += c h K (stages before the
+// last), or for the last stage uout = Smooth(uout + c h Smooth(K_0)).
+template <typename T>
+__device__ void en_rk_fold(const EnArgs &a, const int64_t *kpref, int stage) {
+  const bool fin = stage == a.ns - 1;
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.nclass; c += nt) {
+    const int mi = en_find(kpref, a.nmem, c);
+    const EnMember &M = a.mem[mi];
+    const int64_t cl = c - M.class0;
+    const int32_t b0 = M.class_ptr[cl], e0 = M.class_ptr[cl + 1];
+    const T cnt = (T)(e0 - b0), ch = (T)M.ch[stage];
+    T *uout = (T *)M.u[1 - a.par];
+    const T *src = stage == 0 ? (const T *)M.u[a.par] : uout;
+    T *Kx = (T *)M.K[fin ? 0 : stage];
+    T acc = T(0);
+    for (int32_t k = b0; k < e0; k++) acc = __fadd_rn_t(acc, __ldcg(Kx + M.members[k]));
+    acc = acc / cnt;
+    if (!fin) {
+      for (int32_t k = b0; k < e0; k++) {
+        const int64_t m = M.members[k];
+        Kx[m] = acc;
+        uout[m] = rk_accum_point(src[m], acc, ch);
+      }
+    } else {
+      T acc2 = T(0);
+      for (int32_t k = b0; k < e0; k++)
+        acc2 = __fadd_rn_t(acc2, rk_accum_point(src[M.members[k]], acc, ch));
+      acc2 = acc2 / cnt;
+      for (int32_t k = b0; k < e0; k++) uout[M.members[k]] = acc2;
+      if (!isfinite((double)acc2)) a.ctl->nonfinite[mi] = 1;
+    }
+  }
+}
+
+// One RK stage of every member (step_b of GExRKStepper, gexrk_stepper.ipp:
+// 252-341): stages before the last are RHS | fold; the last is stage input
+// and Smooth | RHS | fold.
+template <typename T>
+__global__ void __launch_bounds__(512) k_en_rk_stage(EnArgs a, int stage) {
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_kpref[EN_MAXMEM + 1];
+  en_load_pref(a.chunk_pref, s_cpref, a.nmem);
+  en_load_pref(a.class_pref, s_kpref, a.nmem);
+  __syncthreads();
+  const bool fin = stage == a.ns - 1;
+  if (fin) {
+    en_rk_stage_input<T>(a, s_kpref, stage);
+    en_barrier(a.ctl, NoWork{});
+  }
+  en_rk_elements<T>(a, s_cpref, fin, stage);
+  en_barrier(a.ctl, NoWork{});
+  en_rk_fold<T>(a, s_kpref, stage);
+}
+
+// element phase alone (the autotuner's timing kernel): stage 0 of step_b
+template <typename T>
+__global__ void __launch_bounds__(512) k_en_rk_tune(EnArgs a) {
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1];
+  en_load_pref(a.chunk_pref, s_cpref, a.nmem);
+  __syncthreads();
+  en_rk_elements<T>(a, s_cpref, false, 0);
+}
+
+// ---- CG members (2-d box lattices) -----------------------------------------
+// One affine element's Helmholtz apply p L u + q M u (the arithmetic of
+// k_helm2d, GHelmholtz::reg_prod, sem/ghelmholtz.ipp:309-378) by a team,
+// input gathered from the lattice by ld(c), output element-local.
+template <typename T, int N, class LD>
+__device__ __forceinline__ void en_box_apply(const LaneTeam &tm, const EnMember &M, int64_t e,
+                                             const T *D, const T *W, T *s, const LD &ld, T p,
+                                             T q, T *__restrict__ out) {
+  constexpr int NN = N * N;
+  T *su = s, *sgx = s + NN, *sgy = s + 2 * NN;
+  const T *eg = sizeof(T) == 8 ? (const T *)M.egeom64 : (const T *)M.egeom32;
+  const T X0 = eg[e * 3], X1 = eg[e * 3 + 1], J = eg[e * 3 + 2];
+  const int ey = (int)(e / M.ne0), ex = (int)(e - (int64_t)ey * M.ne0);
+  const BoxWalk &w = M.walk;
+  for (int a = tm.rank(); a < NN; a += tm.size()) {
+    const int i = a % N, j = a / N;
+    int gx = ex * (N - 1) + i, gy = ey * (N - 1) + j;
+    if (w.per[0] && gx == w.M[0]) gx = 0;
+    if (w.per[1] && gy == w.M[1]) gy = 0;
+    su[a] = ld((int64_t)gy * w.M[0] + gx);
+  }
+  tm.sync();
+  for (int a = tm.rank(); a < NN; a += tm.size()) {
+    const int i = a % N, j = a / N;
+    T dx = D[i] * su[j * N];
+    T dy = D[j] * su[i];
+#pragma unroll
+    for (int m = 1; m < N; m++) {
+      dx = fma(D[i + m * N], su[j * N + m], dx);
+      dy = fma(D[j + m * N], su[m * N + i], dy);
+    }
+    const T mass = W[j] * W[i] * J;
+    sgx[a] = mass * (dx * (X0 * X0));
+    sgy[a] = mass * (dy * (X1 * X1));
+  }
+  tm.sync();
+  for (int a = tm.rank(); a < NN; a += tm.size()) {
+    const int i = a % N, j = a / N;
+    T ox = D[i * N] * sgx[j * N];
+    T oy = D[j * N] * sgy[i];
+#pragma unroll
+    for (int m = 1; m < N; m++) {
+      ox = fma(D[m + i * N], sgx[j * N + m], ox);
+      oy = fma(D[m + j * N], sgy[m * N + i], oy);
+    }
+    T o = ox + oy;
+    o *= p;
+    T mu = W[j] * W[i] * J * su[a];
+    mu *= q;
+    o += mu;
+    out[e * NN + a] = o;
+  }
+}
+
+struct LdW {  // FP32 search direction
+  const float *w;
+  __device__ __forceinline__ float operator()(int64_t c) const { return w[c]; }
+};
+struct LdX {  // FP64 solution plus the FP32 correction not yet added
+  const double *x;
+  const float *d;
+  __device__ __forceinline__ double operator()(int64_t c) const { return x[c] + (double)d[c]; }
+};
+
+template <int N>
+__device__ void en_cg_elem(const LaneTeam &tm, const EnMember &M, int64_t e, int mode,
+                           const float *Df, const float *Wf, const double *Dd, const double *Wd,
+                           void *slice, double p, double q) {
+  if (mode == EN_INNER)
+    en_box_apply<float, N>(tm, M, e, Df, Wf, (float *)slice, LdW{M.w32}, (float)p, (float)q,
+                           (float *)M.aE);
+  else
+    en_box_apply<double, N>(tm, M, e, Dd, Wd, (double *)slice, LdX{M.xL, M.dL}, p, q, M.aE);
+}
+
+// words (doubles) of a CG warp's basis region: D and W in FP64 and FP32
+__host__ __device__ __forceinline__ int en_cg_basis_doubles(int N) {
+  return en_basis_words<double>(N) + (en_basis_words<float>(N) + 1) / 2;
+}
+
+__device__ void en_cg_elements(const EnArgs &a, const int64_t *cpref, const int *mode) {
+  extern __shared__ __align__(16) unsigned char en_smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  double *ws = reinterpret_cast<double *>(en_smem + (size_t)wib * a.wbytes);
+  const int64_t nw = (int64_t)gridDim.x * wpb;
+  int cur = -1;
+  for (int64_t ch = (int64_t)blockIdx.x * wpb + wib; ch < a.nchunk; ch += nw) {
+    const int mi = en_find(cpref, a.nmem, ch);
+    const int md = a.all_inner ? EN_INNER : mode[mi];
+    if (md == EN_DONE) continue;  // warp-uniform
+    const EnMember &M = a.mem[mi];
+    const int N = M.N;
+    double *Dd = ws, *Wd = ws + N * N;
+    float *Df = reinterpret_cast<float *>(ws + en_basis_words<double>(N)), *Wf = Df + N * N;
+    if (mi != cur) {
+      for (int i = lane; i < N * N; i += 32) {
+        Dd[i] = M.D[i];
+        Df[i] = (float)M.D[i];
+      }
+      for (int i = lane; i < N; i += 32) {
+        Wd[i] = M.W[i];
+        Wf[i] = (float)M.W[i];
+      }
+      __syncwarp();
+      cur = mi;
+    }
+    const int team = M.team, tid = lane / team;
+    const int64_t e = (ch - M.chunk0) * M.epw + tid;
+    if (e < M.ne) {
+      const LaneTeam tm{lane - tid * team, team, team_mask(team, tid)};
+      void *slice = ws + en_cg_basis_doubles(N) + (size_t)tid * 3 * N * N;
+      switch (N) {
+        case 3: en_cg_elem<3>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 4: en_cg_elem<4>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 5: en_cg_elem<5>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 6: en_cg_elem<6>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 7: en_cg_elem<7>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 8: en_cg_elem<8>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 9: en_cg_elem<9>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        default: en_cg_elem<10>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Block partials: every warp folds its lanes (fixed tree), then the warps'
+// values are folded in warp order; partials[(mi*2 + k)*gridDim.x + block].
+__device__ __forceinline__ double en_warp_fold(double v, bool max) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = max ? fmax(v, w) : v + w;
+  }
+  return v;
+}
+
+struct EnAcc {  // per-member, per-warp partials in shared memory
+  double v[EN_MAXMEM][2][EN_MAXWARPS];
+};
+
+__device__ __forceinline__ void en_acc_put(EnAcc &s, int mi, double a0, double a1, bool max1) {
+  a0 = en_warp_fold(a0, false);
+  a1 = en_warp_fold(a1, max1);
+  if ((threadIdx.x & 31) == 0) {
+    s.v[mi][0][threadIdx.x >> 5] = a0;
+    s.v[mi][1][threadIdx.x >> 5] = a1;
+  }
+}
+
+__device__ void en_acc_publish(const EnArgs &a, EnAcc &s, const int *active, bool max1) {
+  __syncthreads();
+  const int wpb = blockDim.x >> 5;
+  for (int t = threadIdx.x; t < 2 * a.nmem; t += blockDim.x) {
+    const int mi = t >> 1, k = t & 1;
+    if (!active[mi]) continue;
+    double v = s.v[mi][k][0];
+    for (int w = 1; w < wpb; w++) v = (k == 1 && max1) ? fmax(v, s.v[mi][k][w]) : v + s.v[mi][k][w];
+    a.partials[(int64_t)(mi * 2 + k) * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+// In the last block: the two totals of member mi (one warp), valid in all
+// lanes.
+__device__ __forceinline__ void en_acc_total(const EnArgs &a, int mi, bool max1, double &t0,
+                                             double &t1) {
+  const int lane = threadIdx.x & 31;
+  double v0 = 0.0, v1 = 0.0;
+  const volatile double *p0 = a.partials + (int64_t)(mi * 2) * gridDim.x;
+  const volatile double *p1 = p0 + gridDim.x;
+  for (int b = lane; b < (int)gridDim.x; b += 32) {
+    v0 += p0[b];
+    v1 = max1 ? fmax(v1, p1[b]) : v1 + p1[b];
+  }
+  t0 = en_warp_fold(v0, false);
+  t1 = en_warp_fold(v1, max1);
+}
+
+__device__ __forceinline__ double en_norm(const EnArgs &a, const EnCG &s, double t) {
+  return a.normtype == GF_NORM_INF ? t : sqrt(t / s.nd);
+}
+
+__device__ __forceinline__ void en_slice(int64_t nL, int64_t &lo, int64_t &hi) {
+  lo = nL * blockIdx.x / gridDim.x;
+  hi = nL * (blockIdx.x + 1) / gridDim.x;
+}
+
+__device__ __forceinline__ double en_nterm(bool inf, int cnt, double r) {
+  return inf ? fabs(r) : (double)cnt * r * r;
+}
+
+// One CG iteration of every member still running (see the file comment).
+__global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1];
+  __shared__ int s_mode[EN_MAXMEM], s_act[EN_MAXMEM];
+  __shared__ EnAcc s_acc;
+  en_load_pref(a.chunk_pref, s_cpref, a.nmem);
+  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) {
+    s_mode[i] = __ldcg(&a.cg[i].next);
+    s_act[i] = s_mode[i] != EN_DONE;
+  }
+  __syncthreads();
+  const bool inf = a.normtype == GF_NORM_INF;
+  // 1. element applies: INNER q_E = A w (FP32); REFINE a_E = A (x + d) (FP64)
+  en_cg_elements(a, s_cpref, s_mode);
+  en_barrier(a.ctl, NoWork{});
+  // 2. assembly: INNER q = mask DSS_Sum(q_E), <w, q>; REFINE x += d,
+  //    r = mask (b_L - DSS_Sum(a_E)), norm(r)
+  for (int mi = 0; mi < a.nmem; mi++) {
+    if (!s_act[mi]) continue;
+    const EnMember &M = a.mem[mi];
+    int64_t lo, hi;
+    en_slice(M.nL, lo, hi);
+    double a0 = 0.0, a1 = 0.0;
+    if (s_mode[mi] == EN_INNER) {
+      const float *qE = (const float *)M.aE;
+      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+        const BoxCopies k = M.walk.copies((int)c);
+        float s = 0.f;
+        k.each([&](int m) { s = __fadd_rn(s, __ldcg(qE + m)); });
+        const float qv = (!M.maskL8 || M.maskL8[c]) ? s : 0.f;
+        M.q32[c] = qv;
+        a0 += (double)M.w32[c] * (double)qv;
+      }
+    } else {
+      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+        const BoxCopies k = M.walk.copies((int)c);
+        double s = 0.0;
+        k.each([&](int m) { s = __dadd_rn(s, __ldcg(M.aE + m)); });
+        M.xL[c] = M.xL[c] + (double)M.dL[c];
+        M.dL[c] = 0.f;
+        const double r = (!M.maskL8 || M.maskL8[c]) ? M.bL[c] - s : 0.0;
+        M.r64[c] = r;
+        a1 = inf ? fmax(a1, fabs(r)) : a1 + en_nterm(false, k.count(), r);
+      }
+    }
+    en_acc_put(s_acc, mi, a0, a1, inf);
+  }
+  en_acc_publish(a, s_acc, s_act, inf);
+  en_barrier(a.ctl, [&] {
+    const int wpb = blockDim.x >> 5, wib = threadIdx.x >> 5;
+    for (int mi = wib; mi < a.nmem; mi += wpb) {
+      if (!s_act[mi]) continue;
+      double t0, t1;
+      en_acc_total(a, mi, inf, t0, t1);
+      if ((threadIdx.x & 31) != 0) continue;
+      EnCG &S = a.cg[mi];
+      if (s_mode[mi] == EN_INNER) {
+        S.alpha = S.rho / t0;
+        if (!isfinite(S.alpha)) {
+          S.status = 2;
+          S.next = EN_DONE;
+        }
+      } else {
+        const double rn = en_norm(a, S, t1);
+        S.rnorm64 = rn;
+        S.sweeps++;
+        if (!isfinite(rn)) {
+          S.status = 2;
+          S.next = EN_DONE;
+        } else if (rn <= S.rtol) {
+          S.status = 0;
+          S.next = EN_DONE;
+        } else if (S.iters >= a.maxit || S.sweeps > a.max_refine) {
+          S.status = 1;
+          S.next = EN_DONE;
+        }
+      }
+    }
+  });
+  // 3. INNER: d += alpha w, r -= alpha q, z = Dinv r, <r, z>, norm(r);
+  //    REFINE (not converged): r32 = r, w = z = Dinv r, <r, z>, norm(r)
+  for (int mi = 0; mi < a.nmem; mi++) {
+    if (!s_act[mi]) continue;
+    const EnMember &M = a.mem[mi];
+    const EnCG &S = a.cg[mi];
+    if (__ldcg(&S.next) == EN_DONE) {
+      if (threadIdx.x == 0) s_act[mi] = 0;  // read again only after the next __syncthreads
+      continue;
+    }
+    int64_t lo, hi;
+    en_slice(M.nL, lo, hi);
+    double a0 = 0.0, a1 = 0.0;
+    if (s_mode[mi] == EN_INNER) {
+      const float al = (float)__ldcg(&S.alpha);
+      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+        const float wv = M.w32[c];
+        M.dL[c] = fmaf(al, wv, M.dL[c]);
+        const float r = fmaf(-al, M.q32[c], M.r32[c]);
+        M.r32[c] = r;
+        const float z = M.dinv32[c] * r;
+        a0 += (double)r * (double)z;
+        const int cnt = inf ? 1 : M.walk.copies((int)c).count();
+        a1 = inf ? fmax(a1, fabs((double)r)) : a1 + en_nterm(false, cnt, (double)r);
+      }
+    } else {
+      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+        const float r = (float)M.r64[c];
+        M.r32[c] = r;
+        const float z = M.dinv32[c] * r;
+        M.w32[c] = z;
+        a0 += (double)r * (double)z;
+        const int cnt = inf ? 1 : M.walk.copies((int)c).count();
+        a1 = inf ? fmax(a1, fabs((double)r)) : a1 + en_nterm(false, cnt, (double)r);
+      }
+    }
+    en_acc_put(s_acc, mi, a0, a1, inf);
+  }
+  __syncthreads();
+  en_acc_publish(a, s_acc, s_act, inf);
+  en_barrier(a.ctl, [&] {
+    const int wpb = blockDim.x >> 5, wib = threadIdx.x >> 5;
+    for (int mi = wib; mi < a.nmem; mi += wpb) {
+      if (!s_act[mi]) continue;
+      double t0, t1;
+      en_acc_total(a, mi, inf, t0, t1);
+      if ((threadIdx.x & 31) != 0) continue;
+      EnCG &S = a.cg[mi];
+      const double rn = en_norm(a, S, t1);
+      if (s_mode[mi] == EN_INNER) {
+        S.beta = t0 / S.rho;
+        S.rho = t0;
+        S.rnorm = rn;
+        S.iters++;
+        if (!isfinite(S.beta) || !isfinite(rn)) {
+          S.status = 2;
+          S.next = EN_DONE;
+        } else if (rn <= S.itol || S.iters >= a.maxit) {
+          S.next = EN_REFINE;
+        }
+      } else {
+        S.rho = t0;
+        S.rnorm = rn;
+        S.itol = fmax(a.inner_tol * rn, 0.25 * S.rtol);
+        S.next = (rn > 0.0 && isfinite(t0)) ? EN_INNER : EN_REFINE;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int mi = 0; mi < a.nmem; mi++) any |= (a.cg[mi].next != EN_DONE);
+      a.ctl->any_active = any;
+      a.ctl->launches++;
+    }
+  });
+  // 4. INNER: w = Dinv r + beta w
+  for (int mi = 0; mi < a.nmem; mi++) {
+    if (!s_act[mi] || s_mode[mi] != EN_INNER) continue;
+    const EnMember &M = a.mem[mi];
+    const float be = (float)__ldcg(&a.cg[mi].beta);
+    int64_t lo, hi;
+    en_slice(M.nL, lo, hi);
+    for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x)
+      M.w32[c] = fmaf(be, M.w32[c], M.dinv32[c] * M.r32[c]);
+  }
+  if (a.has_cond && blockIdx.x == 0 && threadIdx.x == 0) {
+    const bool more = __ldcg(&a.ctl->any_active) && !ld_acquire(&a.ctl->err) &&
+                      ld_acquire(&a.ctl->launches) < a.launch_cap;
+    cudaGraphSetConditional(a.cond, more ? 1u : 0u);
+  }
+}
+
+// Solve setup: b_L = DSS_Sum(b_E), x_L from x_E, the Jacobi inverse of the
+// assembled diagonal, norm(b) on the element-local b, the stop threshold.
+__global__ void __launch_bounds__(512) k_en_cg_init(EnArgs a) {
+  __shared__ int s_act[EN_MAXMEM];
+  __shared__ EnAcc s_acc;
+  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) s_act[i] = 1;
+  __syncthreads();
+  const bool inf = a.normtype == GF_NORM_INF;
+  for (int mi = 0; mi < a.nmem; mi++) {
+    const EnMember &M = a.mem[mi];
+    const int N = M.N, NN = N * N;
+    int64_t lo, hi;
+    en_slice(M.nL, lo, hi);
+    double a1 = 0.0;
+    for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+      const BoxCopies k = M.walk.copies((int)c);
+      double s = 0.0, dg = 0.0, x0 = 0.0;
+      bool first = true;
+      k.each([&](int m) {
+        const double bv = M.bE[m];
+        s = __dadd_rn(s, bv);
+        a1 = inf ? fmax(a1, fabs(bv)) : a1 + bv * bv;
+        if (first) x0 = M.xE[m];
+        first = false;
+        const int64_t e = m / NN;
+        const int loc = (int)(m - e * NN), i = loc % N, j = loc / N;
+        const double X0 = M.egeom64[e * 3], X1 = M.egeom64[e * 3 + 1], J = M.egeom64[e * 3 + 2];
+        dg += a.p * (X0 * X0 * J * M.W[j] * M.K1d[i] + X1 * X1 * J * M.W[i] * M.K1d[j]) +
+              a.q * J * M.W[i] * M.W[j];
+      });
+      M.bL[c] = s;
+      M.xL[c] = x0;
+      M.dL[c] = 0.f;
+      M.w32[c] = 0.f;
+      const double di = dg != 0.0 ? 1.0 / dg : 1.0;
+      M.dinv64[c] = di;
+      M.dinv32[c] = (float)di;
+    }
+    en_acc_put(s_acc, mi, 0.0, a1, inf);
+  }
+  en_acc_publish(a, s_acc, s_act, inf);
+  en_barrier(a.ctl, [&] {
+    const int wpb = blockDim.x >> 5, wib = threadIdx.x >> 5;
+    for (int mi = wib; mi < a.nmem; mi += wpb) {
+      double t0, t1;
+      en_acc_total(a, mi, inf, t0, t1);
+      if ((threadIdx.x & 31) != 0) continue;
+      EnCG &S = a.cg[mi];
+      S.bnorm = en_norm(a, S, t1);
+      S.rtol = (a.relative || S.bnorm >= 1.0) ? a.tol * S.bnorm : a.tol;
+      S.next = EN_REFINE;
+      S.iters = S.sweeps = S.status = 0;
+      S.rho = S.alpha = S.beta = 0.0;
+      S.rnorm = S.rnorm64 = S.bnorm;
+    }
+    if (threadIdx.x == 0) {
+      a.ctl->any_active = 1;
+      a.ctl->launches = 0;
+    }
+  });
+}
+
+// x_E = x_L at every element-local node (one thread per node).
+__global__ void k_en_cg_finish(EnArgs a) {
+  for (int mi = 0; mi < a.nmem; mi++) {
+    const EnMember &M = a.mem[mi];
+    const int N = M.N, NN = N * N, P = N - 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M.nlocal;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t e = i / NN;
+      const int loc = (int)(i - e * NN);
+      const int ey = (int)(e / M.ne0), ex = (int)(e - (int64_t)ey * M.ne0);
+      int gx = ex * P + loc % N, gy = ey * P + loc / N;
+      if (M.walk.per[0] && gx == M.walk.M[0]) gx = 0;
+      if (M.walk.per[1] && gy == M.walk.M[1]) gy = 0;
+      M.xE[i] = M.xL[(int64_t)gy * M.walk.M[0] + gx];
+    }
+  }
+}
+
+// element phase alone, every member INNER (the autotuner's timing kernel)
+__global__ void __launch_bounds__(512) k_en_cg_tune(EnArgs a) {
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1];
+  __shared__ int s_mode[EN_MAXMEM];
+  en_load_pref(a.chunk_pref, s_cpref, a.nmem);
+  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) s_mode[i] = EN_INNER;
+  __syncthreads();
+  en_cg_elements(a, s_cpref, s_mode);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct EnShape {
+  int threads = 256, bps = 0;  // bps 0: as many as fit
+  int team[EN_MAXN + 1];       // lanes per element, by point count
+  bool tuned = false;
+  EnShape() {
+    for (int n = 0; n <= EN_MAXN; n++) team[n] = n * n <= 16 ? 8 : (n * n <= 48 ? 16 : 32);
+  }
+};
+
+struct gf_ensemble {
+  gf_context *ctx = nullptr;
+  std::vector<gf_problem *> probs;
+  int kind = -1;  // GF_ENS_RK or GF_ENS_CG, fixed by the members
+  EnShape shape[3];  // RK FP64, RK FP32, CG
+  std::vector<EnMember> host;
+  EnMember *mem_d = nullptr;
+  int64_t *pref_d = nullptr;  // chunk prefix, then class prefix
+  EnCtl *ctl_d = nullptr;
+  EnCtl *ctl_h = nullptr;  // pinned
+  EnCG *cg_d = nullptr;
+  EnCG *cg_h = nullptr;  // pinned
+  double *partials = nullptr;
+  size_t partials_n = 0;
+  std::vector<void *> bufs;  // per-member device buffers
+  size_t buf_key = 0;        // dtype/kind the buffers were made for
+  cudaStream_t cs = nullptr;  // capture stream
+  // cached graphs: RK (1 and 2 steps) per dtype, CG loop
+  cudaGraphExec_t rk_exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int rk_key[2][2][3] = {};  // ns, threads, blocks
+  double rk_nu_key[2][2] = {};  // nu (held in the captured arguments)
+  cudaGraphExec_t cg_exec = nullptr;
+  int cg_key[2] = {};
+  double cg_pkey[5] = {};  // p, q, tol, inner_tol, relative|normtype|maxit|max_refine
+  int rk_eqn = -1;         // equation of the last RK advance (the tuner runs it)
+  double rk_nu = 0.0;
+  bool cooperative = true;
+  uint64_t launches = 0;
+  int last_grid = 0;
+};
+
+namespace {
+
+int en_cap_bytes(gf_ensemble *E, int which, int team_override_n = -1, int team_override = 0) {
+  // dynamic shared bytes per warp for shape `which`
+  size_t wb = 0;
+  for (size_t m = 0; m < E->probs.size(); m++) {
+    const gf_problem *p = E->probs[m];
+    const int N = p->n;
+    int team = E->shape[which].team[N];
+    if (N == team_override_n) team = team_override;
+    const int epw = 32 / team;
+    size_t b;
+    if (which == 2)
+      b = sizeof(double) * (en_cg_basis_doubles(N) + (size_t)epw * 3 * N * N);
+    else if (which == 0)
+      b = sizeof(double) * (en_basis_words<double>(N) + (size_t)epw * 5 * N * N);
+    else
+      b = sizeof(float) * (en_basis_words<float>(N) + (size_t)epw * 5 * N * N);
+    wb = std::max(wb, b);
+  }
+  return (int)((wb + 15) / 16 * 16);
+}
+
+const void *en_kernel(int which) {
+  if (which == 0) return (const void *)k_en_rk_stage<double>;
+  if (which == 1) return (const void *)k_en_rk_stage<float>;
+  return (const void *)k_en_cg_iter;
+}
+
+// Blocks of the cooperative grid for shape `which` (0 if it does not fit).
+int en_grid(gf_ensemble *E, int which, int threads, int bps, int wbytes) {
+  const void *k = en_kernel(which);
+  const size_t smem = (size_t)wbytes * (threads / 32);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  // the tuning kernel runs the same shape; the CG setup kernel is launched
+  // cooperatively on the same grid, so it must fit as well
+  const void *other = which == 0   ? (const void *)k_en_rk_tune<double>
+                      : which == 1 ? (const void *)k_en_rk_tune<float>
+                                   : (const void *)k_en_cg_init;
+  if (cudaFuncSetAttribute(other, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (which == 2) {
+    cudaFuncSetAttribute((const void *)k_en_cg_tune, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    int occ2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, other, threads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    occ = std::min(occ, occ2);
+  }
+  if (occ < 1) return 0;
+  const int b = bps > 0 ? std::min(bps, occ) : occ;
+  return b * E->ctx->sm_count;
+}
+
+// Chunk and class numbering for shape `which`; fills descriptor offsets and
+// the prefix arrays (host), returns totals.
+void en_layout(gf_ensemble *E, int which, std::vector<int64_t> &cpref, std::vector<int64_t> &kpref,
+               int64_t &nchunk, int64_t &nclass) {
+  const int n = (int)E->probs.size();
+  cpref.assign(n + 1, 0);
+  kpref.assign(n + 1, 0);
+  nchunk = nclass = 0;
+  for (int m = 0; m < n; m++) {
+    EnMember &M = E->host[m];
+    M.team = E->shape[which].team[M.N];
+    M.epw = 32 / M.team;
+    M.chunk0 = nchunk;
+    M.nchunk = (M.ne + M.epw - 1) / M.epw;
+    M.class0 = nclass;
+    cpref[m] = nchunk;
+    kpref[m] = nclass;
+    nchunk += M.nchunk;
+    nclass += which == 2 ? M.nL : M.nclass;
+  }
+  cpref[n] = nchunk;
+  kpref[n] = nclass;
+}
+
+int en_upload(gf_ensemble *E, int which, EnArgs &a) {
+  gf_context *ctx = E->ctx;
+  std::vector<int64_t> cp, kp;
+  int64_t nchunk, nclass;
+  en_layout(E, which, cp, kp, nchunk, nclass);
+  const int n = (int)E->probs.size();
+  cudaStream_t st = ctx->stream;
+  GF_CUDA(ctx, cudaMemcpyAsync(E->mem_d, E->host.data(), sizeof(EnMember) * n,
+                               cudaMemcpyHostToDevice, st));
+  GF_CUDA(ctx, cudaMemcpyAsync(E->pref_d, cp.data(), sizeof(int64_t) * (n + 1),
+                               cudaMemcpyHostToDevice, st));
+  GF_CUDA(ctx, cudaMemcpyAsync(E->pref_d + EN_MAXMEM + 1, kp.data(), sizeof(int64_t) * (n + 1),
+                               cudaMemcpyHostToDevice, st));
+  // the host arrays are pageable: finish the copies before they change
+  GF_CUDA(ctx, cudaStreamSynchronize(st));
+  memset(&a, 0, sizeof(a));
+  a.mem = E->mem_d;
+  a.nmem = n;
+  a.chunk_pref = E->pref_d;
+  a.class_pref = E->pref_d + EN_MAXMEM + 1;
+  a.nchunk = nchunk;
+  a.nclass = nclass;
+  a.ctl = E->ctl_d;
+  a.cg = E->cg_d;
+  a.partials = E->partials;
+  a.wbytes = en_cap_bytes(E, which);
+  return GF_OK;
+}
+
+cudaError_t en_launch(gf_ensemble *E, const void *k, int grid, int threads, size_t smem,
+                      cudaStream_t st, void **args, bool coop) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = coop ? at : nullptr;
+  cfg.numAttrs = coop ? 1 : 0;
+  E->launches++;
+  return cudaLaunchKernelExC(&cfg, k, args);
+}
+
+int en_check_partials(gf_ensemble *E, int grid) {
+  const size_t need = (size_t)2 * EN_MAXMEM * std::max(grid, 1);
+  if (E->partials_n >= need) return GF_OK;
+  if (E->partials) cudaFree(E->partials);
+  E->partials = nullptr;
+  GF_CUDA(E->ctx, cudaMalloc(&E->partials, sizeof(double) * need));
+  E->partials_n = need;
+  return GF_OK;
+}
+
+void en_drop_graphs(gf_ensemble *E) {
+  for (auto &row : E->rk_exec)
+    for (auto &g : row)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  if (E->cg_exec) {
+    cudaGraphExecDestroy(E->cg_exec);
+    E->cg_exec = nullptr;
+  }
+}
+
+void en_free_bufs(gf_ensemble *E) {
+  for (void *b : E->bufs) cudaFree(b);
+  E->bufs.clear();
+  E->buf_key = 0;
+}
+
+void *en_alloc(gf_ensemble *E, size_t bytes) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, std::max<size_t>(bytes, 16));
+  E->bufs.push_back(p);
+  return p;
+}
+
+// Scratch vectors of every member: RK (u[1], K[0..2], uf) or CG.
+int en_buffers(gf_ensemble *E, int which) {
+  const size_t key = (size_t)which + 1;
+  if (E->buf_key == key) return GF_OK;
+  en_drop_graphs(E);
+  en_free_bufs(E);
+  for (size_t m = 0; m < E->probs.size(); m++) {
+    EnMember &M = E->host[m];
+    if (which < 2) {
+      const size_t b = (which == 0 ? sizeof(double) : sizeof(float)) * (size_t)M.nlocal;
+      M.u[1] = en_alloc(E, b);
+      for (int k = 0; k < 3; k++) M.K[k] = en_alloc(E, b);
+      M.uf = en_alloc(E, b);
+      if (!M.u[1] || !M.K[0] || !M.K[1] || !M.K[2] || !M.uf) goto oom;
+    } else {
+      const size_t L = (size_t)M.nL;
+      M.bL = (double *)en_alloc(E, 8 * L);
+      M.xL = (double *)en_alloc(E, 8 * L);
+      M.r64 = (double *)en_alloc(E, 8 * L);
+      M.dinv64 = (double *)en_alloc(E, 8 * L);
+      M.aE = (double *)en_alloc(E, 8 * (size_t)M.nlocal);
+      M.dL = (float *)en_alloc(E, 4 * L);
+      M.r32 = (float *)en_alloc(E, 4 * L);
+      M.w32 = (float *)en_alloc(E, 4 * L);
+      M.q32 = (float *)en_alloc(E, 4 * L);
+      M.dinv32 = (float *)en_alloc(E, 4 * L);
+      if (!M.bL || !M.xL || !M.r64 || !M.dinv64 || !M.aE || !M.dL || !M.r32 || !M.w32 ||
+          !M.q32 || !M.dinv32)
+        goto oom;
+    }
+  }
+  E->buf_key = key;
+  return GF_OK;
+oom:
+  en_free_bufs(E);
+  return gf_fail(E->ctx, GF_ERR_NOMEM, "ensemble scratch allocation failed");
+}
+
+// Time `reps` launches of the tuning kernel of shape `which`; returns ms
+// per launch or a negative value when the shape does not fit.
+float en_time_shape(gf_ensemble *E, int which, int reps) {
+  EnShape &S = E->shape[which];
+  EnArgs a;
+  if (en_upload(E, which, a)) return -1.f;
+  const int grid = en_grid(E, which, S.threads, S.bps, a.wbytes);
+  if (grid <= 0) return -1.f;
+  const void *k = which == 0   ? (const void *)k_en_rk_tune<double>
+                  : which == 1 ? (const void *)k_en_rk_tune<float>
+                               : (const void *)k_en_cg_tune;
+  a.all_inner = 1;
+  a.ns = 1;
+  a.eqn = E->rk_eqn;
+  a.nu = E->rk_nu;
+  void *args[1] = {&a};
+  const size_t smem = (size_t)a.wbytes * (S.threads / 32);
+  cudaStream_t st = E->ctx->stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = -1.f;
+  for (int r = 0; r < reps + 2; r++) {
+    cudaEventRecord(e0, st);
+    if (en_launch(E, k, grid, S.threads, smem, st, args, false) != cudaSuccess) {
+      cudaGetLastError();
+      best = -1.f;
+      break;
+    }
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 2 && (best < 0.f || ms < best)) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+int en_which(int kind, int dtype) {
+  if (kind == GF_ENS_CG) return 2;
+  return dtype == GF_F32 ? 1 : 0;
+}
+
+}  // namespace
+
+extern "C" int gf_ensemble_create(gf_ctx_t ctx, int n, const gf_problem_t *members,
+                                  gf_ensemble_t *out) {
+  if (!ctx || !out) return GF_ERR_ARG;
+  *out = nullptr;
+  GF_REQUIRE(ctx, n >= 1 && n <= EN_MAXMEM && members, "1..%d members", EN_MAXMEM);
+  int kind = -1;
+  for (int m = 0; m < n; m++) {
+    const gf_problem *p = members[m];
+    GF_REQUIRE(ctx, p && p->ctx == ctx, "member %d is not a problem of this context", m);
+    GF_REQUIRE(ctx, p->dim == 2, "member %d: ensembles take 2-d members", m);
+    GF_REQUIRE(ctx, p->n >= EN_MINN && p->n <= EN_MAXN, "member %d: order %d outside 2..%d", m,
+               p->n - 1, EN_MAXN - 1);
+    int k;
+    if (p->geom >= GF_GEOM_DEFORMED) {
+      GF_REQUIRE(ctx, p->dgeom_d && p->dgeom_f && p->gmet_d && p->gmet_f,
+                 "member %d: deformed geometry missing", m);
+      k = GF_ENS_RK;
+    } else {
+      BoxWalk w{};
+      GF_REQUIRE(ctx, p->has_box && p->egeom_d && p->egeom_f && dss_box_walk(p, w),
+                 "member %d: CG members are box grids with affine elements", m);
+      k = GF_ENS_CG;
+    }
+    GF_REQUIRE(ctx, kind < 0 || kind == k,
+               "members mix deformed (RK) and box (CG) problems; make one ensemble of each");
+    kind = k;
+  }
+  gf_ensemble *E = new gf_ensemble;
+  E->ctx = ctx;
+  E->kind = kind;
+  E->probs.assign(members, members + n);
+  E->host.resize(n);
+  for (int m = 0; m < n; m++) {
+    gf_problem *p = members[m];
+    EnMember &M = E->host[m];
+    memset(&M, 0, sizeof(M));
+    M.N = p->n;
+    M.nxy = p->nxy ? p->nxy : p->dim;
+    M.ne = p->ne;
+    M.nlocal = p->nlocal;
+    M.nclass = p->nclass;
+    for (int i = 0; i < M.N * M.N; i++) M.D[i] = p->D[i];
+    for (int i = 0; i < M.N; i++) {
+      M.W[i] = p->W[i];
+      M.K1d[i] = p->K1[i + i * M.N];
+    }
+    M.class_ptr = p->class_ptr;
+    M.members = p->members;
+    if (kind == GF_ENS_RK) {
+      M.X[0] = p->dgeom_d;
+      M.X[1] = p->dgeom_f;
+      M.G[0] = p->gmet_d;
+      M.G[1] = p->gmet_f;
+      M.J[0] = p->ngeom_d + (int64_t)p->dim * p->nlocal;
+      M.J[1] = p->ngeom_f + (int64_t)p->dim * p->nlocal;
+      M.imass[0] = p->imass_d;
+      M.imass[1] = p->imass_f;
+    } else {
+      M.walk = BoxWalk::make(p->box);
+      M.ne0 = p->box.ne[0];
+      M.nL = p->box.size();
+      M.maskL8 = p->maskL8;
+      M.egeom64 = p->egeom_d;
+      M.egeom32 = p->egeom_f;
+    }
+  }
+  cudaError_t e = cudaMalloc(&E->mem_d, sizeof(EnMember) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&E->pref_d, sizeof(int64_t) * 2 * (EN_MAXMEM + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&E->ctl_d, sizeof(EnCtl));
+  if (e == cudaSuccess) e = cudaMalloc(&E->cg_d, sizeof(EnCG) * EN_MAXMEM);
+  if (e == cudaSuccess) e = cudaMallocHost(&E->ctl_h, sizeof(EnCtl));
+  if (e == cudaSuccess) e = cudaMallocHost(&E->cg_h, sizeof(EnCG) * EN_MAXMEM);
+  if (e == cudaSuccess) e = cudaMemset(E->ctl_d, 0, sizeof(EnCtl));
+  if (e == cudaSuccess) e = cudaMemset(E->cg_d, 0, sizeof(EnCG) * EN_MAXMEM);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    gf_ensemble_destroy(E);
+    return gf_fail(ctx, GF_ERR_NOMEM, "ensemble allocation failed: %s", cudaGetErrorString(e));
+  }
+  ctx->nprob++;
+  *out = E;
+  return GF_OK;
+}
+
+extern "C" int gf_ensemble_destroy(gf_ensemble_t E) {
+  if (!E) return GF_OK;
+  en_drop_graphs(E);
+  en_free_bufs(E);
+  if (E->mem_d) cudaFree(E->mem_d);
+  if (E->pref_d) cudaFree(E->pref_d);
+  if (E->ctl_d) cudaFree(E->ctl_d);
+  if (E->cg_d) cudaFree(E->cg_d);
+  if (E->partials) cudaFree(E->partials);
+  if (E->ctl_h) cudaFreeHost(E->ctl_h);
+  if (E->cg_h) cudaFreeHost(E->cg_h);
+  if (E->cs) cudaStreamDestroy(E->cs);
+  if (E->ctx && E->mem_d) E->ctx->nprob--;
+  delete E;
+  return GF_OK;
+}
+
+extern "C" int gf_ensemble_kind(gf_ensemble_t E) { return E ? E->kind : GF_ERR_ARG; }
+
+extern "C" uint64_t gf_ensemble_launches(gf_ensemble_t E) { return E ? E->launches : 0; }
+
+extern "C" int gf_ensemble_shape(gf_ensemble_t E, int dtype, int *threads, int *blocks,
+                                 int *team_by_n, int *tuned) {
+  if (!E) return GF_ERR_ARG;
+  const int w = en_which(E->kind, dtype);
+  const EnShape &S = E->shape[w];
+  if (threads) *threads = S.threads;
+  if (blocks) *blocks = en_grid(E, w, S.threads, S.bps, en_cap_bytes(E, w));
+  if (team_by_n)
+    for (int n = 0; n <= EN_MAXN; n++) team_by_n[n] = S.team[n];
+  if (tuned) *tuned = S.tuned ? 1 : 0;
+  return GF_OK;
+}
+
+extern "C" int gf_ensemble_set_shape(gf_ensemble_t E, int dtype, int threads, int bps,
+                                     const int *team_by_n) {
+  if (!E) return GF_ERR_ARG;
+  gf_context *ctx = E->ctx;
+  GF_REQUIRE(ctx, threads == 64 || threads == 128 || threads == 256 || threads == 512,
+             "threads per block: 64, 128, 256 or 512");
+  GF_REQUIRE(ctx, bps >= 0 && bps <= 32, "blocks per SM: 0 (as many as fit) .. 32");
+  const int w = en_which(E->kind, dtype);
+  EnShape S = E->shape[w];
+  S.threads = threads;
+  S.bps = bps;
+  if (team_by_n)
+    for (int n = EN_MINN; n <= EN_MAXN; n++) {
+      GF_REQUIRE(ctx, team_by_n[n] == 8 || team_by_n[n] == 16 || team_by_n[n] == 32,
+                 "team widths are 8, 16 or 32 lanes");
+      S.team[n] = team_by_n[n];
+    }
+  const EnShape old = E->shape[w];
+  E->shape[w] = S;
+  if (en_grid(E, w, S.threads, S.bps, en_cap_bytes(E, w)) <= 0) {
+    E->shape[w] = old;
+    return gf_fail(ctx, GF_ERR_ARG, "shape does not fit on the device");
+  }
+  en_drop_graphs(E);
+  return GF_OK;
+}
+
+// The autotuner: coordinate search over threads x blocks per SM, then the
+// team width of each order present, each candidate timed on the element
+// phase of this ensemble (best of `reps` launches).
+extern "C" int gf_ensemble_tune(gf_ensemble_t E, int dtype, int reps) {
+  if (!E) return GF_ERR_ARG;
+  gf_context *ctx = E->ctx;
+  const int w = en_which(E->kind, dtype);
+  GF_REQUIRE(ctx, E->kind == GF_ENS_CG || dtype == GF_F32 || dtype == GF_F64, "bad dtype");
+  if (reps < 1) reps = 5;
+  int rc = en_buffers(E, w);
+  if (rc) return rc;
+  // The timing kernels read and write the ensemble's own scratch only: an
+  // RK member's stage input is its scratch state u[1] and its velocity
+  // components are scratch slopes (the element work does not depend on the
+  // values); a CG member's search direction is its scratch w.  The caller's
+  // buffers are restored afterwards.
+  std::vector<EnMember> saved = E->host;
+  if (E->kind == GF_ENS_RK) {
+    for (auto &M : E->host) {
+      M.u[0] = M.u[1];
+      M.c[0] = M.K[1];
+      M.c[1] = M.K[2];
+      M.c[2] = M.uf;
+    }
+    if (E->rk_eqn < 0) E->rk_eqn = GF_EQN_ADVECT;
+  }
+  EnShape &S = E->shape[w];
+  EnShape best = S;
+  float tbest = en_time_shape(E, w, reps);
+  const int thr[4] = {64, 128, 256, 512};
+  const int bps[4] = {1, 2, 4, 0};
+  for (int ti = 0; ti < 4; ti++)
+    for (int bi = 0; bi < 4; bi++) {
+      S = best;
+      S.threads = thr[ti];
+      S.bps = bps[bi];
+      const float t = en_time_shape(E, w, reps);
+      if (t > 0.f && (tbest < 0.f || t < tbest)) {
+        tbest = t;
+        best = S;
+      }
+    }
+  bool seen[EN_MAXN + 1] = {};
+  for (auto *p : E->probs) seen[p->n] = true;
+  const int teams[3] = {8, 16, 32};
+  for (int n = EN_MINN; n <= EN_MAXN; n++) {
+    if (!seen[n]) continue;
+    for (int k = 0; k < 3; k++) {
+      S = best;
+      S.team[n] = teams[k];
+      const float t = en_time_shape(E, w, reps);
+      if (t > 0.f && (tbest < 0.f || t < tbest)) {
+        tbest = t;
+        best = S;
+      }
+    }
+  }
+  best.tuned = true;
+  S = best;
+  E->host = saved;
+  en_drop_graphs(E);
+  if (tbest < 0.f) return gf_fail(ctx, GF_ERR_CUDA, "no ensemble shape could be launched");
+  return GF_OK;
+}
+
+// ---- RK --------------------------------------------------------------------
+extern "C" int gf_ensemble_rk_advance(gf_ensemble_t E, int dtype, const gf_rk_traits *tr,
+                                      void *const *u, const void *const *c, const double *dt,
+                                      int nsteps) {
+  if (!E) return GF_ERR_ARG;
+  gf_context *ctx = E->ctx;
+  GF_REQUIRE(ctx, E->kind == GF_ENS_RK, "this ensemble holds CG (box) members");
+  GF_REQUIRE(ctx, tr && u && dt && nsteps >= 0, "traits, u and dt are required");
+  GF_REQUIRE(ctx, dtype == GF_F32 || dtype == GF_F64, "unknown dtype %d", dtype);
+  GF_REQUIRE(ctx, tr->eqn == GF_EQN_ADVECT || tr->eqn == GF_EQN_HEAT,
+             "ensemble RK evolves advection or heat members");
+  GF_REQUIRE(ctx, tr->nstate == 1, "one state component per member");
+  GF_REQUIRE(ctx, tr->scheme >= GF_RK1 && tr->scheme <= GF_RK4, "ensemble RK runs step_b (RK1..RK4)");
+  GF_REQUIRE(ctx, tr->eqn != GF_EQN_ADVECT || c, "advection needs the members' velocities");
+  const int n = (int)E->probs.size();
+  for (int m = 0; m < n; m++) {
+    GF_REQUIRE(ctx, u[m], "member %d: state missing", m);
+    if (tr->eqn == GF_EQN_ADVECT)
+      for (int k = 0; k < E->host[m].nxy; k++)
+        GF_REQUIRE(ctx, c[3 * m + k], "member %d: velocity component %d missing", m, k);
+  }
+  int capturing = 0;
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    GF_CUDA(ctx, cudaStreamIsCapturing(ctx->stream, &cs));
+    capturing = cs != cudaStreamCaptureStatusNone;
+  }
+  GF_REQUIRE(ctx, !capturing, "the ensemble captures its own graphs; call it outside a capture");
+  if (nsteps == 0) return GF_OK;
+  const int w = en_which(GF_ENS_RK, dtype);
+  int rc = en_buffers(E, w);
+  if (rc) return rc;
+  double alpha[4], beta[4][4], cc[4];
+  gfrk::butcher(tr->scheme, alpha, beta, cc);
+  const int ns = tr->scheme;
+  if (E->rk_eqn != tr->eqn) en_drop_graphs(E);
+  E->rk_eqn = tr->eqn;
+  E->rk_nu = tr->nu;
+  for (int m = 0; m < n; m++) {
+    EnMember &M = E->host[m];
+    M.u[0] = u[m];
+    for (int k = 0; k < 3; k++)
+      M.c[k] = (tr->eqn == GF_EQN_ADVECT && k < M.nxy) ? c[3 * m + k] : nullptr;
+    // coefficients rounded as the single-problem stepper rounds them
+    for (int s = 0; s < 4; s++) {
+      for (int j = 0; j < 3; j++) {
+        if (dtype == GF_F32) {
+          const float h = (float)dt[m];
+          M.coef[s][j] = (double)((float)beta[s][j] * h);
+        } else {
+          M.coef[s][j] = beta[s][j] * dt[m];
+        }
+      }
+      M.ch[s] = dtype == GF_F32 ? (double)((float)cc[s] * (float)dt[m]) : cc[s] * dt[m];
+    }
+  }
+  EnArgs a;
+  if ((rc = en_upload(E, w, a))) return rc;
+  const EnShape &S = E->shape[w];
+  const int grid = en_grid(E, w, S.threads, S.bps, a.wbytes);
+  if (grid <= 0) return gf_fail(ctx, GF_ERR_UNSUPPORTED, "ensemble shape does not fit");
+  a.ns = ns;
+  a.eqn = tr->eqn;
+  a.nu = tr->nu;
+  const size_t smem = (size_t)a.wbytes * (S.threads / 32);
+  const void *k = en_kernel(w);
+  cudaStream_t st = ctx->stream;
+  GF_CUDA(ctx, cudaMemsetAsync(E->ctl_d, 0, sizeof(EnCtl), st));
+  // graphs of 2 steps (par 0 then 1) and 1 step (par 0), rebuilt when the
+  // scheme or shape changes; the kernels read the descriptors from device
+  // memory, so the same graph serves any bound state
+  auto build = [&](int steps, cudaGraphExec_t &exec, int *key, double &nukey) -> int {
+    if (exec && key[0] == ns && key[1] == S.threads && key[2] == grid && nukey == tr->nu)
+      return GF_OK;
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    for (int attempt = 0; attempt < 2; attempt++) {
+      const bool coop = E->cooperative;
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(E->cs, cudaStreamCaptureModeRelaxed);
+      for (int s = 0; e == cudaSuccess && s < steps; s++)
+        for (int stg = 0; e == cudaSuccess && stg < ns; stg++) {
+          EnArgs b = a;
+          b.par = s & 1;
+          int sv = stg;
+          void *args[2] = {&b, &sv};
+          e = en_launch(E, k, grid, S.threads, smem, E->cs, args, coop);
+        }
+      cudaError_t e2 = cudaStreamEndCapture(E->cs, &g);
+      if (e == cudaSuccess) e = e2;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e == cudaSuccess) break;
+      cudaGetLastError();
+      exec = nullptr;
+      if (!coop) return gf_fail(ctx, GF_ERR_CUDA, "ensemble graph capture failed: %s",
+                                cudaGetErrorString(e));
+      E->cooperative = false;  // capture without the cooperative attribute
+    }
+    key[0] = ns;
+    key[1] = S.threads;
+    key[2] = grid;
+    nukey = tr->nu;
+    return GF_OK;
+  };
+  const int di = dtype == GF_F32 ? 1 : 0;
+  if (nsteps >= 2 && (rc = build(2, E->rk_exec[di][1], E->rk_key[di][1], E->rk_nu_key[di][1])))
+    return rc;
+  if ((nsteps & 1) && (rc = build(1, E->rk_exec[di][0], E->rk_key[di][0], E->rk_nu_key[di][0])))
+    return rc;
+  for (int s = 0; s + 1 < nsteps; s += 2) GF_CUDA(ctx, cudaGraphLaunch(E->rk_exec[di][1], st));
+  if (nsteps & 1) {
+    GF_CUDA(ctx, cudaGraphLaunch(E->rk_exec[di][0], st));
+    const size_t bytes = (dtype == GF_F32 ? 4 : 8) * 1;
+    for (int m = 0; m < n; m++)
+      GF_CUDA(ctx, cudaMemcpyAsync(E->host[m].u[0], E->host[m].u[1], bytes * E->host[m].nlocal,
+                                   cudaMemcpyDeviceToDevice, st));
+  }
+  E->last_grid = grid;
+  GF_CUDA(ctx, cudaMemcpyAsync(E->ctl_h, E->ctl_d, sizeof(EnCtl), cudaMemcpyDeviceToHost, st));
+  GF_CUDA(ctx, cudaStreamSynchronize(st));
+  if (E->ctl_h->err) return gf_fail(ctx, GF_ERR_CUDA, "ensemble grid barrier timed out");
+  for (int m = 0; m < n; m++)
+    if (E->ctl_h->nonfinite[m])
+      return gf_fail(ctx, GF_ERR_NONFINITE, "member %d: non-finite state after the last step", m);
+  return GF_OK;
+}
+
+// ---- CG --------------------------------------------------------------------
+extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, double p, double q,
+                                    const double *const *b, double *const *x, int *iters,
+                                    double *final_norm, int *status) {
+  if (!E) return GF_ERR_ARG;
+  gf_context *ctx = E->ctx;
+  GF_REQUIRE(ctx, E->kind == GF_ENS_CG, "this ensemble holds RK (deformed) members");
+  GF_REQUIRE(ctx, tr && b && x, "traits, b and x are required");
+  GF_REQUIRE(ctx, tr->precision == GF_CG_MIXED, "ensemble CG runs FP32 iterations with FP64 refinement");
+  GF_REQUIRE(ctx, tr->precond == GF_PRECOND_JACOBI, "ensemble CG takes the Jacobi preconditioner");
+  GF_REQUIRE(ctx, tr->normtype == GF_NORM_EUC || tr->normtype == GF_NORM_INF,
+             "ensemble CG norms: EUC or INF");
+  GF_REQUIRE(ctx, tr->maxit >= 1 && tr->tol > 0.0, "maxit >= 1 and tol > 0");
+  const int n = (int)E->probs.size();
+  for (int m = 0; m < n; m++) GF_REQUIRE(ctx, b[m] && x[m], "member %d: b or x missing", m);
+  int rc = en_buffers(E, 2);
+  if (rc) return rc;
+  for (int m = 0; m < n; m++) {
+    E->host[m].bE = b[m];
+    E->host[m].xE = x[m];
+  }
+  EnArgs a;
+  if ((rc = en_upload(E, 2, a))) return rc;
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    GF_CUDA(ctx, cudaStreamIsCapturing(ctx->stream, &cs));
+    GF_REQUIRE(ctx, cs == cudaStreamCaptureStatusNone,
+               "the ensemble captures its own graphs; call it outside a capture");
+  }
+  const EnShape &S = E->shape[2];
+  const int grid = en_grid(E, 2, S.threads, S.bps, a.wbytes);
+  if (grid <= 0) return gf_fail(ctx, GF_ERR_UNSUPPORTED, "ensemble shape does not fit");
+  if ((rc = en_check_partials(E, grid))) return rc;
+  a.partials = E->partials;
+  a.p = p;
+  a.q = q;
+  a.tol = tr->tol;
+  a.inner_tol = tr->inner_tol > 0.0 ? tr->inner_tol : 1e-4;
+  a.normtype = tr->normtype;
+  a.maxit = tr->maxit;
+  a.max_refine = tr->max_refine > 0 ? tr->max_refine : 64;
+  a.relative = tr->relative;
+  a.launch_cap = (unsigned)std::min<int64_t>(0x7fffffff, 2LL * tr->maxit + 4LL * a.max_refine + 16);
+  for (int m = 0; m < n; m++) {
+    E->cg_h[m] = EnCG{};
+    E->cg_h[m].nd = (double)E->host[m].nlocal;
+  }
+  cudaStream_t st = ctx->stream;
+  GF_CUDA(ctx, cudaMemcpyAsync(E->cg_d, E->cg_h, sizeof(EnCG) * n, cudaMemcpyHostToDevice, st));
+  GF_CUDA(ctx, cudaMemsetAsync(E->ctl_d, 0, sizeof(EnCtl), st));
+  const size_t smem = (size_t)a.wbytes * (S.threads / 32);
+  {
+    void *args[1] = {&a};
+    GF_CUDA(ctx, en_launch(E, (const void *)k_en_cg_init, grid, S.threads, smem, st, args,
+                           E->cooperative));
+  }
+  // the iteration loop: a WHILE node whose body is one cooperative launch;
+  // the kernel's block 0 clears the condition once no member is running
+  // the captured kernel holds p, q and the traits in its arguments
+  const double pkey[5] = {p, q, a.tol, a.inner_tol,
+                          (double)a.relative + 2.0 * a.normtype + 8.0 * a.max_refine +
+                              1024.0 * (double)a.maxit};
+  if (!(E->cg_exec && E->cg_key[0] == S.threads && E->cg_key[1] == grid &&
+        std::equal(pkey, pkey + 5, E->cg_pkey))) {
+    if (E->cg_exec) cudaGraphExecDestroy(E->cg_exec);
+    E->cg_exec = nullptr;
+    for (int attempt = 0; attempt < 2; attempt++) {
+      const bool coop = E->cooperative;
+      cudaGraph_t g = nullptr, body = nullptr;
+      cudaGraphConditionalHandle h = 0;
+      cudaError_t e = cudaGraphCreate(&g, 0);
+      if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+      cudaGraphNodeParams np = {};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+      if (e == cudaSuccess) {
+        body = np.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(E->cs, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed);
+      }
+      if (e == cudaSuccess) {
+        EnArgs b2 = a;
+        b2.cond = h;
+        b2.has_cond = 1;
+        void *args[1] = {&b2};
+        e = en_launch(E, (const void *)k_en_cg_iter, grid, S.threads, smem, E->cs, args, coop);
+        cudaError_t e2 = cudaStreamEndCapture(E->cs, &body);
+        if (e == cudaSuccess) e = e2;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&E->cg_exec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e == cudaSuccess) break;
+      cudaGetLastError();
+      E->cg_exec = nullptr;
+      if (!coop)
+        return gf_fail(ctx, GF_ERR_CUDA, "ensemble CG capture failed: %s", cudaGetErrorString(e));
+      E->cooperative = false;
+    }
+    E->cg_key[0] = S.threads;
+    E->cg_key[1] = grid;
+    std::copy(pkey, pkey + 5, E->cg_pkey);
+  }
+  GF_CUDA(ctx, cudaGraphLaunch(E->cg_exec, st));
+  E->launches++;
+  k_en_cg_finish<<<std::max(1, ctx->sm_count * 4), 256, 0, st>>>(a);
+  GF_CHECK_LAUNCH(ctx);
+  E->last_grid = grid;
+  GF_CUDA(ctx, cudaMemcpyAsync(E->cg_h, E->cg_d, sizeof(EnCG) * n, cudaMemcpyDeviceToHost, st));
+  GF_CUDA(ctx, cudaMemcpyAsync(E->ctl_h, E->ctl_d, sizeof(EnCtl), cudaMemcpyDeviceToHost, st));
+  GF_CUDA(ctx, cudaStreamSynchronize(st));
+  E->launches += E->ctl_h->launches;
+  if (E->ctl_h->err) return gf_fail(ctx, GF_ERR_CUDA, "ensemble grid barrier timed out");
+  int worst = GF_OK;
+  for (int m = 0; m < n; m++) {
+    const EnCG &C = E->cg_h[m];
+    if (iters) iters[m] = C.iters;
+    if (final_norm) final_norm[m] = C.rnorm64;
+    if (status) status[m] = C.status;
+    if (C.status == 2) worst = GF_ERR_NONFINITE;
+    else if (C.status == 1 && worst == GF_OK) worst = GF_CG_NOCONVERGE;
+    if (C.next != EN_DONE && worst == GF_OK) worst = GF_CG_NOCONVERGE;
+  }
+  if (worst == GF_ERR_NONFINITE) return gf_fail(ctx, worst, "ensemble CG breakdown (non-finite)");
+  return worst;
+}

@@ -63,15 +63,8 @@ __global__ void k_stage_sum(int64_t n, const T *__restrict__ uin, int nk, const 
                             const T *__restrict__ K1, const T *__restrict__ K2, T b0, T b1, T b2,
                             T *__restrict__ y) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    T s = T(0);
-    if (nk > 0) s = T(1) * s + b0 * K0[i];
-    if (nk > 1) s = T(1) * s + b1 * K1[i];
-    if (nk > 2) s = T(1) * s + b2 * K2[i];
-    T v = uin[i];
-    v += s;
-    y[i] = v;
-  }
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = rk_stage_point(uin[i], nk, K0, K1, K2, b0, b1, b2, i);
 }
 
 // flag[0] = 1 when any of the nstate fields holds a non-finite value

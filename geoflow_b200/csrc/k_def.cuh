@@ -50,11 +50,28 @@ enum { DEF_HELM = 0, DEF_DUDT = 1, DEF_ADVECT = 2, DEF_DERIV = 3 };
 // mode DEF_HELM: uo = p L u (+ q M u); DEF_DUDT: uo = Minv(-nu L u - adv)
 // (heat when nv == 0); DEF_ADVECT: uo = adv = M sum_k c_k du/dx_k;
 // DEF_DERIV: uo = du/dx_{idir}.  nv velocity components c0..c2.
-// One element e of k_def, by the threads of the block (the body shared by
-// k_def and the ensemble kernels, api_ensemble.cu).  BB is a basis with
-// members D[N*N] and W[N]; smem holds (1 + 2 DIM) N^DIM values of T.
-template <typename T, int N, int DIM, class LD, typename TO, class BB>
-__device__ __forceinline__ void def_element(const BB &B, const DefGeom<T> &g, int64_t e, int mode,
+// The threads that share one element: the whole block (k_def), or a group
+// of lanes of one warp (the ensemble kernels, api_ensemble.cu).
+struct BlockTeam {
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct LaneTeam {
+  int r, n;
+  unsigned mask;  // the team's lanes
+  __device__ __forceinline__ int rank() const { return r; }
+  __device__ __forceinline__ int size() const { return n; }
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+};
+
+// One element e of k_def, by the threads of team tm (the body shared by
+// k_def and the ensemble kernels).  BB is a basis with members D[N*N] and
+// W[N]; smem holds (1 + 2 DIM) N^DIM values of T.  Each node's arithmetic
+// is the same whichever thread of whichever team computes it.
+template <typename T, int N, int DIM, class LD, typename TO, class BB, class TM>
+__device__ __forceinline__ void def_element(const TM &tm, const BB &B, const DefGeom<T> &g,
+                                            int64_t e, int mode,
                                             T p, const T *__restrict__ pvec, T q,
                                             const T *__restrict__ qvec, int use_mass, const LD &ld,
                                             int nv, const T *__restrict__ c0,
@@ -70,20 +87,20 @@ __device__ __forceinline__ void def_element(const BB &B, const DefGeom<T> &g, in
   const int64_t nl = g.nlocal;
   // load
   if (DIM == 3) {
-    for (int ij = threadIdx.x; ij < NN; ij += blockDim.x) {
+    for (int ij = tm.rank(); ij < NN; ij += tm.size()) {
       typename LD::value_type lv[N];
       ld.template zline<N>(e, ij % N, ij / N, lv);
 #pragma unroll
       for (int k = 0; k < N; k++) su[k * NN + ij] = (T)lv[k];
     }
   } else {
-    for (int a = threadIdx.x; a < NN; a += blockDim.x)
+    for (int a = tm.rank(); a < NN; a += tm.size())
       su[a] = (T)ld.template point2<N>(e, a % N, a / N);
   }
-  __syncthreads();
+  tm.sync();
   const int st[3] = {1, N, NN};
   // reference gradient D_j u
-  for (int a = threadIdx.x; a < NE; a += blockDim.x) {
+  for (int a = tm.rank(); a < NE; a += tm.size()) {
     const int li[3] = {a % N, (a / N) % N, DIM == 3 ? a / NN : 0};
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
@@ -94,9 +111,9 @@ __device__ __forceinline__ void def_element(const BB &B, const DefGeom<T> &g, in
       sd[d * NE + a] = s;
     }
   }
-  __syncthreads();
+  tm.sync();
   // pointwise metric terms
-  for (int a = threadIdx.x; a < NE; a += blockDim.x) {
+  for (int a = tm.rank(); a < NE; a += tm.size()) {
     const int64_t node = base + a;
     if (mode == DEF_DERIV) {
       T du = sd[a] * g.X[(0 * g.nxy + idir - 1) * nl + node];
@@ -135,9 +152,9 @@ __device__ __forceinline__ void def_element(const BB &B, const DefGeom<T> &g, in
     }
   }
   if (mode == DEF_ADVECT || mode == DEF_DERIV) return;
-  __syncthreads();
+  tm.sync();
   // transposed divergence sum_j D_j^T g_j, then the mode's combination
-  for (int a = threadIdx.x; a < NE; a += blockDim.x) {
+  for (int a = tm.rank(); a < NE; a += tm.size()) {
     const int64_t node = base + a;
     const int li[3] = {a % N, (a / N) % N, DIM == 3 ? a / NN : 0};
     T o = T(0);
@@ -178,8 +195,8 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(16) unsigned char smem_def[];
   const int64_t e = blockIdx.x;
   if (e >= ne) return;
-  def_element<T, N, DIM, LD, TO>(B, g, e, mode, p, pvec, q, qvec, use_mass, ld, nv, c0, c1, c2,
-                                 idir, imass, uo, reinterpret_cast<T *>(smem_def));
+  def_element<T, N, DIM, LD, TO>(BlockTeam{}, B, g, e, mode, p, pvec, q, qvec, use_mass, ld, nv, c0,
+                                 c1, c2, idir, imass, uo, reinterpret_cast<T *>(smem_def));
 }
 
 }  // namespace gfk

@@ -129,6 +129,20 @@ template <typename T>
 __device__ __forceinline__ T rk_accum_point(T uout, T K, T ch) {
   return add_rn(uout, mul_rn(K, ch));
 }
+// step_b stage input (252-341): y = uin + ((0 + b0 K0) + b1 K1 + ...), the
+// isum accumulation over the nk earlier slopes
+template <typename T>
+__device__ __forceinline__ T rk_stage_point(T uin, int nk, const T *__restrict__ K0,
+                                            const T *__restrict__ K1, const T *__restrict__ K2,
+                                            T b0, T b1, T b2, int64_t i) {
+  T s = T(0);
+  if (nk > 0) s = T(1) * s + b0 * K0[i];
+  if (nk > 1) s = T(1) * s + b1 * K1[i];
+  if (nk > 2) s = T(1) * s + b2 * K2[i];
+  T v = uin;
+  v += s;
+  return v;
+}
 
 enum { FUSE_EULER = 0, FUSE_ACCUM_AFTER = 1, FUSE_ACCUM_BEFORE = 2 };
 

@@ -135,7 +135,10 @@ class IcosGrid:
     tolerance tol_frac times the smallest node spacing, as GGFX::init).
     refine: GF_ICOS_BISECTION or GF_ICOS_LAGRANGIAN."""
 
-    def __init__(self, level, p, radius=1.0, refine=A.GF_ICOS_BISECTION, tol_frac=0.001):
+    def __init__(self, level, p, radius=1.0, refine=A.GF_ICOS_BISECTION, tol_frac=0.001,
+                 ctx=None):
+        """ctx: match the classes on that context's GPU
+        (gf_classes_from_coords_device, the same classes bit for bit)."""
         lib = _lib()
         self.dim, self.p, self.n, self.level, self.radius = 2, int(p), int(p) + 1, level, radius
         ne, nl = C.c_int64(), C.c_int64()
@@ -163,9 +166,22 @@ class IcosGrid:
         self.node_class = np.zeros(N, dtype=np.int32)
         self.class_ptr = np.zeros(N + 1, dtype=np.int32)
         self.members = np.zeros(N, dtype=np.int32)
-        nc = lib.gf_classes_from_coords(3, N, xyz_c, tol_frac * self.minnodedist,
-                                        A.ptr(self.node_class), A.ptr(self.class_ptr),
-                                        A.ptr(self.members))
+        if ctx is None:
+            nc = lib.gf_classes_from_coords(3, N, xyz_c, tol_frac * self.minnodedist,
+                                            A.ptr(self.node_class), A.ptr(self.class_ptr),
+                                            A.ptr(self.members))
+        else:
+            import torch
+            dev = ctx.torch_device
+            xd = [torch.from_numpy(a).to(dev) for a in self.xyz]
+            outs = [torch.zeros(N, dtype=torch.int32, device=dev),
+                    torch.zeros(N + 1, dtype=torch.int32, device=dev),
+                    torch.zeros(N, dtype=torch.int32, device=dev)]
+            nc = lib.gf_classes_from_coords_device(ctx.handle, 3, N, A.ptr_array(xd),
+                                                   tol_frac * self.minnodedist,
+                                                   *[A.ptr(t) for t in outs])
+            if nc >= 0:
+                self.node_class, self.class_ptr, self.members = (t.cpu().numpy() for t in outs)
         if nc < 0:
             raise A.GFError(nc, "gf_classes_from_coords")
         self.nclass = int(nc)

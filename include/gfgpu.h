@@ -470,6 +470,58 @@ int gf_adjoint_gradient(gf_problem_t prob, const gf_rk_traits *traits,
                         const double *const *u_obs, double dt, int nsteps,
                         int checkpoint_every, double *J, double *const *grad);
 
+/* ---- ensembles of independent problems (no reference counterpart: the
+ * reference runs one problem per process) ----
+ * Up to 64 2-d members of orders 2..9 advanced together, one persistent
+ * cooperative launch per RK stage or CG iteration, captured in CUDA graphs.
+ * Members are either all deformed / embedded problems (GF_ENS_RK: e.g.
+ * icosahedral-sphere advection, each member bit-identical to gf_rk_advance
+ * on it alone) or all box problems with affine elements (GF_ENS_CG:
+ * Helmholtz solves).  The problems must outlive the ensemble. */
+typedef struct gf_ensemble *gf_ensemble_t;
+enum { GF_ENS_RK = 0, GF_ENS_CG = 1 };
+int gf_ensemble_create(gf_ctx_t ctx, int n, const gf_problem_t *members, gf_ensemble_t *out);
+int gf_ensemble_destroy(gf_ensemble_t ens);
+/* GF_ENS_RK or GF_ENS_CG */
+int gf_ensemble_kind(gf_ensemble_t ens);
+/* kernels launched by the ensemble so far (graph launches counted per kernel) */
+uint64_t gf_ensemble_launches(gf_ensemble_t ens);
+/* Advances member m's state u[m] (device, dtype, N_local) by nsteps step_b
+ * steps (GExRKStepper, gexrk_stepper.ipp:252-341) of size dt[m]: traits eqn
+ * GF_EQN_ADVECT (velocity c[3*m + k], k < the member's physical
+ * coordinates) or GF_EQN_HEAT (c may be NULL), nstate 1, scheme RK1..RK4.
+ * Returns GF_ERR_NONFINITE when a member's state is not finite after the
+ * last step.  Synchronises; not callable while the stream is captured. */
+int gf_ensemble_rk_advance(gf_ensemble_t ens, int dtype, const gf_rk_traits *traits,
+                           void *const *u, const void *const *c, const double *dt, int nsteps);
+/* Solves (p L + q M) x[m] = b[m] for every member m (device FP64 E-vectors;
+ * x holds the initial guess): GCG::solve_impl(A, b, x) (gcg.ipp:239-382) with
+ * the Jacobi preconditioner, FP32 iterations and FP64 residual refinement
+ * each time an FP32 run has reduced its residual by traits->inner_tol
+ * (default 1e-4).  traits: precision GF_CG_MIXED, precond GF_PRECOND_JACOBI,
+ * normtype EUC or INF, maxit (FP32 iterations per member), tol, relative,
+ * max_refine (default 64).  Per member (host arrays, may be NULL): FP32
+ * iterations, the last FP64 residual norm, status 0 converged / 1 no
+ * convergence / 2 breakdown.  Returns 0, GF_CG_NOCONVERGE if any member did
+ * not converge, or GF_ERR_NONFINITE.  Synchronises. */
+int gf_ensemble_cg_solve(gf_ensemble_t ens, const gf_cg_traits *traits, double p, double q,
+                         const double *const *b, double *const *x, int *iters,
+                         double *final_norm, int *status);
+/* The autotuner: times the element phase of candidate launch shapes
+ * (threads per block, blocks per SM, lanes per element for each order
+ * present) on this ensemble's members, with the ensemble's own scratch as
+ * the data, and keeps the fastest.  An RK ensemble is timed on the equation
+ * of its last advance (advection before the first). */
+int gf_ensemble_tune(gf_ensemble_t ens, int dtype, int reps);
+/* The current shape: threads per block, cooperative blocks, lanes per
+ * element by GLL point count (team_by_n[n], n <= 10), tuned flag. */
+int gf_ensemble_shape(gf_ensemble_t ens, int dtype, int *threads, int *blocks, int *team_by_n,
+                      int *tuned);
+/* Sets a shape (threads 64..512, blocks per SM 0 = as many as fit, team
+ * widths 8/16/32 by point count, or NULL to keep them). */
+int gf_ensemble_set_shape(gf_ensemble_t ens, int dtype, int threads, int blocks_per_sm,
+                          const int *team_by_n);
+
 #ifdef __cplusplus
 }
 #endif
