@@ -94,7 +94,7 @@ def parse():
     ap.add_argument("--mg-ratio", type=float, default=0.0,
                     help="multigrid: lmax/lmin of the smoothing interval (0: library default)")
     ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "pmg", "apply", "adjoint", "graphs",
-                                       "rk", "maps"],
+                                       "ensemble", "rk", "maps"],
                     default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
@@ -465,11 +465,10 @@ def adjoint_bench(ctx, ne=16, p=6, nsteps=50, ck=10, reps=3):
 
 # ---------------------------------------------------------------------------
 def graph_bench(ctx, reps=3):
-    """Small, launch-bound workloads: (1) 2-d periodic advection-diffusion on
-    16^2 elements p = 4 (c = (1, 0.5), nu = 0.01, dt = 1e-4, RK4, 200 steps)
-    by direct calls vs one CUDA graph; (2) an ensemble of 16 independent
-    2-d periodic boxes (8^2..64^2 elements, p = 3..8, seeded) advanced 20
-    RK4 steps, member by member vs one ensemble graph."""
+    """The small, launch-bound CPU-runnable case: 2-d periodic
+    advection-diffusion on 16^2 elements p = 4 (c = (1, 0.5), nu = 0.01,
+    dt = 1e-4, RK4, 200 steps) by direct calls vs one CUDA graph, each
+    against the reference's own run of it."""
     import torch
     from geoflow_b200 import GBurgers, Graph, GridBox, Problem, workloads as W
     from geoflow_b200 import _abi as A
@@ -527,30 +526,219 @@ def graph_bench(ctx, reps=3):
             "graph": float(np.max(np.abs(u_graph - r200)) / np.max(np.abs(r200))),
             "same_initial_state": same_ic}}
     G.close()
-    rng = np.random.default_rng(SEED + 6)
-    members = [box(int(rng.choice([8, 16, 24, 32, 48, 64])), int(rng.integers(3, 9)), SEED + 10 + i)
-               for i in range(16)]
-    steps = 20
+    return out
+
+
+# ---------------------------------------------------------------------------
+def ensemble_bench(ctx, steps=10, reps=3):
+    """The batched ensemble: (1) 16 icosahedral-sphere advection members
+    (level 3..5, p 4..8, cosine bell with seeded centre, solid-body wind,
+    RK4, dt at CFL 0.25) as one gf_ensemble, one persistent launch per stage,
+    FP32, against the same members stepped one by one by gf_rk_advance
+    (every member bit-identical), with the FP32-vs-FP64 difference; (2) 16
+    2-d Dirichlet box Helmholtz solves (8^2..64^2 elements, p 3..8, seeded
+    sinusoidal RHS, (M + K)x = b to 1e-10 relative EUC residual), one
+    persistent launch per CG iteration (FP32 PCG, FP64 refinement), against
+    the members solved one by one (gf_cg_solve, mixed and FP64), each
+    member's FP64 residual recomputed by the FP64 apply.  Launch shapes
+    from the autotuner."""
+    import torch
+    from geoflow_b200 import (CGTraits, Ensemble, GBurgers, GCG, GGFX, GHelmholtz, GMass,
+                              GridBox, IcosGrid, Problem, workloads as W)
+    from geoflow_b200 import _abi as A
+    dev = ctx.torch_device
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, prep=None):
+        ts = []
+        for _ in range(reps):
+            if prep:
+                prep()
+            torch.cuda.synchronize()
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e) / 1e3)
+        return statistics.median(ts)
+
+    out = {}
+    # ---- (1) icosahedral advection members ----
+    t0 = time.perf_counter()
+    mem = []
+    for level, p, lat0, lon0 in W.icos_members():
+        g = IcosGrid(level, p, ctx=ctx)
+        prob = g.problem(ctx)
+        u0 = W.icos_cosine_bell(g.xyz, lat0, lon0)
+        c = W.icos_solid_body_wind(g.xyz)
+        cmax = float(np.max(np.sqrt(sum(a * a for a in c))))
+        mem.append((g, prob, u0, c, 0.25 * g.minnodedist / cmax))
+    setup_s = time.perf_counter() - t0
+    probs = [m[1] for m in mem]
+    dts = [m[4] for m in mem]
+    ndof = sum(p.nlocal for p in probs)
+
+    def state(dtype):
+        us = [torch.from_numpy(m[2]).to(dev, dtype) for m in mem]
+        cs = [[torch.from_numpy(a).to(dev, dtype) for a in m[3]] for m in mem]
+        return us, cs
+
+    E = Ensemble(ctx, probs)
+    us, cs = state(torch.float32)
+    u0s = [u.clone() for u in us]
+
+    def reset():
+        for u, v in zip(us, u0s):
+            u.copy_(v)
+
+    E.advance(us, cs, dt=dts, nsteps=1)
+    t1 = time.perf_counter()
+    E.tune(torch.float32, reps=3)
+    tune_s = time.perf_counter() - t1
+    shape = E.shape(torch.float32)
+
+    l0 = E.launches()
+    t_ens = timed(lambda: E.advance(us, cs, dt=dts, nsteps=steps), reset)
+    launches_per_run = (E.launches() - l0) // reps
+    reset()
+    E.advance(us, cs, dt=dts, nsteps=steps)
+    got32 = [u.cpu().numpy() for u in us]
+    Bs = [GBurgers(m[1], A.GF_EQN_ADVECT, 0.0, scheme=A.GF_RK4) for m in mem]
 
     def seq():
-        for _, _, Bm, um, cm in members:
-            Bm.step(um, cm, dt=1e-4, nsteps=steps)
+        for k, B in enumerate(Bs):
+            B.step([us[k]], cs[k], dt=dts[k], nsteps=steps)
 
-    t_seq = timed(seq)
-    graphs = [Bm.capture(um, cm, dt=1e-4, nsteps=steps) for _, _, Bm, um, cm in members]
-    E = Graph.ensemble(graphs)
-    t_ens = timed(E.launch)
-    ndof = sum(pm.nlocal for _, pm, _, _, _ in members)
-    out["ensemble"] = {
-        "workload": ("16 independent 2d periodic advection boxes (8^2..64^2 elements, p=3..8), "
-                     "RK4, 20 steps each, FP64"),
-        "members": [[gm.ne[0], gm.p] for gm, _, _, _, _ in members], "n_local_total": ndof,
-        "sequential_s": t_seq, "ensemble_graph_s": t_ens,
-        "gdofs_per_stage_sequential": ndof * 4 * steps / t_seq / 1e9,
-        "gdofs_per_stage_ensemble": ndof * 4 * steps / t_ens / 1e9}
-    E.close()
-    for gr in graphs:
-        gr.close()
+    t_seq = timed(seq, reset)
+    reset()
+    seq()
+    same = sum(int(np.array_equal(got32[k], us[k].cpu().numpy())) for k in range(len(mem)))
+    us64, cs64 = state(torch.float64)
+    E.advance(us64, cs64, dt=dts, nsteps=steps)
+    err32 = max(float(np.max(np.abs(got32[k] - us64[k].cpu().numpy())) /
+                      np.max(np.abs(us64[k].cpu().numpy()))) for k in range(len(mem)))
+    stages = 4 * steps
+    # algorithmic bytes per node and stage (FP32): stage input u + the mean
+    # 1.5 earlier slopes, 3 velocity, 6 dXi/dX, 3 metric, Jac, inverse mass
+    # read and the slope written by the element phase; the fold reads and
+    # writes the slope and the output state (8 words)
+    alg_b = 4 * (1 + 1.5 + 3 + 6 + 3 + 1 + 1 + 1 + 4)
+    out["icos_advection"] = {
+        "workload": ("16 icosahedral-sphere advection members (level 3..5, p 4..8, cosine bell, "
+                     "solid-body wind), RK4, dt at CFL 0.25, FP32, %d steps" % steps),
+        "members": [[m[0].level, m[0].p] for m in mem], "n_local_total": ndof,
+        "setup_s": setup_s, "tune_s": tune_s, "shape": shape,
+        "ensemble_s": t_ens, "sequential_s": t_seq, "speedup_vs_sequential": t_seq / t_ens,
+        "gdofs_per_stage_ensemble": ndof * stages / t_ens / 1e9,
+        "gdofs_per_stage_sequential": ndof * stages / t_seq / 1e9,
+        "alg_bytes_per_node_stage": alg_b,
+        "hbm_gbs_ensemble": ndof * stages * alg_b / t_ens / 1e9,
+        "launches_per_run": launches_per_run,
+        "members_bit_identical_to_single": f"{same}/{len(mem)}",
+        "f32_rel_diff_vs_f64": err32}
+    del E, us, cs, us64, cs64, u0s, Bs
+    # ---- (2) box Helmholtz members ----
+    bm = []
+    for k, (ne, p) in enumerate(W.box_members()):
+        g = GridBox(2, [ne, ne], p)
+        prob = Problem(ctx, g)
+        f = torch.from_numpy(W.helmholtz2d_rhs(g.xyz, seed=SEED + 20 + k)).to(dev)
+        b = prob.zeros()
+        GMass(prob).opVec_prod(f, None, b)
+        bm.append((g, prob, b))
+    E2 = Ensemble(ctx, [m[1] for m in bm])
+    bs = [m[2] for m in bm]
+    xs = [torch.zeros_like(b) for b in bs]
+
+    def zero():
+        for x in xs:
+            x.zero_()
+
+    def traits(**kw):
+        t = CGTraits()
+        t.maxit, t.normtype, t.tol, t.relative = 50000, A.GF_NORM_EUC, 1e-10, 1
+        t.precond, t.precision, t.check_every = A.GF_PRECOND_JACOBI, A.GF_CG_MIXED, 16
+        for k, v in kw.items():
+            setattr(t, k, v)
+        return t
+
+    def fp64_residual():
+        """each member's mask*DSS_Sum(b - A x) relative to b (EUC), FP64 apply"""
+        worst = 0.0
+        for (g, prob, b), x in zip(bm, xs):
+            H = GHelmholtz(prob)
+            H.set_Lap_scalar(1.0)
+            H.set_mass_scalar(1.0)
+            r = prob.zeros()
+            H.opVec_prod(x, None, r)
+            r = b - r
+            GGFX(prob).doOp(r, GGFX.Sum)
+            r *= torch.from_numpy(g.mask).to(dev)
+            worst = max(worst, float(torch.sqrt((r * r).mean()) / torch.sqrt((b * b).mean())))
+        return worst
+
+    E2.solve(bs, xs, traits())
+    t1 = time.perf_counter()
+    E2.tune(reps=3)
+    tune2_s = time.perf_counter() - t1
+    modes = {"mixed_reliable": {}, "mixed_restart": {"inner_tol": 1e-4},
+             "fp64": {"precision": A.GF_CG_FP64}}
+    runs = {}
+    for name, kw in modes.items():
+        tr = traits(**kw)
+        zero()
+        E2.solve(bs, xs, tr)
+        l0 = E2.launches()
+        t_m = timed(lambda: E2.solve(bs, xs, tr), zero)
+        nl = (E2.launches() - l0) // reps
+        zero()
+        rc, its, nrm, st = E2.solve(bs, xs, tr)
+        runs[name] = {"s": t_m, "iterations": [int(i) for i in its], "rc": int(rc),
+                      "statuses": [int(v) for v in st], "launches_per_solve": nl,
+                      "member_iterations_per_s": float(sum(its)) / t_m,
+                      "max_rel_fp64_residual": fp64_residual(),
+                      "x": [x.clone() for x in xs]}
+    seqs = {}
+    xseq = [torch.zeros_like(b) for b in bs]
+    diff = 0.0
+    for name, prec, ce in (("mixed", A.GF_CG_MIXED, 16), ("fp64", A.GF_CG_FP64, 32)):
+        t2 = CGTraits()
+        t2.maxit, t2.normtype, t2.tol, t2.relative = 50000, A.GF_NORM_EUC, 1e-10, 1
+        t2.precond, t2.precision, t2.check_every = A.GF_PRECOND_JACOBI, prec, ce
+        solvers = []
+        for g, prob, b in bm:
+            H = GHelmholtz(prob)
+            H.set_Lap_scalar(1.0)
+            H.set_mass_scalar(1.0)
+            solvers.append((GCG(t2, prob), H))
+
+        zb = [torch.zeros_like(b) for b in bs]
+
+        def run():  # solve_impl (2), xb = 0: the masked (Dirichlet) solve
+            for (cg, H), b, xb, x in zip(solvers, bs, zb, xseq):
+                cg.solve(H, b, xb, x)
+
+        seqs[name] = timed(run, lambda: [x.zero_() for x in xseq])
+        if name == "fp64":
+            for x in xseq:
+                x.zero_()
+            run()
+    for r in runs.values():
+        r["max_rel_diff_vs_sequential_fp64"] = max(
+            float((a - c).abs().max() / c.abs().max()) for a, c in zip(r.pop("x"), xseq))
+    nL = sum(m[1].nlocal for m in bm)
+    head = runs["mixed_reliable"]
+    out["box_helmholtz"] = {
+        "workload": ("16 2d Dirichlet box Helmholtz solves (M+K)x=b (8^2..64^2 elements, "
+                     "p 3..8), Jacobi PCG to 1e-10 relative EUC residual"),
+        "members": [[m[0].ne[0], m[0].p] for m in bm], "n_local_total": nL,
+        "tune_s": tune2_s, "shape": E2.shape(),
+        "ensemble_s": head["s"], "scheme": "FP32 iterations, FP64 residual every 16 (reliable)",
+        "modes": runs,
+        "sequential_mixed_s": seqs["mixed"], "sequential_fp64_s": seqs["fp64"],
+        "speedup_vs_sequential_mixed": seqs["mixed"] / head["s"],
+        "speedup_vs_sequential_fp64": seqs["fp64"] / head["s"],
+        "speedup_fp64_ensemble_vs_sequential_fp64": seqs["fp64"] / runs["fp64"]["s"]}
     return out
 
 
@@ -759,6 +947,10 @@ def main():
     if args.only == "graphs":
         print(json.dumps({"only": "graphs", "graphs": graph_bench(ctx)}), flush=True)
         return
+    if args.only == "ensemble":
+        print(json.dumps({"only": "ensemble", "ensemble": ensemble_bench(ctx, steps=args.steps)}),
+              flush=True)
+        return
     if args.only == "maps":
         print(json.dumps({"only": "maps", "index_maps": index_map_bench(ctx)}), flush=True)
         return
@@ -830,12 +1022,13 @@ def main():
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    rk = adj = graphs = maps = None
+    rk = adj = graphs = maps = ens = None
     if not args.no_rk:
-        rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p)
+        rk = rk_stage_bench(ctx, args.rk_ne, args.rk_p, steps=100)  # config 3's full 100 steps
         adj = adjoint_bench(ctx)
         graphs = graph_bench(ctx)
         maps = index_map_bench(ctx)
+        ens = ensemble_bench(ctx)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         t_node, cores, nsample = cpu_baseline_sample(args.p, it_64[-1], args.cpu_sample_ne)
@@ -884,6 +1077,7 @@ def main():
         "rk_stage": rk,
         "adjoint": adj,
         "graphs": graphs,
+        "ensemble": ens,
         "index_maps": maps,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -165,7 +165,7 @@ SIGNATURES = {
     "gf_ensemble_cg_solve": (c_int, [c_void_p, C.POINTER(CGTraits), c_double, c_double, P_void,
                                      P_void, P_int, P_double, P_int]),
     "gf_ensemble_tune": (c_int, [c_void_p, c_int, c_int]),
-    "gf_ensemble_shape": (c_int, [c_void_p, c_int, P_int, P_int, P_int, P_int]),
+    "gf_ensemble_shape": (c_int, [c_void_p, c_int, P_int, P_int, P_int, P_int, P_double]),
     "gf_ensemble_set_shape": (c_int, [c_void_p, c_int, c_int, c_int, P_int]),
 }
 

@@ -10,27 +10,29 @@
 // chunk holds 32/team elements of one member.  The chunks of all members
 // are numbered consecutively and the warps of the grid take them round
 // robin, which spreads every member evenly over the GPU whatever its size
-// and order.  Node work is numbered the same way over the members'
-// gather-scatter classes (RK) or, for the CG, cut into one contiguous slice
-// of every member per block, so a block owns the same nodes in every phase
-// and its partial dot products come out in a fixed order.
+// and order.  Node work is numbered the same way: one thread per
+// gather-scatter class of every member (RK), or warp slices of 256 lattice
+// nodes of every member (CG), so a slice's warp owns the same nodes in
+// every phase and writes one partial sum per slice.
 //
 // Phases inside one launch are separated by a grid barrier (an arrival
 // count and a generation word; the spin is bounded and records a timeout
 // instead of waiting for ever).  The kernels are launched cooperatively,
 // so all blocks are resident.  The last block to reach a reducing barrier
-// folds the blocks' partials per member in block order and forms the
-// member's CG scalars before it releases the others: for a given launch
-// shape the scalars are deterministic.
+// folds each member's slice partials in slice order and forms the member's
+// CG scalars before it releases the others: the scalars are deterministic
+// and do not depend on the launch shape.
 //
 // Arithmetic.  An RK member's element body is def_element (k_def.cuh), its
-// folds are those of k_dss_rk_csr / k_dss_csr and its stage sums those of
+// folds are those of k_dss_rk_split / k_dss_split and its stage sums those of
 // step_b (rk_stage_point), so each member advances bit for bit as
 // gf_rk_advance advances it alone.  A CG member runs GCG::solve_impl's DFM
 // iteration (solvers/gcg.ipp:239-382) with a Jacobi preconditioner on the
 // unique lattice nodes: FP32 vectors and applies, FP64 dot products, and
 // restarted refinement, x += d and r = mask DSS_Sum(b - A x) in FP64 each
-// time an FP32 run has reduced its residual by inner_tol.
+// time an FP32 run has reduced its residual by inner_tol.  The CG member is
+// the masked (homogeneous Dirichlet) solve, solve_impl (2) with xb = 0: the
+// form without xb leaves bbv_ unset and masks nothing.
 //
 // Tile shapes (threads per block, blocks per SM, team width per order) are
 // chosen by gf_ensemble_tune, which times the element phase of candidate
@@ -52,8 +54,8 @@ namespace {
 
 constexpr int EN_MINN = 3, EN_MAXN = 10;  // members of order 2..9
 constexpr int EN_MAXMEM = 64;
-constexpr int EN_MAXWARPS = 16;           // threads per block <= 512
 constexpr unsigned EN_SPIN_LIMIT = 1u << 21;
+constexpr int EN_WS = 256;  // lattice nodes per warp slice (CG)
 
 enum { EN_REFINE = 0, EN_INNER = 1, EN_DONE = 2 };
 
@@ -65,8 +67,12 @@ struct EnMember {
   // deformed / embedded geometry, [0] FP64 and [1] FP32
   const void *X[2], *G[2], *J[2], *imass[2];
   const int32_t *class_ptr, *members;
+  const int32_t *sh_ptr, *sh_members;  // classes of several members (shared nodes)
+  int64_t nshared;
+  const float *imult32;                 // 1/multiplicity per node (1: a singleton class)
   // RK state: u[0] the caller's, u[1] scratch; slopes; final-stage input
   void *u[2], *K[3], *uf;
+  void *advb[2];  // advection fast path: adv_element's coefficient planes
   const void *c[3];
   double coef[4][3], ch[4];
   // box lattice (CG)
@@ -78,11 +84,13 @@ struct EnMember {
   const double *bE;
   double *xE, *bL, *xL, *r64, *dinv64, *aE;
   float *dL, *r32, *w32, *q32, *dinv32;
+  double *w64, *q64;  // the FP64 solve's search direction and A w
 };
 
 struct EnCG {
   double rho, alpha, beta, rnorm, rnorm64, rtol, itol, bnorm, nd;
   int next, iters, sweeps, status;
+  int trig;  // reliable form: the FP32 residual met the stop test (the replacement restarts)
 };
 
 struct EnCtl {
@@ -95,17 +103,19 @@ struct EnArgs {
   EnMember *mem;
   int nmem;
   const int64_t *chunk_pref, *class_pref;  // nmem + 1 each
-  int64_t nchunk, nclass;
+  const int64_t *sh_pref;                  // RK: shared-class prefix, nmem + 1
+  int64_t nchunk, nclass, nsh;
   EnCtl *ctl;
   EnCG *cg;
   double *partials;  // [nmem][2][gridDim.x]
   int wbytes;        // dynamic shared bytes per warp
   // RK
-  int ns, par, eqn;
+  int ns, par, eqn, fast;
   double nu;
   // CG
   double p, q, tol, inner_tol;
   int normtype, maxit, max_refine, relative, all_inner;
+  int fp64, reliable, check_every;
   unsigned launch_cap;
   cudaGraphConditionalHandle cond;
   int has_cond;
@@ -229,7 +239,19 @@ struct LoadL2 {  // an element-local vector written earlier in this launch
 
 template <typename T, int N>
 __device__ void en_rhs_elem(const LaneTeam &tm, const EnMember &M, int64_t e, const SBasis<T> &B,
-                            T *slice, bool from_uf, int stage, int par, int eqn, T nu) {
+                            T *slice, bool from_uf, int stage, int par, int eqn, T nu, bool fast) {
+  if (fast) {  // prescribed velocity, nu = 0: adv_element on the coefficient planes
+    const T *b0 = (const T *)M.advb[0], *b1 = (const T *)M.advb[1];
+    if (from_uf)
+      adv_element<T, N>(tm, B, e, LoadL2<T>{(const T *)M.uf}, b0, b1, (T *)M.K[0], slice);
+    else
+      adv_element<T, N>(tm, B, e,
+                        LoadStage<T>{(const T *)M.u[par], (const T *)M.K[0], (const T *)M.K[1],
+                                     (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
+                                     (T)M.coef[stage][2], stage},
+                        b0, b1, (T *)M.K[stage], slice);
+    return;
+  }
   constexpr int pr = sizeof(T) == 4 ? 1 : 0;
   const DefGeom<T> g{(const T *)M.X[pr], (const T *)M.G[pr], (const T *)M.J[pr], M.nxy,
                      M.nlocal};
@@ -258,6 +280,7 @@ __device__ void en_rk_elements(const EnArgs &a, const int64_t *cpref, bool from_
   T *ws = reinterpret_cast<T *>(en_smem + (size_t)wib * a.wbytes);
   const int64_t nw = (int64_t)gridDim.x * wpb;
   const T nu = (T)a.nu;
+  const bool fast = a.fast != 0;
   int cur = -1;
   for (int64_t ch = (int64_t)blockIdx.x * wpb + wib; ch < a.nchunk; ch += nw) {
     const int mi = en_find(cpref, a.nmem, ch);
@@ -276,76 +299,123 @@ __device__ void en_rk_elements(const EnArgs &a, const int64_t *cpref, bool from_
       const SBasis<T> B{ws, ws + N * N};
       T *slice = ws + en_basis_words<T>(N) + tid * 5 * N * N;
       switch (N) {
-        case 3: en_rhs_elem<T, 3>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        case 4: en_rhs_elem<T, 4>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        case 5: en_rhs_elem<T, 5>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        case 6: en_rhs_elem<T, 6>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        case 7: en_rhs_elem<T, 7>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        case 8: en_rhs_elem<T, 8>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        case 9: en_rhs_elem<T, 9>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
-        default: en_rhs_elem<T, 10>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu); break;
+        case 3: en_rhs_elem<T, 3>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 4: en_rhs_elem<T, 4>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 5: en_rhs_elem<T, 5>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 6: en_rhs_elem<T, 6>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 7: en_rhs_elem<T, 7>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 8: en_rhs_elem<T, 8>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 9: en_rhs_elem<T, 9>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        default: en_rhs_elem<T, 10>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
       }
     }
     __syncwarp();
   }
 }
 
+// The node work of an RK stage, split by class size: a class with one
+// member (an interior node, most of them) is folded by the thread of that
+// node, in node order (coalesced, no index arrays: imult = 1 marks it); a
+// class with several members is folded by one thread from the problem's
+// shared-class list (sh_ptr / sh_members, members in ascending local id).
+// Either way the fold is that of k_dss_rk_split: from 0, in member
+// order, divided by the count.  The items are all members' nodes
+// (prefix npref), then all members' shared classes (prefix spref).
+template <class FN, class FC>
+__device__ __forceinline__ void en_rk_items(const EnArgs &a, const int64_t *npref,
+                                            const int64_t *spref, FN node, FC cls) {
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x, total = a.nclass + a.nsh;
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < total; it += nt) {
+    if (it < a.nclass) {
+      const int mi = en_find(npref, a.nmem, it);
+      const EnMember &M = a.mem[mi];
+      const int64_t i = it - npref[mi];
+      if (M.imult32[i] == 1.0f) node(mi, M, i);
+    } else {
+      const int64_t j = it - a.nclass;
+      const int mi = en_find(spref, a.nmem, j);
+      const EnMember &M = a.mem[mi];
+      const int64_t cl = j - spref[mi];
+      cls(mi, M, M.sh_ptr[cl], M.sh_ptr[cl + 1]);
+    }
+  }
+}
+
 // Final-stage input: uf = Smooth(stage sum over the ns-1 earlier slopes).
 template <typename T>
-__device__ void en_rk_stage_input(const EnArgs &a, const int64_t *kpref, int stage) {
-  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.nclass; c += nt) {
-    const int mi = en_find(kpref, a.nmem, c);
-    const EnMember &M = a.mem[mi];
-    const int64_t cl = c - M.class0;
-    const int32_t b0 = M.class_ptr[cl], e0 = M.class_ptr[cl + 1];
-    const T *uin = (const T *)M.u[a.par];
-    const T *K0 = (const T *)M.K[0], *K1 = (const T *)M.K[1], *K2 = (const T *)M.K[2];
-    const T c0 = (T)M.coef[stage][0], c1 = (T)M.coef[stage][1], c2 = (T)M.coef[stage][2];
-    T acc = T(0);
-    for (int32_t k = b0; k < e0; k++) {
-      const int64_t m = M.members[k];
-      acc = __fadd_rn_t(acc, rk_stage_point(uin[m], stage, K0, K1, K2, c0, c1, c2, m));
-    }
-    acc = acc / (T)(e0 - b0);
-    T *uf = (T *)M.uf;
-    for (int32_t k = b0; k < e0; k++) uf[M.members[k]] = acc;
-  }
+__device__ void en_rk_stage_input(const EnArgs &a, const int64_t *npref, const int64_t *spref,
+                                  int stage) {
+  en_rk_items(
+      a, npref, spref,
+      [&](int, const EnMember &M, int64_t i) {
+        const T *uin = (const T *)M.u[a.par];
+        const T v = rk_stage_point(uin[i], stage, (const T *)M.K[0], (const T *)M.K[1],
+                                   (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
+                                   (T)M.coef[stage][2], i);
+        ((T *)M.uf)[i] = __fadd_rn_t(T(0), v) / T(1);
+      },
+      [&](int, const EnMember &M, int32_t b0, int32_t e0) {
+        const T *uin = (const T *)M.u[a.par];
+        const T *K0 = (const T *)M.K[0], *K1 = (const T *)M.K[1], *K2 = (const T *)M.K[2];
+        const T c0 = (T)M.coef[stage][0], c1 = (T)M.coef[stage][1], c2 = (T)M.coef[stage][2];
+        T acc = T(0);
+        for (int32_t k = b0; k < e0; k++) {
+          const int64_t m = M.sh_members[k];
+          acc = __fadd_rn_t(acc, rk_stage_point(uin[m], stage, K0, K1, K2, c0, c1, c2, m));
+        }
+        acc = acc / (T)(e0 - b0);
+        T *uf = (T *)M.uf;
+        for (int32_t k = b0; k < e0; k++) uf[M.sh_members[k]] = acc;
+      });
 }
 
 // Fold of a stage: Smooth K_stage and uout += c h K (stages before the
 // last), or for the last stage uout = Smooth(uout + c h Smooth(K_0)).
 template <typename T>
-__device__ void en_rk_fold(const EnArgs &a, const int64_t *kpref, int stage) {
+__device__ void en_rk_fold(const EnArgs &a, const int64_t *npref, const int64_t *spref,
+                           int stage) {
   const bool fin = stage == a.ns - 1;
-  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.nclass; c += nt) {
-    const int mi = en_find(kpref, a.nmem, c);
-    const EnMember &M = a.mem[mi];
-    const int64_t cl = c - M.class0;
-    const int32_t b0 = M.class_ptr[cl], e0 = M.class_ptr[cl + 1];
-    const T cnt = (T)(e0 - b0), ch = (T)M.ch[stage];
-    T *uout = (T *)M.u[1 - a.par];
-    const T *src = stage == 0 ? (const T *)M.u[a.par] : uout;
-    T *Kx = (T *)M.K[fin ? 0 : stage];
-    T acc = T(0);
-    for (int32_t k = b0; k < e0; k++) acc = __fadd_rn_t(acc, __ldcg(Kx + M.members[k]));
-    acc = acc / cnt;
-    if (!fin) {
-      for (int32_t k = b0; k < e0; k++) {
-        const int64_t m = M.members[k];
-        Kx[m] = acc;
-        uout[m] = rk_accum_point(src[m], acc, ch);
-      }
-    } else {
-      T acc2 = T(0);
-      for (int32_t k = b0; k < e0; k++)
-        acc2 = __fadd_rn_t(acc2, rk_accum_point(src[M.members[k]], acc, ch));
-      acc2 = acc2 / cnt;
-      for (int32_t k = b0; k < e0; k++) uout[M.members[k]] = acc2;
-      if (!isfinite((double)acc2)) a.ctl->nonfinite[mi] = 1;
-    }
-  }
+  en_rk_items(
+      a, npref, spref,
+      [&](int mi, const EnMember &M, int64_t i) {
+        const T ch = (T)M.ch[stage];
+        T *uout = (T *)M.u[1 - a.par];
+        const T *src = stage == 0 ? (const T *)M.u[a.par] : uout;
+        T *Kx = (T *)M.K[fin ? 0 : stage];
+        const T acc = __fadd_rn_t(T(0), __ldcg(Kx + i)) / T(1);
+        if (!fin) {
+          Kx[i] = acc;
+          uout[i] = rk_accum_point(src[i], acc, ch);
+        } else {
+          const T acc2 = __fadd_rn_t(T(0), rk_accum_point(src[i], acc, ch)) / T(1);
+          uout[i] = acc2;
+          if (!isfinite((double)acc2)) a.ctl->nonfinite[mi] = 1;
+        }
+      },
+      [&](int mi, const EnMember &M, int32_t b0, int32_t e0) {
+        const T cnt = (T)(e0 - b0), ch = (T)M.ch[stage];
+        T *uout = (T *)M.u[1 - a.par];
+        const T *src = stage == 0 ? (const T *)M.u[a.par] : uout;
+        T *Kx = (T *)M.K[fin ? 0 : stage];
+        const int32_t *mem = M.sh_members;
+        T acc = T(0);
+        for (int32_t k = b0; k < e0; k++) acc = __fadd_rn_t(acc, __ldcg(Kx + mem[k]));
+        acc = acc / cnt;
+        if (!fin) {
+          for (int32_t k = b0; k < e0; k++) {
+            const int64_t m = mem[k];
+            Kx[m] = acc;
+            uout[m] = rk_accum_point(src[m], acc, ch);
+          }
+        } else {
+          T acc2 = T(0);
+          for (int32_t k = b0; k < e0; k++)
+            acc2 = __fadd_rn_t(acc2, rk_accum_point(src[mem[k]], acc, ch));
+          acc2 = acc2 / cnt;
+          for (int32_t k = b0; k < e0; k++) uout[mem[k]] = acc2;
+          if (!isfinite((double)acc2)) a.ctl->nonfinite[mi] = 1;
+        }
+      });
 }
 
 // One RK stage of every member (step_b of GExRKStepper, gexrk_stepper.ipp:
@@ -353,18 +423,19 @@ __device__ void en_rk_fold(const EnArgs &a, const int64_t *kpref, int stage) {
 // and Smooth | RHS | fold.
 template <typename T>
 __global__ void __launch_bounds__(512) k_en_rk_stage(EnArgs a, int stage) {
-  __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_kpref[EN_MAXMEM + 1];
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_npref[EN_MAXMEM + 1], s_spref[EN_MAXMEM + 1];
   en_load_pref(a.chunk_pref, s_cpref, a.nmem);
-  en_load_pref(a.class_pref, s_kpref, a.nmem);
+  en_load_pref(a.class_pref, s_npref, a.nmem);
+  en_load_pref(a.sh_pref, s_spref, a.nmem);
   __syncthreads();
   const bool fin = stage == a.ns - 1;
   if (fin) {
-    en_rk_stage_input<T>(a, s_kpref, stage);
+    en_rk_stage_input<T>(a, s_npref, s_spref, stage);
     en_barrier(a.ctl, NoWork{});
   }
   en_rk_elements<T>(a, s_cpref, fin, stage);
   en_barrier(a.ctl, NoWork{});
-  en_rk_fold<T>(a, s_kpref, stage);
+  en_rk_fold<T>(a, s_npref, s_spref, stage);
 }
 
 // element phase alone (the autotuner's timing kernel): stage 0 of step_b
@@ -390,6 +461,7 @@ __device__ __forceinline__ void en_box_apply(const LaneTeam &tm, const EnMember 
   const T X0 = eg[e * 3], X1 = eg[e * 3 + 1], J = eg[e * 3 + 2];
   const int ey = (int)(e / M.ne0), ex = (int)(e - (int64_t)ey * M.ne0);
   const BoxWalk &w = M.walk;
+#pragma unroll 4
   for (int a = tm.rank(); a < NN; a += tm.size()) {
     const int i = a % N, j = a / N;
     int gx = ex * (N - 1) + i, gy = ey * (N - 1) + j;
@@ -434,6 +506,10 @@ struct LdW {  // FP32 search direction
   const float *w;
   __device__ __forceinline__ float operator()(int64_t c) const { return w[c]; }
 };
+struct LdW64 {  // FP64 search direction
+  const double *w;
+  __device__ __forceinline__ double operator()(int64_t c) const { return w[c]; }
+};
 struct LdX {  // FP64 solution plus the FP32 correction not yet added
   const double *x;
   const float *d;
@@ -441,12 +517,14 @@ struct LdX {  // FP64 solution plus the FP32 correction not yet added
 };
 
 template <int N>
-__device__ void en_cg_elem(const LaneTeam &tm, const EnMember &M, int64_t e, int mode,
+__device__ void en_cg_elem(const LaneTeam &tm, const EnMember &M, int64_t e, int mode, bool f64,
                            const float *Df, const float *Wf, const double *Dd, const double *Wd,
                            void *slice, double p, double q) {
-  if (mode == EN_INNER)
+  if (mode == EN_INNER && !f64)
     en_box_apply<float, N>(tm, M, e, Df, Wf, (float *)slice, LdW{M.w32}, (float)p, (float)q,
                            (float *)M.aE);
+  else if (mode == EN_INNER)
+    en_box_apply<double, N>(tm, M, e, Dd, Wd, (double *)slice, LdW64{M.w64}, p, q, M.aE);
   else
     en_box_apply<double, N>(tm, M, e, Dd, Wd, (double *)slice, LdX{M.xL, M.dL}, p, q, M.aE);
 }
@@ -462,6 +540,7 @@ __device__ void en_cg_elements(const EnArgs &a, const int64_t *cpref, const int 
   double *ws = reinterpret_cast<double *>(en_smem + (size_t)wib * a.wbytes);
   const int64_t nw = (int64_t)gridDim.x * wpb;
   int cur = -1;
+  const bool f64 = a.fp64 != 0;
   for (int64_t ch = (int64_t)blockIdx.x * wpb + wib; ch < a.nchunk; ch += nw) {
     const int mi = en_find(cpref, a.nmem, ch);
     const int md = a.all_inner ? EN_INNER : mode[mi];
@@ -488,14 +567,14 @@ __device__ void en_cg_elements(const EnArgs &a, const int64_t *cpref, const int 
       const LaneTeam tm{lane - tid * team, team, team_mask(team, tid)};
       void *slice = ws + en_cg_basis_doubles(N) + (size_t)tid * 3 * N * N;
       switch (N) {
-        case 3: en_cg_elem<3>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        case 4: en_cg_elem<4>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        case 5: en_cg_elem<5>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        case 6: en_cg_elem<6>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        case 7: en_cg_elem<7>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        case 8: en_cg_elem<8>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        case 9: en_cg_elem<9>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
-        default: en_cg_elem<10>(tm, M, e, md, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 3: en_cg_elem<3>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 4: en_cg_elem<4>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 5: en_cg_elem<5>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 6: en_cg_elem<6>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 7: en_cg_elem<7>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 8: en_cg_elem<8>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        case 9: en_cg_elem<9>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
+        default: en_cg_elem<10>(tm, M, e, md, f64, Df, Wf, Dd, Wd, slice, a.p, a.q); break;
       }
     }
     __syncwarp();
@@ -513,42 +592,64 @@ __device__ __forceinline__ double en_warp_fold(double v, bool max) {
   return v;
 }
 
-struct EnAcc {  // per-member, per-warp partials in shared memory
-  double v[EN_MAXMEM][2][EN_MAXWARPS];
-};
-
-__device__ __forceinline__ void en_acc_put(EnAcc &s, int mi, double a0, double a1, bool max1) {
-  a0 = en_warp_fold(a0, false);
-  a1 = en_warp_fold(a1, max1);
-  if ((threadIdx.x & 31) == 0) {
-    s.v[mi][0][threadIdx.x >> 5] = a0;
-    s.v[mi][1][threadIdx.x >> 5] = a1;
+// The CG's lattice work in warp slices: slice s of member m covers the
+// lattice nodes [s EN_WS, min((s+1) EN_WS, nL)); the slices of all members
+// are numbered consecutively (prefix spref) and the grid's warps take them
+// round robin, so a slice's warp is the same in every phase of a launch and
+// reads back its own writes.  f(mi, M, c, hi, a0, a1) runs the calling
+// lane's nodes c, c + 32, ... < hi; with `part` the warp's folded sums of
+// slice s go to partials[2 s] and partials[2 s + 1].
+template <class F>
+__device__ __forceinline__ void en_ws_loop(const EnArgs &a, const int64_t *spref, const int *act,
+                                           bool part, bool max1, F f) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  const int64_t nw = (int64_t)gridDim.x * wpb;
+  for (int64_t ws = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); ws < a.nclass; ws += nw) {
+    const int mi = en_find(spref, a.nmem, ws);
+    if (!act[mi]) continue;  // warp-uniform
+    const EnMember &M = a.mem[mi];
+    const int64_t lo = (ws - spref[mi]) * EN_WS;
+    const int64_t hi = lo + EN_WS < M.nL ? lo + EN_WS : M.nL;
+    double a0 = 0.0, a1 = 0.0;
+    f(mi, M, lo + lane, hi, a0, a1);
+    if (part) {
+      a0 = en_warp_fold(a0, false);
+      a1 = en_warp_fold(a1, max1);
+      if (lane == 0) {
+        a.partials[2 * ws] = a0;
+        a.partials[2 * ws + 1] = a1;
+      }
+    }
   }
 }
 
-__device__ void en_acc_publish(const EnArgs &a, EnAcc &s, const int *active, bool max1) {
-  __syncthreads();
-  const int wpb = blockDim.x >> 5;
-  for (int t = threadIdx.x; t < 2 * a.nmem; t += blockDim.x) {
-    const int mi = t >> 1, k = t & 1;
-    if (!active[mi]) continue;
-    double v = s.v[mi][k][0];
-    for (int w = 1; w < wpb; w++) v = (k == 1 && max1) ? fmax(v, s.v[mi][k][w]) : v + s.v[mi][k][w];
-    a.partials[(int64_t)(mi * 2 + k) * gridDim.x + blockIdx.x] = v;
-  }
-}
-
-// In the last block: the two totals of member mi (one warp), valid in all
-// lanes.
-__device__ __forceinline__ void en_acc_total(const EnArgs &a, int mi, bool max1, double &t0,
-                                             double &t1) {
+// In the last block: the two totals of member mi over its slices (one
+// warp), valid in all lanes.  Lane l folds slices l, l + 32, ... in order
+// (four loads issued ahead of the adds), then the lanes fold in a fixed
+// tree: deterministic for a given member layout.
+__device__ __forceinline__ void en_acc_total(const EnArgs &a, const int64_t *spref, int mi,
+                                             bool max1, double &t0, double &t1) {
   const int lane = threadIdx.x & 31;
+  const int64_t s0 = spref[mi], s1 = spref[mi + 1];
   double v0 = 0.0, v1 = 0.0;
-  const volatile double *p0 = a.partials + (int64_t)(mi * 2) * gridDim.x;
-  const volatile double *p1 = p0 + gridDim.x;
-  for (int b = lane; b < (int)gridDim.x; b += 32) {
-    v0 += p0[b];
-    v1 = max1 ? fmax(v1, p1[b]) : v1 + p1[b];
+  int64_t s = s0 + lane;
+  for (; s + 96 < s1; s += 128) {
+    double x[4], y[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      x[k] = __ldcg(a.partials + 2 * (s + 32 * k));
+      y[k] = __ldcg(a.partials + 2 * (s + 32 * k) + 1);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      v0 += x[k];
+      v1 = max1 ? fmax(v1, y[k]) : v1 + y[k];
+    }
+  }
+  for (; s < s1; s += 32) {
+    v0 += __ldcg(a.partials + 2 * s);
+    const double y = __ldcg(a.partials + 2 * s + 1);
+    v1 = max1 ? fmax(v1, y) : v1 + y;
   }
   t0 = en_warp_fold(v0, false);
   t1 = en_warp_fold(v1, max1);
@@ -558,74 +659,89 @@ __device__ __forceinline__ double en_norm(const EnArgs &a, const EnCG &s, double
   return a.normtype == GF_NORM_INF ? t : sqrt(t / s.nd);
 }
 
-__device__ __forceinline__ void en_slice(int64_t nL, int64_t &lo, int64_t &hi) {
-  lo = nL * blockIdx.x / gridDim.x;
-  hi = nL * (blockIdx.x + 1) / gridDim.x;
-}
-
-__device__ __forceinline__ double en_nterm(bool inf, int cnt, double r) {
-  return inf ? fabs(r) : (double)cnt * r * r;
+// norm contribution of a lattice value r with `cnt` element copies
+__device__ __forceinline__ void en_nacc(bool inf, double &acc, int cnt, double r) {
+  acc = inf ? fmax(acc, fabs(r)) : acc + (double)cnt * r * r;
 }
 
 // One CG iteration of every member still running (see the file comment).
+// A member is in one of three states: INNER (one PCG iteration: FP32
+// vectors in the mixed solve, FP64 in the FP64 solve), REFINE (the FP64
+// residual r = mask DSS_Sum(b - A (x + d)) with x += d, then the restart of
+// the FP32 run, or in the reliable-update form the residual replaced under
+// the kept search direction; the FP64 solve passes here once, at its
+// start) or DONE.  a.all_inner (the autotuner) runs every member as INNER
+// and leaves the states alone.
 __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
-  __shared__ int64_t s_cpref[EN_MAXMEM + 1];
-  __shared__ int s_mode[EN_MAXMEM], s_act[EN_MAXMEM];
-  __shared__ EnAcc s_acc;
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_spref[EN_MAXMEM + 1];
+  __shared__ int s_mode[EN_MAXMEM], s_act[EN_MAXMEM], s_act3[EN_MAXMEM];
   en_load_pref(a.chunk_pref, s_cpref, a.nmem);
+  en_load_pref(a.class_pref, s_spref, a.nmem);
   for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) {
-    s_mode[i] = __ldcg(&a.cg[i].next);
+    s_mode[i] = a.all_inner ? EN_INNER : __ldcg(&a.cg[i].next);
     s_act[i] = s_mode[i] != EN_DONE;
   }
   __syncthreads();
-  const bool inf = a.normtype == GF_NORM_INF;
-  // 1. element applies: INNER q_E = A w (FP32); REFINE a_E = A (x + d) (FP64)
+  const bool inf = a.normtype == GF_NORM_INF, f64 = a.fp64 != 0;
+  const bool tune = a.all_inner != 0;
+  // 1. element applies: INNER q_E = A w; REFINE a_E = A (x + d) (FP64)
   en_cg_elements(a, s_cpref, s_mode);
   en_barrier(a.ctl, NoWork{});
   // 2. assembly: INNER q = mask DSS_Sum(q_E), <w, q>; REFINE x += d,
   //    r = mask (b_L - DSS_Sum(a_E)), norm(r)
-  for (int mi = 0; mi < a.nmem; mi++) {
-    if (!s_act[mi]) continue;
-    const EnMember &M = a.mem[mi];
-    int64_t lo, hi;
-    en_slice(M.nL, lo, hi);
-    double a0 = 0.0, a1 = 0.0;
-    if (s_mode[mi] == EN_INNER) {
-      const float *qE = (const float *)M.aE;
-      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
-        const BoxCopies k = M.walk.copies((int)c);
-        float s = 0.f;
-        k.each([&](int m) { s = __fadd_rn(s, __ldcg(qE + m)); });
-        const float qv = (!M.maskL8 || M.maskL8[c]) ? s : 0.f;
-        M.q32[c] = qv;
-        a0 += (double)M.w32[c] * (double)qv;
-      }
-    } else {
-      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
-        const BoxCopies k = M.walk.copies((int)c);
-        double s = 0.0;
-        k.each([&](int m) { s = __dadd_rn(s, __ldcg(M.aE + m)); });
-        M.xL[c] = M.xL[c] + (double)M.dL[c];
-        M.dL[c] = 0.f;
-        const double r = (!M.maskL8 || M.maskL8[c]) ? M.bL[c] - s : 0.0;
-        M.r64[c] = r;
-        a1 = inf ? fmax(a1, fabs(r)) : a1 + en_nterm(false, k.count(), r);
-      }
-    }
-    en_acc_put(s_acc, mi, a0, a1, inf);
-  }
-  en_acc_publish(a, s_acc, s_act, inf);
+  en_ws_loop(a, s_spref, s_act, true, inf,
+             [&](int mi, const EnMember &M, int64_t c, int64_t hi, double &a0, double &a1) {
+               const uint8_t *__restrict__ mk = M.maskL8;
+               if (s_mode[mi] == EN_INNER && !f64) {
+                 const float *__restrict__ qE = (const float *)M.aE;
+                 const float *__restrict__ w = M.w32;
+                 float *__restrict__ q = M.q32;
+#pragma unroll 4
+                 for (; c < hi; c += 32) {
+                   const BoxCopies k = M.walk.copies((int)c);
+                   float sm = 0.f;
+                   k.each([&](int m) { sm = __fadd_rn(sm, __ldcg(qE + m)); });
+                   const float qv = (!mk || mk[c]) ? sm : 0.f;
+                   q[c] = qv;
+                   a0 += (double)w[c] * (double)qv;
+                 }
+               } else if (s_mode[mi] == EN_INNER) {
+                 const double *__restrict__ qE = M.aE;
+                 const double *__restrict__ w = M.w64;
+                 double *__restrict__ q = M.q64;
+#pragma unroll 4
+                 for (; c < hi; c += 32) {
+                   const BoxCopies k = M.walk.copies((int)c);
+                   double sm = 0.0;
+                   k.each([&](int m) { sm = __dadd_rn(sm, __ldcg(qE + m)); });
+                   const double qv = (!mk || mk[c]) ? sm : 0.0;
+                   q[c] = qv;
+                   a0 += w[c] * qv;
+                 }
+               } else {
+                 for (; c < hi; c += 32) {
+                   const BoxCopies k = M.walk.copies((int)c);
+                   double sm = 0.0;
+                   k.each([&](int m) { sm = __dadd_rn(sm, __ldcg(M.aE + m)); });
+                   M.xL[c] = M.xL[c] + (double)M.dL[c];
+                   M.dL[c] = 0.f;
+                   const double r = (!M.maskL8 || M.maskL8[c]) ? M.bL[c] - sm : 0.0;
+                   M.r64[c] = r;
+                   en_nacc(inf, a1, k.count(), r);
+                 }
+               }
+             });
   en_barrier(a.ctl, [&] {
     const int wpb = blockDim.x >> 5, wib = threadIdx.x >> 5;
     for (int mi = wib; mi < a.nmem; mi += wpb) {
       if (!s_act[mi]) continue;
       double t0, t1;
-      en_acc_total(a, mi, inf, t0, t1);
+      en_acc_total(a, s_spref, mi, inf, t0, t1);
       if ((threadIdx.x & 31) != 0) continue;
       EnCG &S = a.cg[mi];
       if (s_mode[mi] == EN_INNER) {
         S.alpha = S.rho / t0;
-        if (!isfinite(S.alpha)) {
+        if (!tune && !isfinite(S.alpha)) {
           S.status = 2;
           S.next = EN_DONE;
         }
@@ -636,66 +752,93 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
         if (!isfinite(rn)) {
           S.status = 2;
           S.next = EN_DONE;
-        } else if (rn <= S.rtol) {
+        } else if (!f64 && rn <= S.rtol) {
           S.status = 0;
           S.next = EN_DONE;
         } else if (S.iters >= a.maxit || S.sweeps > a.max_refine) {
-          S.status = 1;
+          S.status = (rn <= S.rtol) ? 0 : 1;
           S.next = EN_DONE;
         }
       }
     }
   });
-  // 3. INNER: d += alpha w, r -= alpha q, z = Dinv r, <r, z>, norm(r);
-  //    REFINE (not converged): r32 = r, w = z = Dinv r, <r, z>, norm(r)
-  for (int mi = 0; mi < a.nmem; mi++) {
-    if (!s_act[mi]) continue;
-    const EnMember &M = a.mem[mi];
-    const EnCG &S = a.cg[mi];
-    if (__ldcg(&S.next) == EN_DONE) {
-      if (threadIdx.x == 0) s_act[mi] = 0;  // read again only after the next __syncthreads
-      continue;
-    }
-    int64_t lo, hi;
-    en_slice(M.nL, lo, hi);
-    double a0 = 0.0, a1 = 0.0;
-    if (s_mode[mi] == EN_INNER) {
-      const float al = (float)__ldcg(&S.alpha);
-      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
-        const float wv = M.w32[c];
-        M.dL[c] = fmaf(al, wv, M.dL[c]);
-        const float r = fmaf(-al, M.q32[c], M.r32[c]);
-        M.r32[c] = r;
-        const float z = M.dinv32[c] * r;
-        a0 += (double)r * (double)z;
-        const int cnt = inf ? 1 : M.walk.copies((int)c).count();
-        a1 = inf ? fmax(a1, fabs((double)r)) : a1 + en_nterm(false, cnt, (double)r);
-      }
-    } else {
-      for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
-        const float r = (float)M.r64[c];
-        M.r32[c] = r;
-        const float z = M.dinv32[c] * r;
-        M.w32[c] = z;
-        a0 += (double)r * (double)z;
-        const int cnt = inf ? 1 : M.walk.copies((int)c).count();
-        a1 = inf ? fmax(a1, fabs((double)r)) : a1 + en_nterm(false, cnt, (double)r);
-      }
-    }
-    en_acc_put(s_acc, mi, a0, a1, inf);
-  }
+  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x)
+    s_act3[i] = s_act[i] && (tune || __ldcg(&a.cg[i].next) != EN_DONE);
   __syncthreads();
-  en_acc_publish(a, s_acc, s_act, inf);
+  // 3. INNER: x (FP64) or d (FP32) += alpha w, r -= alpha q, z = Dinv r,
+  //    <r, z>, norm(r); REFINE (not finished): z = Dinv r (r32 = r in the
+  //    mixed solve), w = z unless the direction is kept, <r, z>, norm(r)
+  en_ws_loop(a, s_spref, s_act3, true, inf,
+             [&](int mi, const EnMember &M, int64_t c, int64_t hi, double &a0, double &a1) {
+               const EnCG &S = a.cg[mi];
+               const bool inner = s_mode[mi] == EN_INNER;
+               if (inner && !f64) {
+                 const float al = (float)__ldcg(&S.alpha);
+                 float *__restrict__ d = M.dL;
+                 float *__restrict__ rr = M.r32;
+                 const float *__restrict__ w = M.w32;
+                 const float *__restrict__ q = M.q32;
+                 const float *__restrict__ di = M.dinv32;
+#pragma unroll 4
+                 for (; c < hi; c += 32) {
+                   d[c] = fmaf(al, w[c], d[c]);
+                   const float r = fmaf(-al, q[c], rr[c]);
+                   rr[c] = r;
+                   const float z = di[c] * r;
+                   a0 += (double)r * (double)z;
+                   en_nacc(inf, a1, inf ? 1 : M.walk.copies((int)c).count(), (double)r);
+                 }
+               } else if (inner) {
+                 const double al = __ldcg(&S.alpha);
+                 double *__restrict__ x = M.xL;
+                 double *__restrict__ rr = M.r64;
+                 const double *__restrict__ w = M.w64;
+                 const double *__restrict__ q = M.q64;
+                 const double *__restrict__ di = M.dinv64;
+#pragma unroll 4
+                 for (; c < hi; c += 32) {
+                   x[c] = fma(al, w[c], x[c]);
+                   const double r = fma(-al, q[c], rr[c]);
+                   rr[c] = r;
+                   const double z = di[c] * r;
+                   a0 += r * z;
+                   en_nacc(inf, a1, inf ? 1 : M.walk.copies((int)c).count(), r);
+                 }
+               } else if (f64) {
+                 for (; c < hi; c += 32) {
+                   const double r = M.r64[c];
+                   const double z = M.dinv64[c] * r;
+                   M.w64[c] = z;
+                   a0 += r * z;
+                   en_nacc(inf, a1, inf ? 1 : M.walk.copies((int)c).count(), r);
+                 }
+               } else {
+                 const bool keep = a.reliable != 0 && !__ldcg(&S.trig);
+                 for (; c < hi; c += 32) {
+                   const float r = (float)M.r64[c];
+                   M.r32[c] = r;
+                   const float z = M.dinv32[c] * r;
+                   if (!keep) M.w32[c] = z;
+                   a0 += (double)r * (double)z;
+                   en_nacc(inf, a1, inf ? 1 : M.walk.copies((int)c).count(), (double)r);
+                 }
+               }
+             });
   en_barrier(a.ctl, [&] {
     const int wpb = blockDim.x >> 5, wib = threadIdx.x >> 5;
     for (int mi = wib; mi < a.nmem; mi += wpb) {
-      if (!s_act[mi]) continue;
+      if (!s_act3[mi]) continue;
       double t0, t1;
-      en_acc_total(a, mi, inf, t0, t1);
+      en_acc_total(a, s_spref, mi, inf, t0, t1);
       if ((threadIdx.x & 31) != 0) continue;
       EnCG &S = a.cg[mi];
       const double rn = en_norm(a, S, t1);
+      if (tune) {
+        S.beta = 0.0;
+        continue;
+      }
       if (s_mode[mi] == EN_INNER) {
+        const double rho_prev = S.rho;
         S.beta = t0 / S.rho;
         S.rho = t0;
         S.rnorm = rn;
@@ -703,34 +846,83 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
         if (!isfinite(S.beta) || !isfinite(rn)) {
           S.status = 2;
           S.next = EN_DONE;
+        } else if (f64) {  // GCG's loop test on the recurrence residual
+          if (rn <= S.rtol) {
+            S.status = 0;
+            S.next = EN_DONE;
+          } else if (S.iters >= a.maxit) {
+            S.status = 1;
+            S.next = EN_DONE;
+          }
+        } else if (a.reliable && !S.trig) {  // FP64 check at convergence or every check_every
+          if (rn <= S.rtol || S.iters % a.check_every == 0 || S.iters >= a.maxit) {
+            // the replaced residual takes this iteration's direction update:
+            // keep the rho of its alpha for the replacement's beta.  When the
+            // FP32 residual met the stop test the replacement restarts
+            // instead (w = z): past the FP32 accuracy floor a kept direction
+            // stalls
+            S.next = EN_REFINE;
+            S.rho = rho_prev;
+            S.trig = rn <= S.rtol;
+          }
         } else if (rn <= S.itol || S.iters >= a.maxit) {
           S.next = EN_REFINE;
         }
       } else {
+        // the kept direction continues with beta = rho'/rho (0 at the start)
+        S.beta = (a.reliable && !S.trig && S.rho != 0.0) ? t0 / S.rho : 0.0;
         S.rho = t0;
         S.rnorm = rn;
-        S.itol = fmax(a.inner_tol * rn, 0.25 * S.rtol);
+        // restart target; the reliable form falls back to it after its FP32
+        // residual met the stop test and the FP64 one did not
+        S.itol = fmax((a.inner_tol > 0.0 ? a.inner_tol : 1e-4) * rn, 0.25 * S.rtol);
         S.next = (rn > 0.0 && isfinite(t0)) ? EN_INNER : EN_REFINE;
+        if (f64 && !(rn > 0.0)) {  // exact solution: nothing to iterate
+          S.status = 0;
+          S.next = EN_DONE;
+        }
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !tune) {
       int any = 0;
       for (int mi = 0; mi < a.nmem; mi++) any |= (a.cg[mi].next != EN_DONE);
       a.ctl->any_active = any;
       a.ctl->launches++;
     }
   });
-  // 4. INNER: w = Dinv r + beta w
-  for (int mi = 0; mi < a.nmem; mi++) {
-    if (!s_act[mi] || s_mode[mi] != EN_INNER) continue;
-    const EnMember &M = a.mem[mi];
-    const float be = (float)__ldcg(&a.cg[mi].beta);
-    int64_t lo, hi;
-    en_slice(M.nL, lo, hi);
-    for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x)
-      M.w32[c] = fmaf(be, M.w32[c], M.dinv32[c] * M.r32[c]);
+  // 4. w = Dinv r + beta w: INNER (unless a reliable update replaces the
+  //    residual next); REFINE with a kept direction
+  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) {
+    int w4 = 0;
+    if (s_act3[i]) {
+      const bool inner = s_mode[i] == EN_INNER, keep = a.reliable && !f64;
+      if (inner)
+        w4 = !(keep && !tune && __ldcg(&a.cg[i].next) == EN_REFINE);
+      else
+        w4 = keep && !__ldcg(&a.cg[i].trig);
+    }
+    s_act[i] = w4;
   }
+  __syncthreads();
+  en_ws_loop(a, s_spref, s_act, false, inf,
+             [&](int mi, const EnMember &M, int64_t c, int64_t hi, double &, double &) {
+               if (f64) {
+                 const double be = __ldcg(&a.cg[mi].beta);
+                 double *__restrict__ w = M.w64;
+                 const double *__restrict__ di = M.dinv64;
+                 const double *__restrict__ r = M.r64;
+#pragma unroll 4
+                 for (; c < hi; c += 32) w[c] = fma(be, w[c], di[c] * r[c]);
+               } else {
+                 const float be = (float)__ldcg(&a.cg[mi].beta);
+                 float *__restrict__ w = M.w32;
+                 const float *__restrict__ di = M.dinv32;
+                 const float *__restrict__ r = M.r32;
+#pragma unroll 4
+                 for (; c < hi; c += 32) w[c] = fmaf(be, w[c], di[c] * r[c]);
+               }
+             });
   if (a.has_cond && blockIdx.x == 0 && threadIdx.x == 0) {
     const bool more = __ldcg(&a.ctl->any_active) && !ld_acquire(&a.ctl->err) &&
                       ld_acquire(&a.ctl->launches) < a.launch_cap;
@@ -738,58 +930,57 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
   }
 }
 
-// Solve setup: b_L = DSS_Sum(b_E), x_L from x_E, the Jacobi inverse of the
-// assembled diagonal, norm(b) on the element-local b, the stop threshold.
+// Solve setup: b_L = DSS_Sum(b_E), x_L = mask x_E (solve_impl (2) with
+// xb = 0, gcg.ipp:362-382), the Jacobi inverse of the assembled diagonal,
+// norm(b) on the element-local b, the stop threshold.
 __global__ void __launch_bounds__(512) k_en_cg_init(EnArgs a) {
+  __shared__ int64_t s_spref[EN_MAXMEM + 1];
   __shared__ int s_act[EN_MAXMEM];
-  __shared__ EnAcc s_acc;
+  en_load_pref(a.class_pref, s_spref, a.nmem);
   for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) s_act[i] = 1;
   __syncthreads();
   const bool inf = a.normtype == GF_NORM_INF;
-  for (int mi = 0; mi < a.nmem; mi++) {
-    const EnMember &M = a.mem[mi];
-    const int N = M.N, NN = N * N;
-    int64_t lo, hi;
-    en_slice(M.nL, lo, hi);
-    double a1 = 0.0;
-    for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
-      const BoxCopies k = M.walk.copies((int)c);
-      double s = 0.0, dg = 0.0, x0 = 0.0;
-      bool first = true;
-      k.each([&](int m) {
-        const double bv = M.bE[m];
-        s = __dadd_rn(s, bv);
-        a1 = inf ? fmax(a1, fabs(bv)) : a1 + bv * bv;
-        if (first) x0 = M.xE[m];
-        first = false;
-        const int64_t e = m / NN;
-        const int loc = (int)(m - e * NN), i = loc % N, j = loc / N;
-        const double X0 = M.egeom64[e * 3], X1 = M.egeom64[e * 3 + 1], J = M.egeom64[e * 3 + 2];
-        dg += a.p * (X0 * X0 * J * M.W[j] * M.K1d[i] + X1 * X1 * J * M.W[i] * M.K1d[j]) +
-              a.q * J * M.W[i] * M.W[j];
-      });
-      M.bL[c] = s;
-      M.xL[c] = x0;
-      M.dL[c] = 0.f;
-      M.w32[c] = 0.f;
-      const double di = dg != 0.0 ? 1.0 / dg : 1.0;
-      M.dinv64[c] = di;
-      M.dinv32[c] = (float)di;
-    }
-    en_acc_put(s_acc, mi, 0.0, a1, inf);
-  }
-  en_acc_publish(a, s_acc, s_act, inf);
+  en_ws_loop(a, s_spref, s_act, true, inf,
+             [&](int mi, const EnMember &M, int64_t c, int64_t hi, double &, double &a1) {
+               const int N = M.N, NN = N * N;
+               for (; c < hi; c += 32) {
+                 const BoxCopies k = M.walk.copies((int)c);
+                 double sm = 0.0, dg = 0.0, x0 = 0.0;
+                 bool first = true;
+                 k.each([&](int m) {
+                   const double bv = M.bE[m];
+                   sm = __dadd_rn(sm, bv);
+                   a1 = inf ? fmax(a1, fabs(bv)) : a1 + bv * bv;
+                   if (first) x0 = M.xE[m];
+                   first = false;
+                   const int64_t e = m / NN;
+                   const int loc = (int)(m - e * NN), i = loc % N, j = loc / N;
+                   const double X0 = M.egeom64[e * 3], X1 = M.egeom64[e * 3 + 1],
+                                J = M.egeom64[e * 3 + 2];
+                   dg += a.p * (X0 * X0 * J * M.W[j] * M.K1d[i] + X1 * X1 * J * M.W[i] * M.K1d[j]) +
+                         a.q * J * M.W[i] * M.W[j];
+                 });
+                 M.bL[c] = sm;
+                 M.xL[c] = (!M.maskL8 || M.maskL8[c]) ? x0 : 0.0;  // x = mask x + xb, xb = 0
+                 M.dL[c] = 0.f;
+                 M.w32[c] = 0.f;
+                 M.w64[c] = 0.0;
+                 const double di = dg != 0.0 ? 1.0 / dg : 1.0;
+                 M.dinv64[c] = di;
+                 M.dinv32[c] = (float)di;
+               }
+             });
   en_barrier(a.ctl, [&] {
     const int wpb = blockDim.x >> 5, wib = threadIdx.x >> 5;
     for (int mi = wib; mi < a.nmem; mi += wpb) {
       double t0, t1;
-      en_acc_total(a, mi, inf, t0, t1);
+      en_acc_total(a, s_spref, mi, inf, t0, t1);
       if ((threadIdx.x & 31) != 0) continue;
       EnCG &S = a.cg[mi];
       S.bnorm = en_norm(a, S, t1);
       S.rtol = (a.relative || S.bnorm >= 1.0) ? a.tol * S.bnorm : a.tol;
       S.next = EN_REFINE;
-      S.iters = S.sweeps = S.status = 0;
+      S.iters = S.sweeps = S.status = S.trig = 0;
       S.rho = S.alpha = S.beta = 0.0;
       S.rnorm = S.rnorm64 = S.bnorm;
     }
@@ -818,16 +1009,6 @@ __global__ void k_en_cg_finish(EnArgs a) {
   }
 }
 
-// element phase alone, every member INNER (the autotuner's timing kernel)
-__global__ void __launch_bounds__(512) k_en_cg_tune(EnArgs a) {
-  __shared__ int64_t s_cpref[EN_MAXMEM + 1];
-  __shared__ int s_mode[EN_MAXMEM];
-  en_load_pref(a.chunk_pref, s_cpref, a.nmem);
-  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) s_mode[i] = EN_INNER;
-  __syncthreads();
-  en_cg_elements(a, s_cpref, s_mode);
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -837,6 +1018,7 @@ struct EnShape {
   int threads = 256, bps = 0;  // bps 0: as many as fit
   int team[EN_MAXN + 1];       // lanes per element, by point count
   bool tuned = false;
+  float ms = -1.f;  // the tuner's time per launch of the chosen shape
   EnShape() {
     for (int n = 0; n <= EN_MAXN; n++) team[n] = n * n <= 16 ? 8 : (n * n <= 48 ? 16 : 32);
   }
@@ -868,6 +1050,7 @@ struct gf_ensemble {
   double cg_pkey[5] = {};  // p, q, tol, inner_tol, relative|normtype|maxit|max_refine
   int rk_eqn = -1;         // equation of the last RK advance (the tuner runs it)
   double rk_nu = 0.0;
+  int cg_fp64 = 0;         // precision of the last CG solve (the tuner runs it)
   bool cooperative = true;
   uint64_t launches = 0;
   int last_grid = 0;
@@ -927,8 +1110,6 @@ int en_grid(gf_ensemble *E, int which, int threads, int bps, int wbytes) {
     return 0;
   }
   if (which == 2) {
-    cudaFuncSetAttribute((const void *)k_en_cg_tune, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
     int occ2 = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, other, threads, smem) != cudaSuccess) {
       cudaGetLastError();
@@ -943,12 +1124,16 @@ int en_grid(gf_ensemble *E, int which, int threads, int bps, int wbytes) {
 
 // Chunk and class numbering for shape `which`; fills descriptor offsets and
 // the prefix arrays (host), returns totals.
+// Work numbering of shape `which`: element chunks (cpref); RK node items
+// (kpref, all nodes) and shared classes (spref); CG lattice warp slices
+// (kpref).
 void en_layout(gf_ensemble *E, int which, std::vector<int64_t> &cpref, std::vector<int64_t> &kpref,
-               int64_t &nchunk, int64_t &nclass) {
+               std::vector<int64_t> &spref, int64_t &nchunk, int64_t &nclass, int64_t &nsh) {
   const int n = (int)E->probs.size();
   cpref.assign(n + 1, 0);
   kpref.assign(n + 1, 0);
-  nchunk = nclass = 0;
+  spref.assign(n + 1, 0);
+  nchunk = nclass = nsh = 0;
   for (int m = 0; m < n; m++) {
     EnMember &M = E->host[m];
     M.team = E->shape[which].team[M.N];
@@ -958,18 +1143,21 @@ void en_layout(gf_ensemble *E, int which, std::vector<int64_t> &cpref, std::vect
     M.class0 = nclass;
     cpref[m] = nchunk;
     kpref[m] = nclass;
+    spref[m] = nsh;
     nchunk += M.nchunk;
-    nclass += which == 2 ? M.nL : M.nclass;
+    nclass += which == 2 ? (M.nL + EN_WS - 1) / EN_WS : M.nlocal;
+    nsh += which == 2 ? 0 : M.nshared;
   }
   cpref[n] = nchunk;
   kpref[n] = nclass;
+  spref[n] = nsh;
 }
 
 int en_upload(gf_ensemble *E, int which, EnArgs &a) {
   gf_context *ctx = E->ctx;
-  std::vector<int64_t> cp, kp;
-  int64_t nchunk, nclass;
-  en_layout(E, which, cp, kp, nchunk, nclass);
+  std::vector<int64_t> cp, kp, sp;
+  int64_t nchunk, nclass, nsh;
+  en_layout(E, which, cp, kp, sp, nchunk, nclass, nsh);
   const int n = (int)E->probs.size();
   cudaStream_t st = ctx->stream;
   GF_CUDA(ctx, cudaMemcpyAsync(E->mem_d, E->host.data(), sizeof(EnMember) * n,
@@ -978,6 +1166,8 @@ int en_upload(gf_ensemble *E, int which, EnArgs &a) {
                                cudaMemcpyHostToDevice, st));
   GF_CUDA(ctx, cudaMemcpyAsync(E->pref_d + EN_MAXMEM + 1, kp.data(), sizeof(int64_t) * (n + 1),
                                cudaMemcpyHostToDevice, st));
+  GF_CUDA(ctx, cudaMemcpyAsync(E->pref_d + 2 * (EN_MAXMEM + 1), sp.data(),
+                               sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
   // the host arrays are pageable: finish the copies before they change
   GF_CUDA(ctx, cudaStreamSynchronize(st));
   memset(&a, 0, sizeof(a));
@@ -985,8 +1175,10 @@ int en_upload(gf_ensemble *E, int which, EnArgs &a) {
   a.nmem = n;
   a.chunk_pref = E->pref_d;
   a.class_pref = E->pref_d + EN_MAXMEM + 1;
+  a.sh_pref = E->pref_d + 2 * (EN_MAXMEM + 1);
   a.nchunk = nchunk;
   a.nclass = nclass;
+  a.nsh = nsh;
   a.ctl = E->ctl_d;
   a.cg = E->cg_d;
   a.partials = E->partials;
@@ -1006,12 +1198,11 @@ cudaError_t en_launch(gf_ensemble *E, const void *k, int grid, int threads, size
   at[0].val.cooperative = 1;
   cfg.attrs = coop ? at : nullptr;
   cfg.numAttrs = coop ? 1 : 0;
-  E->launches++;
   return cudaLaunchKernelExC(&cfg, k, args);
 }
 
-int en_check_partials(gf_ensemble *E, int grid) {
-  const size_t need = (size_t)2 * EN_MAXMEM * std::max(grid, 1);
+int en_check_partials(gf_ensemble *E, int64_t nslice) {
+  const size_t need = (size_t)2 * std::max<int64_t>(nslice, 1);
   if (E->partials_n >= need) return GF_OK;
   if (E->partials) cudaFree(E->partials);
   E->partials = nullptr;
@@ -1060,7 +1251,10 @@ int en_buffers(gf_ensemble *E, int which) {
       M.u[1] = en_alloc(E, b);
       for (int k = 0; k < 3; k++) M.K[k] = en_alloc(E, b);
       M.uf = en_alloc(E, b);
-      if (!M.u[1] || !M.K[0] || !M.K[1] || !M.K[2] || !M.uf) goto oom;
+      M.advb[0] = en_alloc(E, b);
+      M.advb[1] = en_alloc(E, b);
+      if (!M.u[1] || !M.K[0] || !M.K[1] || !M.K[2] || !M.uf || !M.advb[0] || !M.advb[1])
+        goto oom;
     } else {
       const size_t L = (size_t)M.nL;
       M.bL = (double *)en_alloc(E, 8 * L);
@@ -1073,8 +1267,10 @@ int en_buffers(gf_ensemble *E, int which) {
       M.w32 = (float *)en_alloc(E, 4 * L);
       M.q32 = (float *)en_alloc(E, 4 * L);
       M.dinv32 = (float *)en_alloc(E, 4 * L);
+      M.w64 = (double *)en_alloc(E, 8 * L);
+      M.q64 = (double *)en_alloc(E, 8 * L);
       if (!M.bL || !M.xL || !M.r64 || !M.dinv64 || !M.aE || !M.dL || !M.r32 || !M.w32 ||
-          !M.q32 || !M.dinv32)
+          !M.q32 || !M.dinv32 || !M.w64 || !M.q64)
         goto oom;
     }
   }
@@ -1093,13 +1289,24 @@ float en_time_shape(gf_ensemble *E, int which, int reps) {
   if (en_upload(E, which, a)) return -1.f;
   const int grid = en_grid(E, which, S.threads, S.bps, a.wbytes);
   if (grid <= 0) return -1.f;
+  // RK: the element phase of stage 0 (no grid barrier); CG: one whole
+  // iteration of every member (cooperative: its barriers and reductions
+  // depend on the block count)
   const void *k = which == 0   ? (const void *)k_en_rk_tune<double>
                   : which == 1 ? (const void *)k_en_rk_tune<float>
-                               : (const void *)k_en_cg_tune;
+                               : (const void *)k_en_cg_iter;
   a.all_inner = 1;
   a.ns = 1;
   a.eqn = E->rk_eqn;
   a.nu = E->rk_nu;
+  a.fp64 = E->cg_fp64;
+  a.check_every = 1;
+  a.fast = E->rk_eqn == GF_EQN_ADVECT && E->rk_nu == 0.0;
+  if (which == 2) {
+    if (en_check_partials(E, a.nclass)) return -1.f;
+    a.partials = E->partials;
+    if (cudaMemsetAsync(E->ctl_d, 0, sizeof(EnCtl), E->ctx->stream) != cudaSuccess) return -1.f;
+  }
   void *args[1] = {&a};
   const size_t smem = (size_t)a.wbytes * (S.threads / 32);
   cudaStream_t st = E->ctx->stream;
@@ -1109,11 +1316,13 @@ float en_time_shape(gf_ensemble *E, int which, int reps) {
   float best = -1.f;
   for (int r = 0; r < reps + 2; r++) {
     cudaEventRecord(e0, st);
-    if (en_launch(E, k, grid, S.threads, smem, st, args, false) != cudaSuccess) {
+    if (en_launch(E, k, grid, S.threads, smem, st, args, which == 2 && E->cooperative) !=
+        cudaSuccess) {
       cudaGetLastError();
       best = -1.f;
       break;
     }
+    E->launches++;
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -1180,6 +1389,10 @@ extern "C" int gf_ensemble_create(gf_ctx_t ctx, int n, const gf_problem_t *membe
     }
     M.class_ptr = p->class_ptr;
     M.members = p->members;
+    M.sh_ptr = p->sh_ptr;
+    M.sh_members = p->sh_members;
+    M.nshared = p->nshared;
+    M.imult32 = p->imult_f;
     if (kind == GF_ENS_RK) {
       M.X[0] = p->dgeom_d;
       M.X[1] = p->dgeom_f;
@@ -1199,7 +1412,7 @@ extern "C" int gf_ensemble_create(gf_ctx_t ctx, int n, const gf_problem_t *membe
     }
   }
   cudaError_t e = cudaMalloc(&E->mem_d, sizeof(EnMember) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&E->pref_d, sizeof(int64_t) * 2 * (EN_MAXMEM + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&E->pref_d, sizeof(int64_t) * 3 * (EN_MAXMEM + 1));
   if (e == cudaSuccess) e = cudaMalloc(&E->ctl_d, sizeof(EnCtl));
   if (e == cudaSuccess) e = cudaMalloc(&E->cg_d, sizeof(EnCG) * EN_MAXMEM);
   if (e == cudaSuccess) e = cudaMallocHost(&E->ctl_h, sizeof(EnCtl));
@@ -1238,7 +1451,7 @@ extern "C" int gf_ensemble_kind(gf_ensemble_t E) { return E ? E->kind : GF_ERR_A
 extern "C" uint64_t gf_ensemble_launches(gf_ensemble_t E) { return E ? E->launches : 0; }
 
 extern "C" int gf_ensemble_shape(gf_ensemble_t E, int dtype, int *threads, int *blocks,
-                                 int *team_by_n, int *tuned) {
+                                 int *team_by_n, int *tuned, double *tuned_ms) {
   if (!E) return GF_ERR_ARG;
   const int w = en_which(E->kind, dtype);
   const EnShape &S = E->shape[w];
@@ -1247,6 +1460,7 @@ extern "C" int gf_ensemble_shape(gf_ensemble_t E, int dtype, int *threads, int *
   if (team_by_n)
     for (int n = 0; n <= EN_MAXN; n++) team_by_n[n] = S.team[n];
   if (tuned) *tuned = S.tuned ? 1 : 0;
+  if (tuned_ms) *tuned_ms = S.ms;
   return GF_OK;
 }
 
@@ -1335,6 +1549,7 @@ extern "C" int gf_ensemble_tune(gf_ensemble_t E, int dtype, int reps) {
     }
   }
   best.tuned = true;
+  best.ms = tbest;
   S = best;
   E->host = saved;
   en_drop_graphs(E);
@@ -1406,9 +1621,28 @@ extern "C" int gf_ensemble_rk_advance(gf_ensemble_t E, int dtype, const gf_rk_tr
   a.ns = ns;
   a.eqn = tr->eqn;
   a.nu = tr->nu;
+  a.fast = tr->eqn == GF_EQN_ADVECT && tr->nu == 0.0;
   const size_t smem = (size_t)a.wbytes * (S.threads / 32);
   const void *k = en_kernel(w);
   cudaStream_t st = ctx->stream;
+  if (a.fast)  // the coefficient planes, by the single-problem stepper's kernel
+    for (int m = 0; m < n; m++) {
+      gf_problem *p = E->probs[m];
+      EnMember &M = E->host[m];
+      const int nc = M.nxy;
+      int r2;
+      if (dtype == GF_F32) {
+        const float *cc[3] = {(const float *)M.c[0], (const float *)M.c[1],
+                              nc > 2 ? (const float *)M.c[2] : nullptr};
+        r2 = gfrk::adv_coef_launch<float>(p, cc, (float *)M.advb[0], (float *)M.advb[1], st);
+      } else {
+        const double *cc[3] = {(const double *)M.c[0], (const double *)M.c[1],
+                               nc > 2 ? (const double *)M.c[2] : nullptr};
+        r2 = gfrk::adv_coef_launch<double>(p, cc, (double *)M.advb[0], (double *)M.advb[1], st);
+      }
+      if (r2) return gf_fail(ctx, r2, "advection coefficients");
+      E->launches++;
+    }
   GF_CUDA(ctx, cudaMemsetAsync(E->ctl_d, 0, sizeof(EnCtl), st));
   // graphs of 2 steps (par 0 then 1) and 1 step (par 0), rebuilt when the
   // scheme or shape changes; the kernels read the descriptors from device
@@ -1452,9 +1686,13 @@ extern "C" int gf_ensemble_rk_advance(gf_ensemble_t E, int dtype, const gf_rk_tr
     return rc;
   if ((nsteps & 1) && (rc = build(1, E->rk_exec[di][0], E->rk_key[di][0], E->rk_nu_key[di][0])))
     return rc;
-  for (int s = 0; s + 1 < nsteps; s += 2) GF_CUDA(ctx, cudaGraphLaunch(E->rk_exec[di][1], st));
+  for (int s = 0; s + 1 < nsteps; s += 2) {
+    GF_CUDA(ctx, cudaGraphLaunch(E->rk_exec[di][1], st));
+    E->launches += 2 * ns;
+  }
   if (nsteps & 1) {
     GF_CUDA(ctx, cudaGraphLaunch(E->rk_exec[di][0], st));
+    E->launches += ns;
     const size_t bytes = (dtype == GF_F32 ? 4 : 8) * 1;
     for (int m = 0; m < n; m++)
       GF_CUDA(ctx, cudaMemcpyAsync(E->host[m].u[0], E->host[m].u[1], bytes * E->host[m].nlocal,
@@ -1478,7 +1716,8 @@ extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, dou
   gf_context *ctx = E->ctx;
   GF_REQUIRE(ctx, E->kind == GF_ENS_CG, "this ensemble holds RK (deformed) members");
   GF_REQUIRE(ctx, tr && b && x, "traits, b and x are required");
-  GF_REQUIRE(ctx, tr->precision == GF_CG_MIXED, "ensemble CG runs FP32 iterations with FP64 refinement");
+  GF_REQUIRE(ctx, tr->precision == GF_CG_MIXED || tr->precision == GF_CG_FP64,
+             "ensemble CG precision: GF_CG_MIXED or GF_CG_FP64");
   GF_REQUIRE(ctx, tr->precond == GF_PRECOND_JACOBI, "ensemble CG takes the Jacobi preconditioner");
   GF_REQUIRE(ctx, tr->normtype == GF_NORM_EUC || tr->normtype == GF_NORM_INF,
              "ensemble CG norms: EUC or INF");
@@ -1502,12 +1741,16 @@ extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, dou
   const EnShape &S = E->shape[2];
   const int grid = en_grid(E, 2, S.threads, S.bps, a.wbytes);
   if (grid <= 0) return gf_fail(ctx, GF_ERR_UNSUPPORTED, "ensemble shape does not fit");
-  if ((rc = en_check_partials(E, grid))) return rc;
+  if ((rc = en_check_partials(E, a.nclass))) return rc;
   a.partials = E->partials;
   a.p = p;
   a.q = q;
   a.tol = tr->tol;
-  a.inner_tol = tr->inner_tol > 0.0 ? tr->inner_tol : 1e-4;
+  a.fp64 = tr->precision == GF_CG_FP64;
+  a.reliable = !a.fp64 && !(tr->inner_tol > 0.0);
+  a.inner_tol = tr->inner_tol > 0.0 ? tr->inner_tol : 0.0;
+  a.check_every = tr->check_every > 0 ? tr->check_every : 16;
+  E->cg_fp64 = a.fp64;
   a.normtype = tr->normtype;
   a.maxit = tr->maxit;
   a.max_refine = tr->max_refine > 0 ? tr->max_refine : 64;
@@ -1525,13 +1768,15 @@ extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, dou
     void *args[1] = {&a};
     GF_CUDA(ctx, en_launch(E, (const void *)k_en_cg_init, grid, S.threads, smem, st, args,
                            E->cooperative));
+    E->launches++;
   }
   // the iteration loop: a WHILE node whose body is one cooperative launch;
   // the kernel's block 0 clears the condition once no member is running
   // the captured kernel holds p, q and the traits in its arguments
-  const double pkey[5] = {p, q, a.tol, a.inner_tol,
-                          (double)a.relative + 2.0 * a.normtype + 8.0 * a.max_refine +
-                              1024.0 * (double)a.maxit};
+  const double pkey[5] = {p, q, a.tol, a.inner_tol + 1e6 * a.check_every,
+                          (double)a.relative + 2.0 * a.normtype + 8.0 * a.fp64 +
+                              16.0 * a.reliable + 32.0 * a.max_refine +
+                              65536.0 * (double)a.maxit};
   if (!(E->cg_exec && E->cg_key[0] == S.threads && E->cg_key[1] == grid &&
         std::equal(pkey, pkey + 5, E->cg_pkey))) {
     if (E->cg_exec) cudaGraphExecDestroy(E->cg_exec);
@@ -1590,7 +1835,7 @@ extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, dou
   for (int m = 0; m < n; m++) {
     const EnCG &C = E->cg_h[m];
     if (iters) iters[m] = C.iters;
-    if (final_norm) final_norm[m] = C.rnorm64;
+    if (final_norm) final_norm[m] = a.fp64 ? C.rnorm : C.rnorm64;
     if (status) status[m] = C.status;
     if (C.status == 2) worst = GF_ERR_NONFINITE;
     else if (C.status == 1 && worst == GF_OK) worst = GF_CG_NOCONVERGE;

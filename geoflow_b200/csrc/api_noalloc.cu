@@ -18,11 +18,12 @@
 // are read.  Two calls that overlap on the GPU (for example on two streams)
 // race on the array; order them on one stream.
 //
-// In host code the array's name is only a host-side stand-in, so the first
-// call on each device looks up its device address with cudaGetSymbolAddress
-// (that device current) and passes the address to the kernel.  Make that
-// first call before any stream capture.
-#include <mutex>
+// In host code the array's name is only a host-side stand-in, so every
+// call looks up its device address on the current device with
+// cudaGetSymbolAddress and passes the address to the kernel (cheap once the
+// library's module is loaded there; nothing is cached, so a call after
+// cudaDeviceReset finds the reloaded array).  The first call on a device
+// may load the module: make it before any stream capture.
 
 #include "gf_common.cuh"
 #include "k_vec.cuh"
@@ -37,9 +38,6 @@ constexpr int kThreads = 256;
 // [0, kHeader): the ticket counter (an unsigned int at offset 0);
 // [kHeader, kHeader + kMaxBlocks): one partial sum per block.
 static __device__ __align__(256) double g_noalloc_scratch[kHeader + kMaxBlocks];
-
-std::mutex g_lock;
-void *g_addr[128] = {nullptr};  // device address of the array, per device
 
 __global__ void __launch_bounds__(kThreads)
     k_integrate_noalloc(int64_t n, const double *__restrict__ mass, const double *__restrict__ u,
@@ -74,24 +72,13 @@ extern "C" int gf_integrate_noalloc(int64_t n, const double *mass, const double 
                    (long long)n, (long long)limit);
   if (!result || (n > 0 && (!mass || !u)))
     return gf_fail(nullptr, GF_ERR_ARG, "gf_integrate_noalloc: null pointer");
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
-    return gf_fail(nullptr, GF_ERR_CUDA, "gf_integrate_noalloc: no current CUDA device");
-  void *addr;
-  {
-    std::lock_guard<std::mutex> lk(g_lock);
-    if (!g_addr[dev]) {
-      void *a = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
-      if (e != cudaSuccess || !a)
-        return gf_fail(nullptr, GF_ERR_CUDA, "gf_integrate_noalloc: cudaGetSymbolAddress: %s",
-                       cudaGetErrorString(e));
-      g_addr[dev] = a;
-    }
-    addr = g_addr[dev];
-  }
+  void *addr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+  if (e != cudaSuccess || !addr)
+    return gf_fail(nullptr, GF_ERR_CUDA, "gf_integrate_noalloc: cudaGetSymbolAddress: %s",
+                   cudaGetErrorString(e));
   cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = cudaMemsetAsync(addr, 0, sizeof(unsigned int), st);
+  e = cudaMemsetAsync(addr, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess)
     return gf_fail(nullptr, GF_ERR_CUDA, "gf_integrate_noalloc: %s", cudaGetErrorString(e));
   const unsigned blocks = n > 0 ? (unsigned)((n + kChunk - 1) / kChunk) : 1u;

@@ -359,25 +359,15 @@ int launch_dss(gf_problem *prob, int op, T *u, cudaStream_t st) {
     }
     return GF_OK;
   }
+  const SplitCls sc = split_of(prob);
+  grid = grid_for(sc.n + sc.nsh, 256, prob->ctx->sm_count * 16);
+  prob->launches++;
   switch (op) {
-    case GF_DSS_SUM:
-      prob->launches++;
-      k_dss_csr<T, GF_DSS_SUM><<<grid, 256, 0, st>>>(u, prob->class_ptr, prob->members, prob->nclass);
-      break;
-    case GF_DSS_SMOOTH:
-      prob->launches++;
-      k_dss_csr<T, GF_DSS_SMOOTH><<<grid, 256, 0, st>>>(u, prob->class_ptr, prob->members, prob->nclass);
-      break;
-    case GF_DSS_MAX:
-      prob->launches++;
-      k_dss_csr<T, GF_DSS_MAX><<<grid, 256, 0, st>>>(u, prob->class_ptr, prob->members, prob->nclass);
-      break;
-    case GF_DSS_MIN:
-      prob->launches++;
-      k_dss_csr<T, GF_DSS_MIN><<<grid, 256, 0, st>>>(u, prob->class_ptr, prob->members, prob->nclass);
-      break;
-    default:
-      return GF_ERR_ARG;
+    case GF_DSS_SUM: k_dss_split<T, GF_DSS_SUM><<<grid, 256, 0, st>>>(u, sc); break;
+    case GF_DSS_SMOOTH: k_dss_split<T, GF_DSS_SMOOTH><<<grid, 256, 0, st>>>(u, sc); break;
+    case GF_DSS_MAX: k_dss_split<T, GF_DSS_MAX><<<grid, 256, 0, st>>>(u, sc); break;
+    case GF_DSS_MIN: k_dss_split<T, GF_DSS_MIN><<<grid, 256, 0, st>>>(u, sc); break;
+    default: prob->launches--; return GF_ERR_ARG;
   }
   return GF_OK;
 }

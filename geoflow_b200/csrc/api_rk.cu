@@ -85,9 +85,70 @@ __global__ void k_nonfinite(int64_t n, int nstate, const T *__restrict__ u0,
 }
 
 template <typename T>
+struct AdvLaunch {
+  template <int N>
+  struct F {
+    static int run(gf_problem *prob, const T *u, const T *b0, const T *b1, T *out,
+                   cudaStream_t st) {
+      const Basis<T, N> B = make_basis<T, N>(prob);
+      prob->launches++;
+      k_adv_def<T, N, LoadE<T>><<<(unsigned)((prob->ne + 3) / 4), 128, 0, st>>>(
+          B, prob->ne, LoadE<T>{u}, b0, b1, out);
+      return GF_OK;
+    }
+  };
+};
+
+template <typename T>
+struct AdvCoefLaunch {
+  template <int N>
+  struct F {
+    static int run(gf_problem *prob, const T *const *c, T *b0, T *b1, cudaStream_t st) {
+      const Basis<T, N> B = make_basis<T, N>(prob);
+      prob->launches++;
+      k_adv_coef<T, N><<<grid_for(prob->nlocal, 256, prob->ctx->sm_count * 8), 256, 0, st>>>(
+          B, def_of<T>(prob), c[0], c[1], c[2], imass_of<T>(prob), b0, b1);
+      return GF_OK;
+    }
+  };
+};
+
+template <typename T>
+int adv_coef_launch(gf_problem *prob, const T *const *c, T *b0, T *b1, cudaStream_t st) {
+  return dispatch_n<AdvCoefLaunch<T>::template F>(prob->n, prob, c, b0, b1, st);
+}
+template int adv_coef_launch<double>(gf_problem *, const double *const *, double *, double *,
+                                     cudaStream_t);
+template int adv_coef_launch<float>(gf_problem *, const float *const *, float *, float *,
+                                    cudaStream_t);
+
+template <typename T>
+bool Stepper<T>::adv_ok() const {
+  if (eqn != GF_EQN_ADVECT || nu != T(0) || prob->geom < GF_GEOM_DEFORMED || prob->dim != 2)
+    return false;
+  for (int k = 0; k < gf_nvel(prob); k++)
+    if (!c[k]) return false;
+  return true;
+}
+
+template <typename T>
+bool Stepper<T>::prepare_adv() {
+  advb[0] = advb[1] = nullptr;
+  if (!adv_ok() || !advbuf[0] || !advbuf[1]) return false;
+  const T *cc[3] = {c[0], c[1], gf_nvel(prob) > 2 ? c[2] : nullptr};
+  if (adv_coef_launch<T>(prob, cc, advbuf[0], advbuf[1], st)) return false;
+  advb[0] = advbuf[0];
+  advb[1] = advbuf[1];
+  return true;
+}
+
+template <typename T>
 int Stepper<T>::rhs(T *const *u, T *const *K) {
   const T *f[4] = {nullptr, nullptr, nullptr, nullptr};
   T *o[3] = {nullptr, nullptr, nullptr};
+  if (eqn == GF_EQN_ADVECT && advb[0])
+    return dispatch_n<AdvLaunch<T>::template F>(prob->n, prob, (const T *)u[0],
+                                                (const T *)advb[0], (const T *)advb[1], K[0], st);
   if (eqn == GF_EQN_ADVECT) {
     f[0] = u[0];
     for (int k = 0; k < gf_nvel(prob); k++) f[1 + k] = c[k];
@@ -174,27 +235,27 @@ template <typename T>
 void Stepper<T>::euler_smooth(T *x, T dt, const T *uin, T a, const T *y, T b, T a2, const T *y2,
                               T b2) {
   prob->launches++;
-  k_dss_rk_csr<T, FUSE_EULER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256, 0,
-                                st>>>(x, prob->class_ptr, prob->members, prob->nclass, dt, uin,
-                                      a, y, b, a2, y2, b2, nullptr, nullptr, T(0));
+  const SplitCls sc = split_of(prob);
+  k_dss_rk_split<T, FUSE_EULER><<<grid_for(sc.n + sc.nsh, 256, prob->ctx->sm_count * 16), 256, 0,
+                                  st>>>(x, sc, dt, uin, a, y, b, a2, y2, b2, nullptr, nullptr, T(0));
 }
 
 template <typename T>
 void Stepper<T>::smooth_accum(T *K, T ch, T *uout) {
   prob->launches++;
-  k_dss_rk_csr<T, FUSE_ACCUM_AFTER><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16), 256,
-                                      0, st>>>(K, prob->class_ptr, prob->members, prob->nclass,
-                                               T(0), nullptr, T(0), nullptr, T(0), T(0),
-                                               nullptr, T(0), uout, nullptr, ch);
+  const SplitCls sc = split_of(prob);
+  k_dss_rk_split<T, FUSE_ACCUM_AFTER><<<grid_for(sc.n + sc.nsh, 256, prob->ctx->sm_count * 16), 256,
+                                        0, st>>>(K, sc, T(0), nullptr, T(0), nullptr, T(0), T(0),
+                                                 nullptr, T(0), uout, nullptr, ch);
 }
 
 template <typename T>
 void Stepper<T>::accum_smooth(T *uout, const T *K, T ch) {
   prob->launches++;
-  k_dss_rk_csr<T, FUSE_ACCUM_BEFORE><<<grid_for(prob->nclass, 256, prob->ctx->sm_count * 16),
-                                       256, 0, st>>>(uout, prob->class_ptr, prob->members,
-                                                     prob->nclass, T(0), nullptr, T(0), nullptr,
-                                                     T(0), T(0), nullptr, T(0), nullptr, K, ch);
+  const SplitCls sc = split_of(prob);
+  k_dss_rk_split<T, FUSE_ACCUM_BEFORE><<<grid_for(sc.n + sc.nsh, 256, prob->ctx->sm_count * 16),
+                                         256, 0, st>>>(uout, sc, T(0), nullptr, T(0), nullptr, T(0),
+                                                       T(0), nullptr, T(0), nullptr, K, ch);
 }
 
 // Launch k_dss_rk_box_n / k_dss_smooth_box_n for nstate components; false
@@ -289,6 +350,12 @@ bool Stepper<T>::alloc() {
     utmp[k] = (T *)gf_work(prob, slot++, bytes);
     for (int j = 0; j < 3; j++) K[j][k] = (T *)gf_work(prob, slot++, bytes);
     if (!uold[k] || !utmp[k] || !K[0][k] || !K[1][k] || !K[2][k]) return false;
+  }
+  if (adv_ok()) {
+    const int s2 = sizeof(T) == 8 ? 70 : 72;
+    advbuf[0] = (T *)gf_work(prob, s2, bytes);
+    advbuf[1] = (T *)gf_work(prob, s2 + 1, bytes);
+    if (!advbuf[0] || !advbuf[1]) return false;
   }
   return true;
 }
@@ -426,6 +493,7 @@ int advance(gf_problem *prob, const gf_rk_traits *tr, void *const *u, const void
   gf_context *ctx = prob->ctx;
   Stepper<T> S(prob, tr, c);
   if (!S.alloc()) return gf_fail(ctx, GF_ERR_NOMEM, "RK work allocation failed");
+  S.prepare_adv();  // advection with a prescribed velocity and nu = 0
   T *uu[3] = {nullptr, nullptr, nullptr};
   for (int k = 0; k < tr->nstate; k++) uu[k] = (T *)u[k];
   for (int s = 0; s < nsteps; s++) {

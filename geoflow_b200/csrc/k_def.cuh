@@ -184,6 +184,64 @@ __device__ __forceinline__ void def_element(const TM &tm, const BB &B, const Def
   }
 }
 
+// ---- pure advection with a prescribed velocity and no diffusion ----
+// GBurgers::dudt_impl's pure-advection branch (pdes/gburgers.ipp:237-245)
+// with nu = 0 reduces to dudt = -M^-1 M sum_k c_k du/dx_k
+//   = b_0 D_0 u + b_1 D_1 u,   b_j = -(imass M) sum_k c_k dXi_j/dX_k,
+// and c is fixed over a step_b advance, so the steppers form b_0, b_1 once
+// per advance (adv_coef_point) and every RHS call reads 2 planes per node
+// instead of the 2 nxy metric planes, nxy velocity components, Jac, the
+// metric G and the inverse mass.  (The diffusion term nu L u vanishes at
+// nu = 0 but for the sign of a zero.)  Rounding differs from the general
+// kernel's order; both steppers use these same functions, so the ensemble
+// and gf_rk_advance agree bit for bit.
+template <typename T>
+__device__ __forceinline__ void adv_coef_point(int64_t node, int li0, int li1, const T *W,
+                                               const DefGeom<T> &g, const T *c0, const T *c1,
+                                               const T *c2, const T *imass, T &b0, T &b1) {
+  const int64_t nl = g.nlocal;
+  const T *cv[3] = {c0, c1, c2};
+  T a[2];
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    T s = g.X[(j * g.nxy + 0) * nl + node] * cv[0][node];
+    for (int k = 1; k < g.nxy; k++) s = fma(g.X[(j * g.nxy + k) * nl + node], cv[k][node], s);
+    a[j] = s;
+  }
+  T mass = W[li0] * W[li1];
+  mass *= g.J[node];
+  const T f = -(imass[node] * mass);
+  b0 = f * a[0];
+  b1 = f * a[1];
+}
+
+// One 2-d element of the advection right-hand side from the coefficient
+// planes (team tm; smem holds N^2 values).
+template <typename T, int N, class LD, class BB, class TM>
+__device__ __forceinline__ void adv_element(const TM &tm, const BB &B, int64_t e, const LD &ld,
+                                            const T *__restrict__ b0, const T *__restrict__ b1,
+                                            T *__restrict__ out, T *su) {
+  constexpr int NN = N * N;
+  const int64_t base = e * NN;
+#pragma unroll 4
+  for (int a = tm.rank(); a < NN; a += tm.size())
+    su[a] = (T)ld.template point2<N>(e, a % N, a / N);
+  tm.sync();
+#pragma unroll 4
+  for (int a = tm.rank(); a < NN; a += tm.size()) {
+    const int i = a % N, j = a / N;
+    const T c0 = b0[base + a], c1 = b1[base + a];
+    T d0 = B.D[i] * su[j * N];
+    T d1 = B.D[j] * su[i];
+#pragma unroll
+    for (int m = 1; m < N; m++) {
+      d0 = fma(B.D[i + m * N], su[j * N + m], d0);
+      d1 = fma(B.D[j + m * N], su[m * N + i], d1);
+    }
+    out[base + a] = fma(c1, d1, c0 * d0);
+  }
+}
+
 template <typename T, int N, int DIM, class LD, typename TO>
 __global__ void __launch_bounds__(256)
     k_def(const __grid_constant__ Basis<T, N> B, const DefGeom<T> g, int64_t ne, int mode, T p,
@@ -197,6 +255,33 @@ __global__ void __launch_bounds__(256)
   if (e >= ne) return;
   def_element<T, N, DIM, LD, TO>(BlockTeam{}, B, g, e, mode, p, pvec, q, qvec, use_mass, ld, nv, c0,
                                  c1, c2, idir, imass, uo, reinterpret_cast<T *>(smem_def));
+}
+
+// The coefficient planes of adv_element on one 2-d problem (one thread per
+// node).
+template <typename T, int N>
+__global__ void k_adv_coef(const __grid_constant__ Basis<T, N> B, const DefGeom<T> g,
+                           const T *__restrict__ c0, const T *__restrict__ c1,
+                           const T *__restrict__ c2, const T *__restrict__ imass,
+                           T *__restrict__ b0, T *__restrict__ b1) {
+  for (int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; node < g.nlocal;
+       node += (int64_t)gridDim.x * blockDim.x) {
+    const int a = (int)(node % (N * N));
+    adv_coef_point<T>(node, a % N, a / N, B.W, g, c0, c1, c2, imass, b0[node], b1[node]);
+  }
+}
+
+// adv_element on one 2-d problem: one element per warp, four per block.
+template <typename T, int N, class LD>
+__global__ void __launch_bounds__(128)
+    k_adv_def(const __grid_constant__ Basis<T, N> B, int64_t ne, const LD ld,
+              const T *__restrict__ b0, const T *__restrict__ b1, T *__restrict__ out) {
+  __shared__ T su[4][N * N];
+  const int w = threadIdx.x >> 5;
+  const int64_t e = (int64_t)blockIdx.x * 4 + w;
+  if (e >= ne) return;  // whole warps
+  adv_element<T, N>(LaneTeam{(int)(threadIdx.x & 31), 32, 0xffffffffu}, B, e, ld, b0, b1, out,
+                    su[w]);
 }
 
 }  // namespace gfk

@@ -1,11 +1,13 @@
 // k_dss.cuh -- direct-stiffness gather-scatter (GGFX::doOp) kernels.
 //
-// One thread per equivalence class: it gathers the class members in
-// ascending local id, folds them exactly as the reference's reduction
-// functors do (comm/ggfx.hpp:36-76: std::accumulate from 0 for Sum and
-// Smooth, std::max/std::min folds from lowest()/max()), and scatters the
-// result to every member.  The fold order is fixed, so FP64 results are
-// bit-identical to the reference's and independent of the launch shape.
+// One thread per equivalence class (a lattice point on box grids, a node
+// of a singleton class or a shared class on CSR grids): it gathers the
+// class members in ascending local id, folds them exactly as the
+// reference's reduction functors do (comm/ggfx.hpp:36-76: std::accumulate
+// from 0 for Sum and Smooth, std::max/std::min folds from lowest()/max()),
+// and scatters the result to every member.  The fold order is fixed, so
+// FP64 results are bit-identical to the reference's and independent of the
+// launch shape.
 #pragma once
 #include <cfloat>
 
@@ -24,30 +26,6 @@ template <> struct Lim<float> {
   static __device__ __forceinline__ float highest() { return FLT_MAX; }
 };
 
-template <typename T, int OP>
-__device__ __forceinline__ T class_fold(const T *__restrict__ u, const int32_t *__restrict__ mem,
-                                        int32_t b, int32_t e) {
-  T acc;
-  if (OP == GF_DSS_SUM || OP == GF_DSS_SMOOTH) {
-    acc = T(0);
-    for (int32_t k = b; k < e; k++) acc = __fadd_rn_t(acc, u[mem[k]]);
-    if (OP == GF_DSS_SMOOTH) acc = acc / (T)(e - b);
-  } else if (OP == GF_DSS_MAX) {
-    acc = Lim<T>::lowest();
-    for (int32_t k = b; k < e; k++) {
-      T v = u[mem[k]];
-      acc = (acc < v) ? v : acc;
-    }
-  } else {
-    acc = Lim<T>::highest();
-    for (int32_t k = b; k < e; k++) {
-      T v = u[mem[k]];
-      acc = (v < acc) ? v : acc;
-    }
-  }
-  return acc;
-}
-
 // The box-lattice walk of a problem whose gather-scatter can take the box
 // kernels below: a GGridBox problem (classes = lattice points) with no
 // periodic direction of a single element (members then come in the
@@ -58,7 +36,7 @@ inline bool dss_box_walk(const gf_problem *prob, BoxWalk &w) {
   return w.sorted;
 }
 
-// class_fold over the copies of one box-lattice point (ascending local id)
+// The GGFX fold over the copies of one box-lattice point (ascending local id)
 template <typename T, int OP>
 __device__ __forceinline__ T box_fold(const T *__restrict__ u, const BoxCopies &k) {
   T acc;
@@ -82,7 +60,7 @@ __device__ __forceinline__ T box_fold(const T *__restrict__ u, const BoxCopies &
   return acc;
 }
 
-// Box-lattice form of k_dss_csr (GGridBox problems, whose classes are the
+// Box-lattice form of k_dss_split (GGridBox problems, whose classes are the
 // lattice points; no periodic direction with a single element): one thread
 // per lattice point in lattice order, the members computed from the
 // point's coordinates (BoxWalk) in ascending local id, so no index arrays
@@ -99,16 +77,64 @@ __global__ void __launch_bounds__(256) k_dss_box(T *__restrict__ u, BoxWalk w) {
   }
 }
 
-template <typename T, int OP>
-__global__ void __launch_bounds__(256)
-    k_dss_csr(T *__restrict__ u, const int32_t *__restrict__ ptr,
-              const int32_t *__restrict__ mem, int64_t nclass) {
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nclass;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t b = ptr[c], e = ptr[c + 1];
-    const T acc = class_fold<T, OP>(u, mem, b, e);
-    for (int32_t k = b; k < e; k++) u[mem[k]] = acc;
+// The classes of a CSR problem split by size: a class with one member (an
+// interior node, most of them on icosahedral and deformed grids) is folded
+// by the thread of that node, in node order (coalesced, no index arrays;
+// imult = 1 marks it), and a class with several members by one thread from
+// the shared-class list (sh_ptr / sh_members, members in ascending local
+// id).  Items: the n nodes, then the nsh shared classes.  Each class is
+// folded exactly as the full CSR walk folds it.
+struct SplitCls {
+  int64_t n;              // element-local nodes
+  const float *imult;     // 1/multiplicity per node
+  const int32_t *shp;     // nsh + 1
+  const int32_t *shm;
+  int64_t nsh;
+};
+
+inline SplitCls split_of(const gf_problem *p) {
+  return SplitCls{p->nlocal, p->imult_f, p->sh_ptr, p->sh_members, p->nshared};
+}
+
+// f(get, cnt): get(k) is the k-th member (ascending local id) of item it's
+// class, cnt the member count; nothing for a node of a shared class.
+template <class F>
+__device__ __forceinline__ void split_item(const SplitCls &s, int64_t it, F f) {
+  if (it < s.n) {
+    if (s.imult[it] != 1.0f) return;
+    f([&](int) { return it; }, 1);
+  } else {
+    const int64_t c = it - s.n;
+    const int32_t b = s.shp[c], e = s.shp[c + 1];
+    f([&](int k) { return (int64_t)s.shm[b + k]; }, e - b);
   }
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(256) k_dss_split(T *__restrict__ u, SplitCls s) {
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < s.n + s.nsh;
+       it += (int64_t)gridDim.x * blockDim.x)
+    split_item(s, it, [&](auto get, int cnt) {
+      T acc;
+      if (OP == GF_DSS_SUM || OP == GF_DSS_SMOOTH) {
+        acc = T(0);
+        for (int k = 0; k < cnt; k++) acc = __fadd_rn_t(acc, u[get(k)]);
+        if (OP == GF_DSS_SMOOTH) acc = acc / (T)cnt;
+      } else if (OP == GF_DSS_MAX) {
+        acc = Lim<T>::lowest();
+        for (int k = 0; k < cnt; k++) {
+          const T v = u[get(k)];
+          acc = (acc < v) ? v : acc;
+        }
+      } else {
+        acc = Lim<T>::highest();
+        for (int k = 0; k < cnt; k++) {
+          const T v = u[get(k)];
+          acc = (v < acc) ? v : acc;
+        }
+      }
+      for (int k = 0; k < cnt; k++) u[get(k)] = acc;
+    });
 }
 
 // ---- gather-scatter fused with the RK stage updates (api_rk.cu) ----
@@ -146,7 +172,7 @@ __device__ __forceinline__ T rk_stage_point(T uin, int nk, const T *__restrict__
 
 enum { FUSE_EULER = 0, FUSE_ACCUM_AFTER = 1, FUSE_ACCUM_BEFORE = 2 };
 
-// One thread per class, members in ascending local id, Smooth fold:
+// One class per item (SplitCls), members in ascending local id, Smooth fold:
 //   FUSE_EULER:        x_m <- rk_euler_point(x_m, ...) folded           (SSP substep)
 //   FUSE_ACCUM_AFTER:  x_m <- fold(x);  acc_m <- rk_accum_point(acc_m, fold, ch)
 //                      (Smooth K_m, then uout += c_m h K_m)
@@ -154,32 +180,31 @@ enum { FUSE_EULER = 0, FUSE_ACCUM_AFTER = 1, FUSE_ACCUM_BEFORE = 2 };
 //                      (uout += c h K, then Smooth uout)
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256)
-    k_dss_rk_csr(T *__restrict__ x, const int32_t *__restrict__ ptr,
-                 const int32_t *__restrict__ mem, int64_t nclass, T dt, const T *__restrict__ uin,
-                 T a, const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2,
-                 T *__restrict__ acc_out, const T *__restrict__ K, T ch) {
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nclass;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t b0 = ptr[c], e0 = ptr[c + 1];
-    T acc = T(0);
-    for (int32_t k = b0; k < e0; k++) {
-      const int64_t m = mem[k];
-      T v = x[m];
-      if (MODE == FUSE_EULER) v = rk_euler_point(v, dt, uin[m], a, y, b, a2, y2, b2, m);
-      if (MODE == FUSE_ACCUM_BEFORE) v = rk_accum_point(v, K[m], ch);
-      acc = __fadd_rn_t(acc, v);
-    }
-    acc = acc / (T)(e0 - b0);
-    for (int32_t k = b0; k < e0; k++) {
-      const int64_t m = mem[k];
-      x[m] = acc;
-      if (MODE == FUSE_ACCUM_AFTER) acc_out[m] = rk_accum_point(acc_out[m], acc, ch);
-    }
-  }
+    k_dss_rk_split(T *__restrict__ x, SplitCls s, T dt, const T *__restrict__ uin, T a,
+                   const T *__restrict__ y, T b, T a2, const T *__restrict__ y2, T b2,
+                   T *__restrict__ acc_out, const T *__restrict__ K, T ch) {
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < s.n + s.nsh;
+       it += (int64_t)gridDim.x * blockDim.x)
+    split_item(s, it, [&](auto get, int cnt) {
+      T acc = T(0);
+      for (int k = 0; k < cnt; k++) {
+        const int64_t m = get(k);
+        T v = x[m];
+        if (MODE == FUSE_EULER) v = rk_euler_point(v, dt, uin[m], a, y, b, a2, y2, b2, m);
+        if (MODE == FUSE_ACCUM_BEFORE) v = rk_accum_point(v, K[m], ch);
+        acc = __fadd_rn_t(acc, v);
+      }
+      acc = acc / (T)cnt;
+      for (int k = 0; k < cnt; k++) {
+        const int64_t m = get(k);
+        x[m] = acc;
+        if (MODE == FUSE_ACCUM_AFTER) acc_out[m] = rk_accum_point(acc_out[m], acc, ch);
+      }
+    });
 }
 
 // The state components of one fused stage update (pointers per component;
-// y, y2, uin, K, acc may be null as in k_dss_rk_csr).
+// y, y2, uin, K, acc may be null as in k_dss_rk_split).
 template <typename T>
 struct RKComps {
   T *x[3];
@@ -187,11 +212,11 @@ struct RKComps {
   T *acc[3];
 };
 
-// Box-lattice form of k_dss_rk_csr (conditions of k_dss_box) on every
+// Box-lattice form of k_dss_rk_split (conditions of k_dss_box) on every
 // state component in one pass: the copies of a lattice point are computed
 // once, and every component's members are read before any is written (all
 // loads of a point in one memory round trip).  Per component the same
-// stage arithmetic, Smooth fold and order as k_dss_rk_csr: bit-identical.
+// stage arithmetic, Smooth fold and order as k_dss_rk_split: bit-identical.
 template <typename T, int MODE, int NC>
 __global__ void __launch_bounds__(256, 5)
     k_dss_rk_box_n(RKComps<T> p, BoxWalk w, T dt, T a, T b, T a2, T b2, T ch) {

@@ -6,6 +6,10 @@
 namespace gfrk {
 
 void butcher(int order, double *alpha, double beta[4][4], double *c);
+// the coefficient planes of the advection fast path (k_def.cuh
+// adv_coef_point) of a 2-d deformed or embedded problem, velocity c[nxy]
+template <typename T>
+int adv_coef_launch(gf_problem *prob, const T *const *c, T *b0, T *b1, cudaStream_t st);
 int check_traits(gf_problem *prob, const gf_rk_traits *tr, const void *const *u,
                  const void *const *c);
 
@@ -20,6 +24,11 @@ struct Stepper {
   T *uold[3] = {nullptr, nullptr, nullptr};
   T *utmp[3] = {nullptr, nullptr, nullptr};
   T *K[3][3] = {{nullptr}};
+  // advection fast path (prescribed velocity, nu = 0, 2-d deformed or
+  // embedded): coefficient planes b_0, b_1 of adv_element, or null
+  T *advb[2] = {nullptr, nullptr};
+  T *advbuf[2] = {nullptr, nullptr};  // their storage (alloc), unused until prepare_adv
+  bool adv_ok() const;
 
   Stepper(gf_problem *p, const gf_rk_traits *tr, const void *const *cv)
       : prob(p), st(p->ctx->stream), n(p->nlocal), eqn(tr->eqn), nstate(tr->nstate),
@@ -28,6 +37,9 @@ struct Stepper {
       for (int k = 0; k < gf_nvel(p); k++) c[k] = (const T *)cv[k];
   }
   bool alloc();
+  // forms the fast path's coefficients when the problem and equation allow
+  // it (k_def.cuh adv_coef_point); returns false when they do not
+  bool prepare_adv();
   int rhs(T *const *u, T *const *Kout);
   // x = the SSP substep update of dudt(u) before its Smooth (the RHS
   // kernel's MODE_EULER epilogue; 3-d non-deformed problems), then Smooth;

@@ -3,8 +3,9 @@
 The reference runs one problem per process; an ensemble runs many small
 ones at once on one GPU: one persistent cooperative launch per RK stage of
 every member (deformed / embedded 2-d members, e.g. icosahedral-sphere
-advection) or per CG iteration of every member (2-d box Helmholtz solves,
-FP32 iterations with FP64 residual refinement), captured in CUDA graphs.
+advection) or per CG iteration of every member (2-d box Helmholtz solves:
+FP64 iterations, or FP32 iterations with FP64 residual refinement),
+captured in CUDA graphs.
 """
 from __future__ import annotations
 
@@ -84,12 +85,14 @@ class Ensemble:
     def shape(self, dtype=None):
         import torch
         code = A.GF_F32 if dtype in (None, torch.float32) else A.GF_F64
-        th, bl, tu = C.c_int(), C.c_int(), C.c_int()
+        th, bl, tu, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
         team = np.zeros(11, dtype=np.intc)
         self.ctx.check(_lib().gf_ensemble_shape(self.handle, code, C.byref(th), C.byref(bl),
-                                                A.ptr(team), C.byref(tu)), "gf_ensemble_shape")
+                                                A.ptr(team), C.byref(tu), C.byref(ms)),
+                       "gf_ensemble_shape")
         ns = sorted({p.n for p in self.problems})
         return {"threads": th.value, "blocks": bl.value, "tuned": bool(tu.value),
+                "tuned_ms_per_launch": ms.value if tu.value else None,
                 "team_by_n": {n: int(team[n]) for n in ns}}
 
     def set_shape(self, threads, blocks_per_sm=0, team_by_n=None, dtype=None):

@@ -495,15 +495,21 @@ uint64_t gf_ensemble_launches(gf_ensemble_t ens);
 int gf_ensemble_rk_advance(gf_ensemble_t ens, int dtype, const gf_rk_traits *traits,
                            void *const *u, const void *const *c, const double *dt, int nsteps);
 /* Solves (p L + q M) x[m] = b[m] for every member m (device FP64 E-vectors;
- * x holds the initial guess): GCG::solve_impl(A, b, x) (gcg.ipp:239-382) with
- * the Jacobi preconditioner, FP32 iterations and FP64 residual refinement
- * each time an FP32 run has reduced its residual by traits->inner_tol
- * (default 1e-4).  traits: precision GF_CG_MIXED, precond GF_PRECOND_JACOBI,
- * normtype EUC or INF, maxit (FP32 iterations per member), tol, relative,
- * max_refine (default 64).  Per member (host arrays, may be NULL): FP32
- * iterations, the last FP64 residual norm, status 0 converged / 1 no
- * convergence / 2 breakdown.  Returns 0, GF_CG_NOCONVERGE if any member did
- * not converge, or GF_ERR_NONFINITE.  Synchronises. */
+ * x holds the initial guess) with the member's Dirichlet mask applied:
+ * GCG::solve_impl(A, b, xb, x) with xb = 0 (gcg.ipp:239-382; the masked
+ * initial guess, the masked residual; the form without xb masks nothing)
+ * with the Jacobi preconditioner.  traits->precision GF_CG_FP64: FP64
+ * iterations, GCG's stop test on the recurrence residual.  GF_CG_MIXED: FP32
+ * iterations (FP64 dot products) and FP64 residuals: with inner_tol > 0 each
+ * FP32 run restarts from the FP64 residual once it has reduced its own by
+ * inner_tol; with inner_tol = 0 the FP64 residual replaces the FP32 one every
+ * check_every iterations (default 16) under the kept search direction; the
+ * stop test is on the FP64 residual.  traits: precond GF_PRECOND_JACOBI,
+ * normtype EUC or INF, maxit (iterations per member), tol, relative,
+ * max_refine (FP64 residual evaluations, default 64).  Per member (host
+ * arrays, may be NULL): iterations, the final residual norm, status 0
+ * converged / 1 no convergence / 2 breakdown.  Returns 0, GF_CG_NOCONVERGE
+ * if any member did not converge, or GF_ERR_NONFINITE.  Synchronises. */
 int gf_ensemble_cg_solve(gf_ensemble_t ens, const gf_cg_traits *traits, double p, double q,
                          const double *const *b, double *const *x, int *iters,
                          double *final_norm, int *status);
@@ -514,9 +520,12 @@ int gf_ensemble_cg_solve(gf_ensemble_t ens, const gf_cg_traits *traits, double p
  * of its last advance (advection before the first). */
 int gf_ensemble_tune(gf_ensemble_t ens, int dtype, int reps);
 /* The current shape: threads per block, cooperative blocks, lanes per
- * element by GLL point count (team_by_n[n], n <= 10), tuned flag. */
+ * element by GLL point count (team_by_n[n], n <= 10), tuned flag, and the
+ * tuner's measured milliseconds per launch of the timed kernel (the RK
+ * stage's element phase, or one whole CG iteration; -1 before tuning).
+ * Any output may be NULL. */
 int gf_ensemble_shape(gf_ensemble_t ens, int dtype, int *threads, int *blocks, int *team_by_n,
-                      int *tuned);
+                      int *tuned, double *tuned_ms);
 /* Sets a shape (threads 64..512, blocks per SM 0 = as many as fit, team
  * widths 8/16/32 by point count, or NULL to keep them). */
 int gf_ensemble_set_shape(gf_ensemble_t ens, int dtype, int threads, int blocks_per_sm,

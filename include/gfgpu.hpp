@@ -164,6 +164,13 @@ class Helmholtz {
     check(p_.ctx(), gf_helmholtz_apply(p_.get(), GF_F32, lap_, nullptr, q_, nullptr, use_mass_, u, uo),
           "GHelmholtz::opVec_prod");
   }
+  // The reference's three-argument form GHelmholtz::opVec_prod(in, utmp, out)
+  // (sem/ghelmholtz.hpp:58-60, GLinOpBase, sem/glinop_base.hpp:32-34): the
+  // library keeps its own scratch, so utmp is accepted and not touched.
+  template <class Tmp>
+  void opVec_prod(const double *u, Tmp & /*utmp*/, double *uo) { opVec_prod(u, uo); }
+  template <class Tmp>
+  void opVec_prod(const float *u, Tmp & /*utmp*/, float *uo) { opVec_prod(u, uo); }
   double lap() const { return lap_; }
   double mass_scalar() const { return q_; }
   int use_mass() const { return use_mass_; }

@@ -68,6 +68,24 @@ int main() {
   std::printf("cdg_cg: rc=%d iterations=%d err=%.3e\n", rc, cg.iterations(), err);
   if (rc != CG::GCGERR_NONE || !(err < 1e-12)) return 1;
 
+  // the reference's three-argument opVec_prod(in, utmp, out) gives the
+  // two-argument result bit for bit
+  {
+    std::vector<double> utmp;  // stands in for the reference's State utmp
+    double *d_o1 = nullptr, *d_o2 = nullptr;
+    cudaMalloc(&d_o1, N * 8);
+    cudaMalloc(&d_o2, N * 8);
+    L.opVec_prod(d_u, d_o1);
+    L.opVec_prod(d_u, utmp, d_o2);
+    cudaDeviceSynchronize();
+    std::vector<double> o1(N), o2(N);
+    cudaMemcpy(o1.data(), d_o1, N * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(o2.data(), d_o2, N * 8, cudaMemcpyDeviceToHost);
+    cudaFree(d_o1);
+    cudaFree(d_o2);
+    if (std::memcmp(o1.data(), o2.data(), N * 8) != 0) return 3;
+  }
+
   // GGFX Smooth of a continuous field leaves it bit-identical
   std::vector<double> h(N);
   for (int64_t i = 0; i < N; i++) {

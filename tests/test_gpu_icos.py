@@ -55,3 +55,29 @@ def test_cosine_bell_advection_vs_reference(ctx, refpath):
     B = GBurgers(prob, GBurgers.ADVECT, 1e-3, scheme=A.GF_RK4)
     B.step(u, c, dt=float(refpath["icosadv_dt"][0]), nsteps=20)
     assert rel(u[0].cpu().numpy(), refpath["icosadv_u"]) < 1e-10
+
+
+@pytest.mark.parametrize("dtype,bound,tiny", [(torch.float64, 1e-12, 1e-300),
+                                              (torch.float32, 2e-5, 1e-30)])
+def test_prescribed_velocity_fast_path_matches_general_kernel(ctx, dtype, bound, tiny):
+    """Pure advection with nu = 0 takes the coefficient-plane path
+    (k_def.cuh adv_element: b_j = -(imass M) sum_k c_k dXi_j/dX_k formed
+    once per advance); it differs from the general kernel (taken for any
+    nu != 0; here nu = 1e-300 in FP64, 1e-30 in FP32, whose diffusion term
+    is below the rounding)
+    only by rounding order: 1e-12 relative (FP64) and 2e-5 (FP32) after
+    10 RK4 steps on the level-1 p = 5 sphere."""
+    from geoflow_b200 import workloads as W
+    g = IcosGrid(1, 5)
+    prob = g.problem(ctx)
+    u0 = W.icos_cosine_bell(g.xyz, 0.3, 1.2)
+    c = W.icos_solid_body_wind(g.xyz, alpha=0.4)
+    dt = 0.25 * g.minnodedist
+    out = []
+    for nu in (0.0, tiny):
+        u = [torch.from_numpy(u0).to("cuda", dtype)]
+        cc = [torch.from_numpy(a).to("cuda", dtype) for a in c]
+        GBurgers(prob, GBurgers.ADVECT, nu, scheme=A.GF_RK4).step(u, cc, dt=dt, nsteps=10)
+        out.append(u[0].double().cpu().numpy())
+    assert not np.array_equal(out[0], u0)
+    assert rel(out[0], out[1]) < bound
