@@ -90,7 +90,6 @@ struct EnMember {
 struct EnCG {
   double rho, alpha, beta, rnorm, rnorm64, rtol, itol, bnorm, nd;
   int next, iters, sweeps, status;
-  int trig;  // reliable form: the FP32 residual met the stop test (the replacement restarts)
 };
 
 struct EnCtl {
@@ -115,7 +114,7 @@ struct EnArgs {
   // CG
   double p, q, tol, inner_tol;
   int normtype, maxit, max_refine, relative, all_inner;
-  int fp64, reliable, check_every;
+  int fp64;
   unsigned launch_cap;
   cudaGraphConditionalHandle cond;
   int has_cond;
@@ -668,9 +667,7 @@ __device__ __forceinline__ void en_nacc(bool inf, double &acc, int cnt, double r
 // A member is in one of three states: INNER (one PCG iteration: FP32
 // vectors in the mixed solve, FP64 in the FP64 solve), REFINE (the FP64
 // residual r = mask DSS_Sum(b - A (x + d)) with x += d, then the restart of
-// the FP32 run, or in the reliable-update form the residual replaced under
-// the kept search direction; the FP64 solve passes here once, at its
-// start) or DONE.  a.all_inner (the autotuner) runs every member as INNER
+// the FP32 run; the FP64 solve passes here once, at its start) or DONE.  a.all_inner (the autotuner) runs every member as INNER
 // and leaves the states alone.
 __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
   __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_spref[EN_MAXMEM + 1];
@@ -767,7 +764,7 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
   __syncthreads();
   // 3. INNER: x (FP64) or d (FP32) += alpha w, r -= alpha q, z = Dinv r,
   //    <r, z>, norm(r); REFINE (not finished): z = Dinv r (r32 = r in the
-  //    mixed solve), w = z unless the direction is kept, <r, z>, norm(r)
+  //    mixed solve), w = z, <r, z>, norm(r)
   en_ws_loop(a, s_spref, s_act3, true, inf,
              [&](int mi, const EnMember &M, int64_t c, int64_t hi, double &a0, double &a1) {
                const EnCG &S = a.cg[mi];
@@ -813,12 +810,11 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
                    en_nacc(inf, a1, inf ? 1 : M.walk.copies((int)c).count(), r);
                  }
                } else {
-                 const bool keep = a.reliable != 0 && !__ldcg(&S.trig);
                  for (; c < hi; c += 32) {
                    const float r = (float)M.r64[c];
                    M.r32[c] = r;
                    const float z = M.dinv32[c] * r;
-                   if (!keep) M.w32[c] = z;
+                   M.w32[c] = z;
                    a0 += (double)r * (double)z;
                    en_nacc(inf, a1, inf ? 1 : M.walk.copies((int)c).count(), (double)r);
                  }
@@ -838,7 +834,6 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
         continue;
       }
       if (s_mode[mi] == EN_INNER) {
-        const double rho_prev = S.rho;
         S.beta = t0 / S.rho;
         S.rho = t0;
         S.rnorm = rn;
@@ -854,28 +849,15 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
             S.status = 1;
             S.next = EN_DONE;
           }
-        } else if (a.reliable && !S.trig) {  // FP64 check at convergence or every check_every
-          if (rn <= S.rtol || S.iters % a.check_every == 0 || S.iters >= a.maxit) {
-            // the replaced residual takes this iteration's direction update:
-            // keep the rho of its alpha for the replacement's beta.  When the
-            // FP32 residual met the stop test the replacement restarts
-            // instead (w = z): past the FP32 accuracy floor a kept direction
-            // stalls
-            S.next = EN_REFINE;
-            S.rho = rho_prev;
-            S.trig = rn <= S.rtol;
-          }
         } else if (rn <= S.itol || S.iters >= a.maxit) {
           S.next = EN_REFINE;
         }
       } else {
         // the kept direction continues with beta = rho'/rho (0 at the start)
-        S.beta = (a.reliable && !S.trig && S.rho != 0.0) ? t0 / S.rho : 0.0;
+        S.beta = 0.0;
         S.rho = t0;
         S.rnorm = rn;
-        // restart target; the reliable form falls back to it after its FP32
-        // residual met the stop test and the FP64 one did not
-        S.itol = fmax((a.inner_tol > 0.0 ? a.inner_tol : 1e-4) * rn, 0.25 * S.rtol);
+        S.itol = fmax(a.inner_tol * rn, 0.25 * S.rtol);
         S.next = (rn > 0.0 && isfinite(t0)) ? EN_INNER : EN_REFINE;
         if (f64 && !(rn > 0.0)) {  // exact solution: nothing to iterate
           S.status = 0;
@@ -891,19 +873,9 @@ __global__ void __launch_bounds__(512) k_en_cg_iter(EnArgs a) {
       a.ctl->launches++;
     }
   });
-  // 4. w = Dinv r + beta w: INNER (unless a reliable update replaces the
-  //    residual next); REFINE with a kept direction
-  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x) {
-    int w4 = 0;
-    if (s_act3[i]) {
-      const bool inner = s_mode[i] == EN_INNER, keep = a.reliable && !f64;
-      if (inner)
-        w4 = !(keep && !tune && __ldcg(&a.cg[i].next) == EN_REFINE);
-      else
-        w4 = keep && !__ldcg(&a.cg[i].trig);
-    }
-    s_act[i] = w4;
-  }
+  // 4. INNER: w = Dinv r + beta w
+  for (int i = threadIdx.x; i < a.nmem; i += blockDim.x)
+    s_act[i] = s_act3[i] && s_mode[i] == EN_INNER;
   __syncthreads();
   en_ws_loop(a, s_spref, s_act, false, inf,
              [&](int mi, const EnMember &M, int64_t c, int64_t hi, double &, double &) {
@@ -980,7 +952,7 @@ __global__ void __launch_bounds__(512) k_en_cg_init(EnArgs a) {
       S.bnorm = en_norm(a, S, t1);
       S.rtol = (a.relative || S.bnorm >= 1.0) ? a.tol * S.bnorm : a.tol;
       S.next = EN_REFINE;
-      S.iters = S.sweeps = S.status = S.trig = 0;
+      S.iters = S.sweeps = S.status = 0;
       S.rho = S.alpha = S.beta = 0.0;
       S.rnorm = S.rnorm64 = S.bnorm;
     }
@@ -1300,7 +1272,6 @@ float en_time_shape(gf_ensemble *E, int which, int reps) {
   a.eqn = E->rk_eqn;
   a.nu = E->rk_nu;
   a.fp64 = E->cg_fp64;
-  a.check_every = 1;
   a.fast = E->rk_eqn == GF_EQN_ADVECT && E->rk_nu == 0.0;
   if (which == 2) {
     if (en_check_partials(E, a.nclass)) return -1.f;
@@ -1747,9 +1718,7 @@ extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, dou
   a.q = q;
   a.tol = tr->tol;
   a.fp64 = tr->precision == GF_CG_FP64;
-  a.reliable = !a.fp64 && !(tr->inner_tol > 0.0);
-  a.inner_tol = tr->inner_tol > 0.0 ? tr->inner_tol : 0.0;
-  a.check_every = tr->check_every > 0 ? tr->check_every : 16;
+  a.inner_tol = tr->inner_tol > 0.0 ? tr->inner_tol : 1e-4;
   E->cg_fp64 = a.fp64;
   a.normtype = tr->normtype;
   a.maxit = tr->maxit;
@@ -1773,10 +1742,9 @@ extern "C" int gf_ensemble_cg_solve(gf_ensemble_t E, const gf_cg_traits *tr, dou
   // the iteration loop: a WHILE node whose body is one cooperative launch;
   // the kernel's block 0 clears the condition once no member is running
   // the captured kernel holds p, q and the traits in its arguments
-  const double pkey[5] = {p, q, a.tol, a.inner_tol + 1e6 * a.check_every,
+  const double pkey[5] = {p, q, a.tol, a.inner_tol,
                           (double)a.relative + 2.0 * a.normtype + 8.0 * a.fp64 +
-                              16.0 * a.reliable + 32.0 * a.max_refine +
-                              65536.0 * (double)a.maxit};
+                              32.0 * a.max_refine + 65536.0 * (double)a.maxit};
   if (!(E->cg_exec && E->cg_key[0] == S.threads && E->cg_key[1] == grid &&
         std::equal(pkey, pkey + 5, E->cg_pkey))) {
     if (E->cg_exec) cudaGraphExecDestroy(E->cg_exec);

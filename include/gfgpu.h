@@ -500,11 +500,9 @@ int gf_ensemble_rk_advance(gf_ensemble_t ens, int dtype, const gf_rk_traits *tra
  * initial guess, the masked residual; the form without xb masks nothing)
  * with the Jacobi preconditioner.  traits->precision GF_CG_FP64: FP64
  * iterations, GCG's stop test on the recurrence residual.  GF_CG_MIXED: FP32
- * iterations (FP64 dot products) and FP64 residuals: with inner_tol > 0 each
- * FP32 run restarts from the FP64 residual once it has reduced its own by
- * inner_tol; with inner_tol = 0 the FP64 residual replaces the FP32 one every
- * check_every iterations (default 16) under the kept search direction; the
- * stop test is on the FP64 residual.  traits: precond GF_PRECOND_JACOBI,
+ * iterations (FP64 dot products) and FP64 residuals: each FP32 run restarts
+ * from the FP64 residual once it has reduced its own by inner_tol (default
+ * 1e-4); the stop test is on the FP64 residual.  traits: precond GF_PRECOND_JACOBI,
  * normtype EUC or INF, maxit (iterations per member), tol, relative,
  * max_refine (FP64 residual evaluations, default 64).  Per member (host
  * arrays, may be NULL): iterations, the final residual norm, status 0

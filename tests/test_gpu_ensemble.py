@@ -1,8 +1,7 @@
 """Ensembles (gf_ensemble_*): many independent problems advanced by one
-persistent launch per RK stage or CG iteration.  The CG runs in three
-modes: FP32 iterations with the FP64 residual replacing the FP32 one every
-check_every iterations (reliable updates, the default), FP32 runs restarted
-from the FP64 residual (inner_tol > 0), and FP64 iterations.
+persistent launch per RK stage or CG iteration.  The CG runs FP32
+iterations restarted from the FP64 residual (mixed; inner_tol 1e-4 by
+default) or FP64 iterations.
 
 Acceptance:
   * RK members (icosahedral spheres of mixed level and order): every
@@ -173,7 +172,7 @@ def _euc(box, v):
     return float(np.sqrt(np.sum(v * v) / box.N))
 
 
-CG_MODES = {"reliable": {}, "restart": {"inner_tol": 1e-4},
+CG_MODES = {"mixed": {}, "mixed_inner_1e-3": {"inner_tol": 1e-3},
             "fp64": {"precision": A.GF_CG_FP64}}
 
 
