@@ -236,38 +236,101 @@ struct LoadL2 {  // an element-local vector written earlier in this launch
   }
 };
 
+// The final stage's input at an element node: the stage sum (folded as a
+// class of one member) where the node is its class's only member, else the
+// folded value the stage-input pass left in uf.
+template <typename T>
+struct LoadFinal {
+  using value_type = T;
+  const float *imult;
+  const T *uf, *uin, *K0, *K1, *K2;
+  T b0, b1, b2;
+  int nk;
+  __device__ __forceinline__ T at(int64_t i) const {
+    if (imult[i] == 1.0f)
+      return __fadd_rn_t(T(0), rk_stage_point(uin[i], nk, K0, K1, K2, b0, b1, b2, i)) / T(1);
+    return __ldcg(uf + i);
+  }
+  template <int N>
+  __device__ __forceinline__ void zline(int64_t e, int i, int j, T (&out)[N]) const {
+#pragma unroll
+    for (int k = 0; k < N; k++) out[k] = at(e * (N * N * N) + (int64_t)k * N * N + j * N + i);
+  }
+  template <int N>
+  __device__ __forceinline__ T point2(int64_t e, int i, int j) const {
+    return at(e * (N * N) + j * N + i);
+  }
+};
+
+// The stage epilogue at an element node.  A node that is its class's only
+// member is finished here (its fold is (0 + v) / 1: K = that, and uout +=
+// c h K, or in the last stage uout = Smooth(uout + c h K)); a node of a
+// shared class keeps the raw slope for the fold after the barrier.  The
+// arithmetic is that of k_dss_rk_split, node for node.
+template <typename T>
+struct OutStage {
+  const float *imult;
+  T *K;
+  const T *src;
+  T *uout;
+  T ch;
+  int fin;
+  int *nonfinite;
+  __device__ __forceinline__ void operator()(int64_t i, T v) const {
+    if (imult[i] != 1.0f) {
+      K[i] = v;
+      return;
+    }
+    const T acc = __fadd_rn_t(T(0), v) / T(1);
+    if (!fin) {
+      K[i] = acc;
+      uout[i] = rk_accum_point(src[i], acc, ch);
+    } else {
+      const T acc2 = __fadd_rn_t(T(0), rk_accum_point(src[i], acc, ch)) / T(1);
+      uout[i] = acc2;
+      if (!isfinite((double)acc2)) *nonfinite = 1;
+    }
+  }
+};
+
 template <typename T, int N>
-__device__ void en_rhs_elem(const LaneTeam &tm, const EnMember &M, int64_t e, const SBasis<T> &B,
-                            T *slice, bool from_uf, int stage, int par, int eqn, T nu, bool fast) {
+__device__ void en_rhs_elem(const LaneTeam &tm, const EnArgs &a, int mi, const EnMember &M,
+                            int64_t e, const SBasis<T> &B, T *slice, bool fin, int stage, T nu,
+                            bool fast) {
+  const int par = a.par;
+  T *uout = (T *)M.u[1 - par];
+  const OutStage<T> out{M.imult32,
+                        (T *)M.K[fin ? 0 : stage],
+                        stage == 0 ? (const T *)M.u[par] : uout,
+                        uout,
+                        (T)M.ch[stage],
+                        fin,
+                        &a.ctl->nonfinite[mi]};
+  const LoadStage<T> lds{(const T *)M.u[par], (const T *)M.K[0], (const T *)M.K[1],
+                         (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
+                         (T)M.coef[stage][2], stage};
+  const LoadFinal<T> ldf{M.imult32, (const T *)M.uf, lds.uin, lds.K0, lds.K1, lds.K2,
+                         lds.b0, lds.b1, lds.b2, stage};
   if (fast) {  // prescribed velocity, nu = 0: adv_element on the coefficient planes
     const T *b0 = (const T *)M.advb[0], *b1 = (const T *)M.advb[1];
-    if (from_uf)
-      adv_element<T, N>(tm, B, e, LoadL2<T>{(const T *)M.uf}, b0, b1, (T *)M.K[0], slice);
+    if (fin)
+      adv_element<T, N>(tm, B, e, ldf, b0, b1, out, slice);
     else
-      adv_element<T, N>(tm, B, e,
-                        LoadStage<T>{(const T *)M.u[par], (const T *)M.K[0], (const T *)M.K[1],
-                                     (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
-                                     (T)M.coef[stage][2], stage},
-                        b0, b1, (T *)M.K[stage], slice);
+      adv_element<T, N>(tm, B, e, lds, b0, b1, out, slice);
     return;
   }
   constexpr int pr = sizeof(T) == 4 ? 1 : 0;
   const DefGeom<T> g{(const T *)M.X[pr], (const T *)M.G[pr], (const T *)M.J[pr], M.nxy,
                      M.nlocal};
   const T *imass = (const T *)M.imass[pr];
-  const int nv = eqn == GF_EQN_ADVECT ? M.nxy : 0;
+  const int nv = a.eqn == GF_EQN_ADVECT ? M.nxy : 0;
   const T *c0 = (const T *)M.c[0], *c1 = (const T *)M.c[1], *c2 = (const T *)M.c[2];
-  if (from_uf) {
-    def_element<T, N, 2, LoadL2<T>, T>(tm, B, g, e, DEF_DUDT, nu, nullptr, T(0), nullptr, 0,
-                                       LoadL2<T>{(const T *)M.uf}, nv, c0, c1, c2, 0, imass,
-                                       (T *)M.K[0], slice);
-  } else {
-    const LoadStage<T> ld{(const T *)M.u[par], (const T *)M.K[0], (const T *)M.K[1],
-                          (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
-                          (T)M.coef[stage][2], stage};
+  if (fin)
+    def_element<T, N, 2, LoadFinal<T>, T>(tm, B, g, e, DEF_DUDT, nu, nullptr, T(0), nullptr, 0,
+                                          ldf, nv, c0, c1, c2, 0, imass, out, slice);
+  else
     def_element<T, N, 2, LoadStage<T>, T>(tm, B, g, e, DEF_DUDT, nu, nullptr, T(0), nullptr, 0,
-                                          ld, nv, c0, c1, c2, 0, imass, (T *)M.K[stage], slice);
-  }
+                                          lds, nv, c0, c1, c2, 0, imass, out, slice);
 }
 
 // Element phase of an RK stage: K_stage = dudt(stage input), or for the
@@ -298,61 +361,43 @@ __device__ void en_rk_elements(const EnArgs &a, const int64_t *cpref, bool from_
       const SBasis<T> B{ws, ws + N * N};
       T *slice = ws + en_basis_words<T>(N) + tid * 5 * N * N;
       switch (N) {
-        case 3: en_rhs_elem<T, 3>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        case 4: en_rhs_elem<T, 4>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        case 5: en_rhs_elem<T, 5>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        case 6: en_rhs_elem<T, 6>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        case 7: en_rhs_elem<T, 7>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        case 8: en_rhs_elem<T, 8>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        case 9: en_rhs_elem<T, 9>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
-        default: en_rhs_elem<T, 10>(tm, M, e, B, slice, from_uf, stage, a.par, a.eqn, nu, fast); break;
+        case 3: en_rhs_elem<T, 3>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        case 4: en_rhs_elem<T, 4>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        case 5: en_rhs_elem<T, 5>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        case 6: en_rhs_elem<T, 6>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        case 7: en_rhs_elem<T, 7>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        case 8: en_rhs_elem<T, 8>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        case 9: en_rhs_elem<T, 9>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
+        default: en_rhs_elem<T, 10>(tm, a, mi, M, e, B, slice, from_uf, stage, nu, fast); break;
       }
     }
     __syncwarp();
   }
 }
 
-// The node work of an RK stage, split by class size: a class with one
-// member (an interior node, most of them) is folded by the thread of that
-// node, in node order (coalesced, no index arrays: imult = 1 marks it); a
-// class with several members is folded by one thread from the problem's
-// shared-class list (sh_ptr / sh_members, members in ascending local id).
-// Either way the fold is that of k_dss_rk_split: from 0, in member
-// order, divided by the count.  The items are all members' nodes
-// (prefix npref), then all members' shared classes (prefix spref).
-template <class FN, class FC>
-__device__ __forceinline__ void en_rk_items(const EnArgs &a, const int64_t *npref,
-                                            const int64_t *spref, FN node, FC cls) {
-  const int64_t nt = (int64_t)gridDim.x * blockDim.x, total = a.nclass + a.nsh;
-  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < total; it += nt) {
-    if (it < a.nclass) {
-      const int mi = en_find(npref, a.nmem, it);
-      const EnMember &M = a.mem[mi];
-      const int64_t i = it - npref[mi];
-      if (M.imult32[i] == 1.0f) node(mi, M, i);
-    } else {
-      const int64_t j = it - a.nclass;
-      const int mi = en_find(spref, a.nmem, j);
-      const EnMember &M = a.mem[mi];
-      const int64_t cl = j - spref[mi];
-      cls(mi, M, M.sh_ptr[cl], M.sh_ptr[cl + 1]);
-    }
+// The node work of an RK stage after its element phase: the classes of
+// several members (shared nodes; a class of one member is finished by the
+// element phase), one thread each from the problem's shared-class list
+// (sh_ptr / sh_members, members in ascending local id), numbered over all
+// members (prefix spref).  The fold is that of k_dss_rk_split: from 0, in
+// member order, divided by the count.
+template <class FC>
+__device__ __forceinline__ void en_rk_items(const EnArgs &a, const int64_t *spref, FC cls) {
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.nsh; j += nt) {
+    const int mi = en_find(spref, a.nmem, j);
+    const EnMember &M = a.mem[mi];
+    const int64_t cl = j - spref[mi];
+    cls(mi, M, M.sh_ptr[cl], M.sh_ptr[cl + 1]);
   }
 }
 
-// Final-stage input: uf = Smooth(stage sum over the ns-1 earlier slopes).
+// Final-stage input at the shared nodes: uf = Smooth(stage sum over the
+// ns-1 earlier slopes) (the element phase forms it at the other nodes).
 template <typename T>
-__device__ void en_rk_stage_input(const EnArgs &a, const int64_t *npref, const int64_t *spref,
-                                  int stage) {
+__device__ void en_rk_stage_input(const EnArgs &a, const int64_t *spref, int stage) {
   en_rk_items(
-      a, npref, spref,
-      [&](int, const EnMember &M, int64_t i) {
-        const T *uin = (const T *)M.u[a.par];
-        const T v = rk_stage_point(uin[i], stage, (const T *)M.K[0], (const T *)M.K[1],
-                                   (const T *)M.K[2], (T)M.coef[stage][0], (T)M.coef[stage][1],
-                                   (T)M.coef[stage][2], i);
-        ((T *)M.uf)[i] = __fadd_rn_t(T(0), v) / T(1);
-      },
+      a, spref,
       [&](int, const EnMember &M, int32_t b0, int32_t e0) {
         const T *uin = (const T *)M.u[a.par];
         const T *K0 = (const T *)M.K[0], *K1 = (const T *)M.K[1], *K2 = (const T *)M.K[2];
@@ -368,29 +413,14 @@ __device__ void en_rk_stage_input(const EnArgs &a, const int64_t *npref, const i
       });
 }
 
-// Fold of a stage: Smooth K_stage and uout += c h K (stages before the
-// last), or for the last stage uout = Smooth(uout + c h Smooth(K_0)).
+// Fold of a stage at the shared nodes: Smooth K_stage and uout += c h K
+// (stages before the last), or for the last stage uout = Smooth(uout + c h
+// Smooth(K_0)) (the element phase finishes the other nodes).
 template <typename T>
-__device__ void en_rk_fold(const EnArgs &a, const int64_t *npref, const int64_t *spref,
-                           int stage) {
+__device__ void en_rk_fold(const EnArgs &a, const int64_t *spref, int stage) {
   const bool fin = stage == a.ns - 1;
   en_rk_items(
-      a, npref, spref,
-      [&](int mi, const EnMember &M, int64_t i) {
-        const T ch = (T)M.ch[stage];
-        T *uout = (T *)M.u[1 - a.par];
-        const T *src = stage == 0 ? (const T *)M.u[a.par] : uout;
-        T *Kx = (T *)M.K[fin ? 0 : stage];
-        const T acc = __fadd_rn_t(T(0), __ldcg(Kx + i)) / T(1);
-        if (!fin) {
-          Kx[i] = acc;
-          uout[i] = rk_accum_point(src[i], acc, ch);
-        } else {
-          const T acc2 = __fadd_rn_t(T(0), rk_accum_point(src[i], acc, ch)) / T(1);
-          uout[i] = acc2;
-          if (!isfinite((double)acc2)) a.ctl->nonfinite[mi] = 1;
-        }
-      },
+      a, spref,
       [&](int mi, const EnMember &M, int32_t b0, int32_t e0) {
         const T cnt = (T)(e0 - b0), ch = (T)M.ch[stage];
         T *uout = (T *)M.u[1 - a.par];
@@ -419,22 +449,23 @@ __device__ void en_rk_fold(const EnArgs &a, const int64_t *npref, const int64_t 
 
 // One RK stage of every member (step_b of GExRKStepper, gexrk_stepper.ipp:
 // 252-341): stages before the last are RHS | fold; the last is stage input
-// and Smooth | RHS | fold.
+// and Smooth | RHS | fold.  (FP32 fits 64 registers, two 512-thread blocks
+// per SM; FP64 takes 110, one block, rather than spill.)
 template <typename T>
-__global__ void __launch_bounds__(512) k_en_rk_stage(EnArgs a, int stage) {
-  __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_npref[EN_MAXMEM + 1], s_spref[EN_MAXMEM + 1];
+__global__ void __launch_bounds__(512, sizeof(T) == 8 ? 1 : 2)
+    k_en_rk_stage(EnArgs a, int stage) {
+  __shared__ int64_t s_cpref[EN_MAXMEM + 1], s_spref[EN_MAXMEM + 1];
   en_load_pref(a.chunk_pref, s_cpref, a.nmem);
-  en_load_pref(a.class_pref, s_npref, a.nmem);
   en_load_pref(a.sh_pref, s_spref, a.nmem);
   __syncthreads();
   const bool fin = stage == a.ns - 1;
   if (fin) {
-    en_rk_stage_input<T>(a, s_npref, s_spref, stage);
+    en_rk_stage_input<T>(a, s_spref, stage);
     en_barrier(a.ctl, NoWork{});
   }
   en_rk_elements<T>(a, s_cpref, fin, stage);
   en_barrier(a.ctl, NoWork{});
-  en_rk_fold<T>(a, s_npref, s_spref, stage);
+  en_rk_fold<T>(a, s_spref, stage);
 }
 
 // element phase alone (the autotuner's timing kernel): stage 0 of step_b

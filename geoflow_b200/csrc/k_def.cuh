@@ -65,11 +65,19 @@ struct LaneTeam {
   __device__ __forceinline__ void sync() const { __syncwarp(mask); }
 };
 
+// Where an element body writes node values: a plain array (OutPtr), or a
+// policy that finishes the value there (the ensemble's stage epilogue).
+template <typename TO>
+struct OutPtr {
+  TO *__restrict__ p;
+  __device__ __forceinline__ void operator()(int64_t node, TO v) const { p[node] = v; }
+};
+
 // One element e of k_def, by the threads of team tm (the body shared by
 // k_def and the ensemble kernels).  BB is a basis with members D[N*N] and
 // W[N]; smem holds (1 + 2 DIM) N^DIM values of T.  Each node's arithmetic
 // is the same whichever thread of whichever team computes it.
-template <typename T, int N, int DIM, class LD, typename TO, class BB, class TM>
+template <typename T, int N, int DIM, class LD, typename TO, class BB, class TM, class OUT>
 __device__ __forceinline__ void def_element(const TM &tm, const BB &B, const DefGeom<T> &g,
                                             int64_t e, int mode,
                                             T p, const T *__restrict__ pvec, T q,
@@ -77,7 +85,7 @@ __device__ __forceinline__ void def_element(const TM &tm, const BB &B, const Def
                                             int nv, const T *__restrict__ c0,
                                             const T *__restrict__ c1, const T *__restrict__ c2,
                                             int idir, const T *__restrict__ imass,
-                                            TO *__restrict__ uo, T *smem) {
+                                            const OUT &uo, T *smem) {
   constexpr int NN = N * N, NE = DIM == 3 ? NN * N : NN;
   T *su = smem;
   T *sd = su + NE;        // DIM planes: D_j u
@@ -118,7 +126,7 @@ __device__ __forceinline__ void def_element(const TM &tm, const BB &B, const Def
     if (mode == DEF_DERIV) {
       T du = sd[a] * g.X[(0 * g.nxy + idir - 1) * nl + node];
       for (int j = 1; j < DIM; j++) du += sd[j * NE + a] * g.X[(j * g.nxy + idir - 1) * nl + node];
-      uo[node] = (TO)du;
+      uo(node, (TO)du);
       continue;
     }
     if (mode != DEF_ADVECT) {
@@ -145,7 +153,7 @@ __device__ __forceinline__ void def_element(const TM &tm, const BB &B, const Def
       }
       po *= mass;
       if (mode == DEF_ADVECT) {
-        uo[node] = (TO)po;
+        uo(node, (TO)po);
         continue;
       }
       su[a] = po;  // u itself is no longer needed by the rhs
@@ -175,11 +183,11 @@ __device__ __forceinline__ void def_element(const TM &tm, const BB &B, const Def
         t *= qvec ? qvec[node] : q;
         o += t;
       }
-      uo[node] = (TO)o;
+      uo(node, (TO)o);
     } else {  // DEF_DUDT
       o *= p;  // p = nu
       const T r = nv > 0 ? T(-1) * o + T(-1) * su[a] : T(-1) * o;
-      uo[node] = (TO)(imass[node] * r);
+      uo(node, (TO)(imass[node] * r));
     }
   }
 }
@@ -217,10 +225,10 @@ __device__ __forceinline__ void adv_coef_point(int64_t node, int li0, int li1, c
 
 // One 2-d element of the advection right-hand side from the coefficient
 // planes (team tm; smem holds N^2 values).
-template <typename T, int N, class LD, class BB, class TM>
+template <typename T, int N, class LD, class BB, class TM, class OUT>
 __device__ __forceinline__ void adv_element(const TM &tm, const BB &B, int64_t e, const LD &ld,
                                             const T *__restrict__ b0, const T *__restrict__ b1,
-                                            T *__restrict__ out, T *su) {
+                                            const OUT &out, T *su) {
   constexpr int NN = N * N;
   const int64_t base = e * NN;
 #pragma unroll 4
@@ -238,7 +246,7 @@ __device__ __forceinline__ void adv_element(const TM &tm, const BB &B, int64_t e
       d0 = fma(B.D[i + m * N], su[j * N + m], d0);
       d1 = fma(B.D[j + m * N], su[m * N + i], d1);
     }
-    out[base + a] = fma(c1, d1, c0 * d0);
+    out(base + a, fma(c1, d1, c0 * d0));
   }
 }
 
@@ -254,7 +262,8 @@ __global__ void __launch_bounds__(256)
   const int64_t e = blockIdx.x;
   if (e >= ne) return;
   def_element<T, N, DIM, LD, TO>(BlockTeam{}, B, g, e, mode, p, pvec, q, qvec, use_mass, ld, nv, c0,
-                                 c1, c2, idir, imass, uo, reinterpret_cast<T *>(smem_def));
+                                 c1, c2, idir, imass, OutPtr<TO>{uo},
+                                 reinterpret_cast<T *>(smem_def));
 }
 
 // The coefficient planes of adv_element on one 2-d problem (one thread per
@@ -280,8 +289,8 @@ __global__ void __launch_bounds__(128)
   const int w = threadIdx.x >> 5;
   const int64_t e = (int64_t)blockIdx.x * 4 + w;
   if (e >= ne) return;  // whole warps
-  adv_element<T, N>(LaneTeam{(int)(threadIdx.x & 31), 32, 0xffffffffu}, B, e, ld, b0, b1, out,
-                    su[w]);
+  adv_element<T, N>(LaneTeam{(int)(threadIdx.x & 31), 32, 0xffffffffu}, B, e, ld, b0, b1,
+                    OutPtr<T>{out}, su[w]);
 }
 
 }  // namespace gfk
