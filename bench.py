@@ -93,6 +93,12 @@ def parse():
                     help="multigrid: Chebyshev smoothing degree per level and side")
     ap.add_argument("--mg-ratio", type=float, default=0.0,
                     help="multigrid: lmax/lmin of the smoothing interval (0: library default)")
+    ap.add_argument("--ens-members", type=int, default=16,
+                    help="ensemble: members of each kind (the first ones drawn)")
+    ap.add_argument("--ens-max-level", type=int, default=5,
+                    help="ensemble: icosahedral levels above this are lowered to it")
+    ap.add_argument("--ens-fixed-shape", action="store_true",
+                    help="ensemble: a fixed launch shape instead of the autotuner's (profiling)")
     ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "pmg", "apply", "adjoint", "graphs",
                                        "ensemble", "rk", "maps"],
                     default=None,
@@ -530,7 +536,7 @@ def graph_bench(ctx, reps=3):
 
 
 # ---------------------------------------------------------------------------
-def ensemble_bench(ctx, steps=10, reps=3):
+def ensemble_bench(ctx, steps=10, reps=3, members=16, max_level=5, fixed_shape=False):
     """The batched ensemble: (1) 16 icosahedral-sphere advection members
     (level 3..5, p 4..8, cosine bell with seeded centre, solid-body wind,
     RK4, dt at CFL 0.25) as one gf_ensemble, one persistent launch per stage,
@@ -541,7 +547,9 @@ def ensemble_bench(ctx, steps=10, reps=3):
     persistent launch per CG iteration (FP32 PCG, FP64 refinement), against
     the members solved one by one (gf_cg_solve, mixed and FP64), each
     member's FP64 residual recomputed by the FP64 apply.  Launch shapes
-    from the autotuner."""
+    from the autotuner (or, with fixed_shape, 512 threads and 2 blocks per SM,
+    timed by the tuner without a search).  members / max_level shrink the
+    ensemble for profiling runs."""
     import torch
     from geoflow_b200 import (CGTraits, Ensemble, GBurgers, GCG, GGFX, GHelmholtz, GMass,
                               GridBox, IcosGrid, Problem, workloads as W)
@@ -566,8 +574,8 @@ def ensemble_bench(ctx, steps=10, reps=3):
     # ---- (1) icosahedral advection members ----
     t0 = time.perf_counter()
     mem = []
-    for level, p, lat0, lon0 in W.icos_members():
-        g = IcosGrid(level, p, ctx=ctx)
+    for level, p, lat0, lon0 in W.icos_members()[:members]:
+        g = IcosGrid(min(level, max_level), p, ctx=ctx)
         prob = g.problem(ctx)
         u0 = W.icos_cosine_bell(g.xyz, lat0, lon0)
         c = W.icos_solid_body_wind(g.xyz)
@@ -593,7 +601,11 @@ def ensemble_bench(ctx, steps=10, reps=3):
 
     E.advance(us, cs, dt=dts, nsteps=1)
     t1 = time.perf_counter()
-    E.tune(torch.float32, reps=3)
+    if fixed_shape:
+        E.set_shape(512, 2, {n: (8 if n <= 7 else 16) for n in range(3, 11)}, dtype=torch.float32)
+        E.tune(torch.float32, reps=-3)
+    else:
+        E.tune(torch.float32, reps=3)
     tune_s = time.perf_counter() - t1
     shape = E.shape(torch.float32)
 
@@ -639,7 +651,7 @@ def ensemble_bench(ctx, steps=10, reps=3):
     del E, us, cs, us64, cs64, u0s, Bs
     # ---- (2) box Helmholtz members ----
     bm = []
-    for k, (ne, p) in enumerate(W.box_members()):
+    for k, (ne, p) in enumerate(W.box_members()[:members]):
         g = GridBox(2, [ne, ne], p)
         prob = Problem(ctx, g)
         f = torch.from_numpy(W.helmholtz2d_rhs(g.xyz, seed=SEED + 20 + k)).to(dev)
@@ -677,9 +689,13 @@ def ensemble_bench(ctx, steps=10, reps=3):
             worst = max(worst, float(torch.sqrt((r * r).mean()) / torch.sqrt((b * b).mean())))
         return worst
 
-    E2.solve(bs, xs, traits())
+    E2.solve(bs, xs, traits(precision=A.GF_CG_FP64))
     t1 = time.perf_counter()
-    E2.tune(reps=3)
+    if fixed_shape:
+        E2.set_shape(512, 2)
+        E2.tune(reps=-3)
+    else:
+        E2.tune(reps=3)
     tune2_s = time.perf_counter() - t1
     modes = {"mixed": {"inner_tol": 1e-4}, "fp64": {"precision": A.GF_CG_FP64}}
     runs = {}
@@ -948,8 +964,9 @@ def main():
         print(json.dumps({"only": "graphs", "graphs": graph_bench(ctx)}), flush=True)
         return
     if args.only == "ensemble":
-        print(json.dumps({"only": "ensemble", "ensemble": ensemble_bench(ctx, steps=args.steps)}),
-              flush=True)
+        print(json.dumps({"only": "ensemble", "ensemble": ensemble_bench(
+            ctx, steps=args.steps, members=args.ens_members, max_level=args.ens_max_level,
+            fixed_shape=args.ens_fixed_shape)}), flush=True)
         return
     if args.only == "maps":
         print(json.dumps({"only": "maps", "index_maps": index_map_bench(ctx)}), flush=True)

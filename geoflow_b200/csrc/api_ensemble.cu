@@ -1501,7 +1501,8 @@ extern "C" int gf_ensemble_tune(gf_ensemble_t E, int dtype, int reps) {
   gf_context *ctx = E->ctx;
   const int w = en_which(E->kind, dtype);
   GF_REQUIRE(ctx, E->kind == GF_ENS_CG || dtype == GF_F32 || dtype == GF_F64, "bad dtype");
-  if (reps < 1) reps = 5;
+  const bool search = reps >= 0;  // reps < 0: time the current shape |reps| times, no search
+  reps = reps == 0 ? 5 : (reps < 0 ? -reps : reps);
   int rc = en_buffers(E, w);
   if (rc) return rc;
   // The timing kernels read and write the ensemble's own scratch only: an
@@ -1524,7 +1525,7 @@ extern "C" int gf_ensemble_tune(gf_ensemble_t E, int dtype, int reps) {
   float tbest = en_time_shape(E, w, reps);
   const int thr[4] = {64, 128, 256, 512};
   const int bps[4] = {1, 2, 4, 0};
-  for (int ti = 0; ti < 4; ti++)
+  for (int ti = 0; search && ti < 4; ti++)
     for (int bi = 0; bi < 4; bi++) {
       S = best;
       S.threads = thr[ti];
@@ -1538,7 +1539,7 @@ extern "C" int gf_ensemble_tune(gf_ensemble_t E, int dtype, int reps) {
   bool seen[EN_MAXN + 1] = {};
   for (auto *p : E->probs) seen[p->n] = true;
   const int teams[3] = {8, 16, 32};
-  for (int n = EN_MINN; n <= EN_MAXN; n++) {
+  for (int n = EN_MINN; search && n <= EN_MAXN; n++) {
     if (!seen[n]) continue;
     for (int k = 0; k < 3; k++) {
       S = best;
@@ -1550,7 +1551,7 @@ extern "C" int gf_ensemble_tune(gf_ensemble_t E, int dtype, int reps) {
       }
     }
   }
-  best.tuned = true;
+  best.tuned = search || best.tuned;
   best.ms = tbest;
   S = best;
   E->host = saved;

@@ -511,11 +511,13 @@ int gf_ensemble_rk_advance(gf_ensemble_t ens, int dtype, const gf_rk_traits *tra
 int gf_ensemble_cg_solve(gf_ensemble_t ens, const gf_cg_traits *traits, double p, double q,
                          const double *const *b, double *const *x, int *iters,
                          double *final_norm, int *status);
-/* The autotuner: times the element phase of candidate launch shapes
- * (threads per block, blocks per SM, lanes per element for each order
- * present) on this ensemble's members, with the ensemble's own scratch as
- * the data, and keeps the fastest.  An RK ensemble is timed on the equation
- * of its last advance (advection before the first). */
+/* The autotuner: times candidate launch shapes (threads per block, blocks
+ * per SM, lanes per element for each order present) on this ensemble's
+ * members, with the ensemble's own scratch as the data, and keeps the
+ * fastest: best of `reps` launches of the RK stage's element phase (on the
+ * equation of the last advance; advection before the first) or of one
+ * whole CG iteration.  reps < 0 times the current shape |reps| times and
+ * changes nothing (its time is then what gf_ensemble_shape reports). */
 int gf_ensemble_tune(gf_ensemble_t ens, int dtype, int reps);
 /* The current shape: threads per block, cooperative blocks, lanes per
  * element by GLL point count (team_by_n[n], n <= 10), tuned flag, and the
