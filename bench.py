@@ -99,8 +99,8 @@ def parse():
                     help="ensemble: icosahedral levels above this are lowered to it")
     ap.add_argument("--ens-fixed-shape", action="store_true",
                     help="ensemble: a fixed launch shape instead of the autotuner's (profiling)")
-    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "pmg", "apply", "adjoint", "graphs",
-                                       "ensemble", "rk", "maps"],
+    ap.add_argument("--only", choices=["fp64", "mixed", "cheb", "pmg", "pmg64", "pmgkern", "apply",
+                                       "adjoint", "graphs", "ensemble", "rk", "maps"],
                     default=None,
                     help="time only one CG path (for profiling runs)")
     return ap.parse_args()
@@ -282,6 +282,63 @@ def kernel_roofline(ctx, prob, peaks, reps=20):
                      "gdofs": prob.nlocal / t / 1e9, "ms_dirty_flush": times[False] * 1e3}
     lib.gf_set_fp32_apply(prev)
     return res
+
+
+def pmg_launches_per_iteration(m):
+    """Launches of each finest-level kernel per multigrid-preconditioned CG
+    iteration at smoothing degree m: m pre-smoothing steps, the residual,
+    the first post-smoothing term and m more steps, each step after an
+    apply; plus the outer FP64 apply."""
+    return {"apply_fp64": 1, "apply_vcycle": 2 * m + 2, "smoother_step": 2 * m + 1,
+            "residual": 1}
+
+
+def pmg_kernel_roofline(ctx, prob, traits, peaks, reps=10):
+    """The finest-level kernels of a multigrid-preconditioned solve (the
+    instances the solve runs inside its graph), each launched alone through
+    gf_pmg_launch after an L2 flush and timed with CUDA events on the
+    context's stream: the outer FP64 lattice -> element apply, the V-cycle's
+    lattice -> element apply, a smoother step pass and the residual pass.
+    Algorithmic bytes per launch: apply = lattice in + element out +
+    element geometry; step = q_E + b, dinv, x, d in + x, d out + the 1-byte
+    lattice mask; residual = q_E + b in + res out + mask."""
+    import ctypes as C
+    import torch
+    from geoflow_b200 import _abi as A
+    lib = A.load()
+    flush = L2Flush(ctx.torch_device)
+    g = prob.grid
+    tr = traits.to_c()
+    ctx.check(lib.gf_pmg_launch(prob.handle, C.byref(tr), 1.0, 1.0, 1, 1, A.GF_PMG_PREPARE),
+              "gf_pmg_launch")
+    nL, nE, ne, dim = g.nclass, prob.nlocal, g.nelems, g.dim
+    sm = 8 if traits.precond == A.GF_PRECOND_PMG64 else 4
+    kinds = {
+        "apply_fp64": (A.GF_PMG_APPLY64, nL * 8 + nE * 8 + ne * (dim + 1) * 8),
+        "apply_vcycle": (A.GF_PMG_APPLY, nL * sm + nE * sm + ne * (dim + 1) * sm),
+        "smoother_step": (A.GF_PMG_STEP, nE * sm + 6 * nL * sm + nL),
+        "residual": (A.GF_PMG_RESID, nE * sm + 2 * nL * sm + nL),
+    }
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    out = {}
+    for name, (which, alg) in kinds.items():
+        for _ in range(3):
+            ctx.check(lib.gf_pmg_launch(prob.handle, C.byref(tr), 1.0, 1.0, 1, 1, which),
+                      "gf_pmg_launch")
+        ts = []
+        for _ in range(reps):
+            flush(True)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            ctx.check(lib.gf_pmg_launch(prob.handle, C.byref(tr), 1.0, 1.0, 1, 1, which),
+                      "gf_pmg_launch")
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e) / 1e3)
+        t = statistics.mean(ts)
+        out[name] = {"ms": t * 1e3, "alg_bytes": alg, "gbs": alg / t / 1e9,
+                     "frac": alg / t / 1e9 / hbm}
+    return out
 
 
 def dss_timing(ctx, prob, reps=10):
@@ -955,6 +1012,9 @@ def main():
     # FP64 flexible CG with one FP32 p/h-multigrid V-cycle as preconditioner
     tr_pmg = CGTraits(precision=A.GF_CG_MIXED, check_every=4, poly_degree=args.mg_degree,
                       poly_ratio=args.mg_ratio, **dict(common, precond=A.GF_PRECOND_PMG))
+    # the same multigrid with an FP64 V-cycle: what the FP32 V-cycle saves
+    tr_pmg64 = CGTraits(precision=A.GF_CG_FP64, check_every=4, poly_degree=args.mg_degree,
+                        poly_ratio=args.mg_ratio, **dict(common, precond=A.GF_PRECOND_PMG64))
     if args.only == "rk":
         print(json.dumps({"only": "rk", "rk_stage": rk_stage_bench(ctx, args.rk_ne, args.rk_p,
                                                                   steps=args.steps,
@@ -978,9 +1038,15 @@ def main():
         roof = kernel_roofline(ctx, prob, measured_peaks(), reps=args.steps)
         print(json.dumps({"only": "apply", "helm3d": roof}), flush=True)
         return
+    if args.only == "pmgkern":
+        out = {"fp32_vcycle": pmg_kernel_roofline(ctx, prob, tr_pmg, peaks, reps=args.steps),
+               "fp64_vcycle": pmg_kernel_roofline(ctx, prob, tr_pmg64, peaks, reps=args.steps)}
+        print(json.dumps({"only": "pmgkern", "pmg_finest_level": out}), flush=True)
+        return
     if args.only:
-        tr = {"fp64": tr_64, "mixed": tr_mix, "cheb": tr_cheb, "pmg": tr_pmg}[args.only]
-        cold = cold_solve(ctx, prob, H, b, tr) if args.only == "pmg" else None
+        tr = {"fp64": tr_64, "mixed": tr_mix, "cheb": tr_cheb, "pmg": tr_pmg,
+              "pmg64": tr_pmg64}[args.only]
+        cold = cold_solve(ctx, prob, H, b, tr) if args.only in ("pmg", "pmg64") else None
         t, it, rc, x = time_solves(ctx, prob, H, b, tr, args.steps, args.warmup)
         out = {"only": args.only, "s_per_solve": statistics.mean(t), "iterations": it[-1],
                "rc": rc, "first_solve_s": cold}
@@ -1017,25 +1083,34 @@ def main():
     l3 = C_stats(prob)
     t_pmg, it_pmg, rc_pmg, x_pmg = time_solves(ctx, prob, H, b, tr_pmg, args.steps, args.warmup)
     l4 = C_stats(prob)
+    t_cold64 = cold_solve(ctx, prob, H, b, tr_pmg64)
+    l5 = C_stats(prob)
+    t_pmg64, it_pmg64, rc_pmg64, x_pmg64 = time_solves(ctx, prob, H, b, tr_pmg64, args.steps,
+                                                       args.warmup)
+    l6 = C_stats(prob)
     barrier()
     clk = clocks.stop()
     t64 = max_over_ranks(statistics.mean(t_64))
     tmix = max_over_ranks(statistics.mean(t_mix))
     tpmg = max_over_ranks(statistics.mean(t_pmg))
+    tpmg64 = max_over_ranks(statistics.mean(t_pmg64))
     diff = float((x_mix - x_64).abs().max() / x_64.abs().max())
     diff_pmg = float((x_pmg - x_64).abs().max() / x_64.abs().max())
+    diff_pmg64 = float((x_pmg64 - x_64).abs().max() / x_64.abs().max())
     # headline: the fastest complete solver (same problem, same 1e-10
     # relative-residual stop test on the FP64 residual)
-    times = {"fp64": t64, "mixed": tmix, "pmg": tpmg}
+    times = {"fp64": t64, "mixed": tmix, "pmg": tpmg, "pmg64": tpmg64}
+    trs = {"fp64": tr_64, "mixed": tr_mix, "pmg": tr_pmg, "pmg64": tr_pmg64}
     path = min(times, key=times.get)
-    fp64_wins = path == "fp64"
+    fp64_wins = path in ("fp64", "pmg64")
     value = times[path]
-    launches = {"fp64": l1 - l0, "mixed": l2 - l1, "pmg": l4 - l3}[path]
+    launches = {"fp64": l1 - l0, "mixed": l2 - l1, "pmg": l4 - l3, "pmg64": l6 - l5}[path]
     per_step_launches = launches // (args.steps + args.warmup)
     roof = kernel_roofline(ctx, prob, peaks)
+    pmg_roof = {"fp32_vcycle": pmg_kernel_roofline(ctx, prob, tr_pmg, peaks),
+                "fp64_vcycle": pmg_kernel_roofline(ctx, prob, tr_pmg64, peaks)}
     dss = dss_timing(ctx, prob)
-    e2e_t, h2d, d2h = e2e_solve(ctx, prob, H, b, {"fp64": tr_64, "mixed": tr_mix,
-                                                   "pmg": tr_pmg}[path], reps=args.steps)
+    e2e_t, h2d, d2h = e2e_solve(ctx, prob, H, b, trs[path], reps=args.steps)
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
@@ -1056,10 +1131,30 @@ def main():
                           f"box ({nsample} nodes), per node scaled to {prob.nlocal} nodes and "
                           f"{it_64[-1]} iterations (the device FP64 count of the same "
                           f"algorithm)")}
-    head = roof["f64" if fp64_wins else "f32"]
-    kname = (f"k_helm3d_k1<{'double' if fp64_wins else 'float'},{args.p + 1}> "
-             "(3-d Helmholtz apply, element-local in/out)")
-    prof = f"helm3d_k1_{'f64' if fp64_wins else 'f32'}_{args.ne}cube_p{args.p}"
+    if path in ("pmg", "pmg64"):
+        # the multigrid solve's dominant kernel: per iteration its finest
+        # level runs PMG_PER_ITER launches of each timed kernel; the most
+        # device time goes to the Chebyshev smoother's step pass
+        kk = pmg_roof["fp32_vcycle" if path == "pmg" else "fp64_vcycle"]
+        per_iter = pmg_launches_per_iteration(args.mg_degree)
+        share = {k: per_iter[k] * v["ms"] for k, v in kk.items()}
+        top = max(share, key=share.get)
+        head = kk[top]
+        tname = "float" if path == "pmg" else "double"
+        kname = {"smoother_step": f"k_mg_pass_lat<{args.p + 1},MG_STEP,{tname}> (finest-level "
+                                  "Chebyshev smoother step: fold of q_E, residual, x and d update)",
+                 "apply_vcycle": f"k_helm3d_k1<{tname},{args.p + 1},LoadBox> (finest-level "
+                                 "apply, lattice in, element-local out)",
+                 "residual": f"k_mg_pass_lat<{args.p + 1},MG_RESID,{tname}> (finest-level "
+                             "residual pass)",
+                 "apply_fp64": f"k_helm3d_k1<double,{args.p + 1},LoadBox> (outer FP64 apply)",
+                 }[top]
+        prof = f"mg_pass_{top}_{'f32' if path == 'pmg' else 'f64'}_{args.ne}cube_p{args.p}"
+    else:
+        head = roof["f64" if fp64_wins else "f32"]
+        kname = (f"k_helm3d_k1<{'double' if fp64_wins else 'float'},{args.p + 1}> "
+                 "(3-d Helmholtz apply, element-local in/out)")
+        prof = f"helm3d_k1_{'f64' if fp64_wins else 'f32'}_{args.ne}cube_p{args.p}"
     traffic = profile_traffic(prof)
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps,
@@ -1080,17 +1175,26 @@ def main():
                 "scheme": (f"FP64 CG, preconditioner one FP32 p/h-multigrid V-cycle "
                            f"(Chebyshev-Jacobi degree {args.mg_degree}, dense coarsest solve); "
                            "hierarchy built by the first solve and reused")},
+        "pmg_fp64": {"value": tpmg64, "unit": "s", "iterations": it_pmg64[-1], "rc": rc_pmg64,
+                     "first_solve_s": t_cold64,
+                     "scheme": ("the same FP64 CG and multigrid with every level of the "
+                                "V-cycle in FP64")},
         "speedup_mixed_vs_fp64": t64 / tmix,
         "speedup_pmg_vs_fp64": t64 / tpmg,
+        "speedup_pmg_fp64_vs_fp64": t64 / tpmg64,
+        "speedup_fp32_vcycle_vs_fp64_vcycle": tpmg64 / tpmg,
         "solution_rel_diff_mixed_vs_fp64": diff,
         "solution_rel_diff_pmg_vs_fp64": diff_pmg,
-        "cg_iterations_per_s": {"fp64": it_64, "mixed": it_mix, "pmg": it_pmg}[path][-1] / value,
+        "solution_rel_diff_pmg_fp64_vs_fp64": diff_pmg64,
+        "cg_iterations_per_s": {"fp64": it_64, "mixed": it_mix, "pmg": it_pmg,
+                                "pmg64": it_pmg64}[path][-1] / value,
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": head["gbs"], "peak": hbm,
                      "unit": "GB/s", "frac": head["gbs"] / hbm, "peak_source": peak_src,
                      "alg_bytes_per_launch": head["alg_bytes"], "ms_per_launch": head["ms"],
                      "traffic": traffic,
                      "traffic_source": f"profiles/{prof}.md" if traffic else None},
-        "kernels": {"helm3d": roof, "dss_sum": dss},
+        "kernels": {"helm3d": roof, "dss_sum": dss, "pmg_finest_level": pmg_roof,
+                    "pmg_launches_per_iteration": pmg_launches_per_iteration(args.mg_degree)},
         "rk_stage": rk,
         "adjoint": adj,
         "graphs": graphs,

@@ -24,8 +24,10 @@ GF_ERR_NONFINITE, GF_ERR_WATCHDOG, GF_ERR_IO = -5, -6, -7
 GF_F64, GF_F32 = 0, 1
 GF_DSS_SUM, GF_DSS_SMOOTH, GF_DSS_MAX, GF_DSS_MIN = 0, 1, 2, 3
 GF_NORM_INF, GF_NORM_EUC, GF_NORM_L2, GF_NORM_L1 = 0, 1, 2, 3
-GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV, GF_PRECOND_PMG = 0, 1, 2, 3
+GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV, GF_PRECOND_PMG, GF_PRECOND_PMG64 = (
+    0, 1, 2, 3, 4)
 GF_CG_FP64, GF_CG_MIXED = 0, 1
+GF_PMG_PREPARE, GF_PMG_APPLY64, GF_PMG_APPLY, GF_PMG_STEP, GF_PMG_RESID = 0, 1, 2, 3, 4
 GF_GEOM_AFFINE, GF_GEOM_REGULAR, GF_GEOM_DEFORMED, GF_GEOM_EMBEDDED = 0, 1, 2, 3
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
 GF_FILTER_BOYD, GF_FILTER_PROJECTION = 0, 1
@@ -120,6 +122,8 @@ SIGNATURES = {
                             c_void_p, c_void_p, P_int, P_double, P_double]),
     "gf_cg_solve_host": (c_int, [c_void_p, C.POINTER(CGTraits), c_double, c_double, c_int,
                                  P_double, P_double, P_double, P_int, P_double]),
+    "gf_pmg_launch": (c_int, [c_void_p, C.POINTER(CGTraits), c_double, c_double, c_int, c_int,
+                              c_int]),
     "gf_rk_advance": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,
                               c_double, c_int]),
     "gf_rk_advance_host": (c_int, [c_void_p, c_int, C.POINTER(RKTraits), P_void, P_void, c_double,

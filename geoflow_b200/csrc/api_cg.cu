@@ -558,13 +558,15 @@ __global__ void __launch_bounds__(RED_THREADS)
 
 // k_update of the multigrid-preconditioned CG (FP64, no Jacobi weight),
 // which also takes the first smoothing term of the next V-cycle on the new
-// residual (k_mg_start's work: b32 = (float) r, x32 = c0 Dinv32 b32) while r
-// is in registers.  Points written after convergence are never read.
+// residual (k_mg_start's work: bm = (TM) r, xm = c0 Dinv bm in the
+// multigrid's type) while r is in registers.  Points written after
+// convergence are never read.
+template <typename TM>
 __global__ void __launch_bounds__(RED_THREADS)
     k_update_mg(int64_t nL, Weights wt, double *__restrict__ x, const double *__restrict__ w,
                 double *__restrict__ r, const double *__restrict__ q,
-                const float *__restrict__ dinv32, float c0, float *__restrict__ b32,
-                float *__restrict__ x32, double *__restrict__ hist, double *scal,
+                const TM *__restrict__ dinvm, TM c0, TM *__restrict__ bm,
+                TM *__restrict__ xm, double *__restrict__ hist, double *scal,
                 double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
@@ -576,9 +578,9 @@ __global__ void __launch_bounds__(RED_THREADS)
     const double rc = r[c] + (-alpha) * q[c];
     r[c] = rc;
     rho += rc * rc;
-    const float bc = (float)rc;
-    b32[c] = bc;
-    x32[c] = c0 * (dinv32[c] * bc);
+    const TM bc = (TM)rc;
+    bm[c] = bc;
+    xm[c] = c0 * (dinvm[c] * bc);
     const double t = norm_term_L(normtype, rc, wt, c);
     rn = normtype == GF_NORM_INF ? fmax(rn, t) : rn + t;
   }
@@ -719,8 +721,10 @@ __global__ void __launch_bounds__(RED_THREADS)
   fcg_finish(rz, zq, scal, partials, counter, sh);
 }
 
-// w = z + beta w  (FP64 search direction, FP32 preconditioned residual)
-__global__ void k_fcg_w(int64_t nL, double *__restrict__ w, const float *__restrict__ z,
+// w = z + beta w  (FP64 search direction, FP32 or FP64 preconditioned
+// residual)
+template <typename TZ>
+__global__ void k_fcg_w(int64_t nL, double *__restrict__ w, const TZ *__restrict__ z,
                         const double *scal) {
   if (scal[S_DONE] != 0.0) return;
   const double beta = scal[S_BETA];
@@ -801,24 +805,33 @@ __global__ void k_invert(int64_t n, const double *__restrict__ d, double *__rest
 // sum_a J[r][a] x_c(ec pc + a) (J[0] and J[R] are unit rows: shared
 // vertices coincide).  The restriction is the transpose, gathered per
 // coarse point.  Periodic directions wrap (Mf = nec R, Mc = nec pc).
+// The multigrid runs in TM = float (the FP32 V-cycle) or double (the FP64
+// V-cycle); the transfer weights are stored in TM.
 constexpr int MG_XR = 2 * GF_MAXN + 1;
+template <typename TM>
 struct Xfer1D {
   int R, pc, nec, per, Mf, Mc;
-  float J[MG_XR * GF_MAXN];  // J[r * (pc + 1) + a]
+  TM J[MG_XR * GF_MAXN];  // J[r * (pc + 1) + a]
 };
+
+__device__ __forceinline__ float mg_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double mg_fma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float mg_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double mg_add(double a, double b) { return __dadd_rn(a, b); }
 
 // out = T in along direction d (transpose: T^T); in and out are lattices
 // of extents ei and eo that differ only in direction d.
 // mode 0: out = s; 1: out += s; 2: out = mask ? s : 0 (mask of the output)
+template <typename TM>
 __global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1,
-                         const __grid_constant__ Xfer1D T, int transpose,
-                         const float *__restrict__ in, float *__restrict__ out,
+                         const __grid_constant__ Xfer1D<TM> T, int transpose,
+                         const TM *__restrict__ in, TM *__restrict__ out,
                          const uint8_t *__restrict__ mask, int mode, const double *stop) {
   if (stop && *stop != 0.0) return;
   const int R = T.R, pc = T.pc, nc = T.pc + 1, nec = T.nec;
   // the weights in shared memory: along x the threads of a warp read
   // different rows, which the constant (parameter) bank would serialise
-  __shared__ float J[MG_XR * GF_MAXN];
+  __shared__ TM J[MG_XR * GF_MAXN];
   for (int i = threadIdx.x; i < (R + 1) * nc; i += blockDim.x) J[i] = T.J[i];
   __syncthreads();
   // lattice sizes are below 2^31 (32-bit index arithmetic)
@@ -843,33 +856,33 @@ __global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1
       base = g0 + ei0 * g1;
       stride = ei0 * ei1;
     }
-    float s = 0.0f;
+    TM s = 0;
     if (!transpose) {  // fine point gd from coarse element ec
       const int ec = min(gd / R, nec - 1), r = gd - ec * R;
       for (int a = 0; a < nc; a++) {
         int c = ec * pc + a;
         if (c >= T.Mc) c -= T.Mc;
-        s = fmaf(J[r * nc + a], in[base + c * stride], s);
+        s = mg_fma(J[r * nc + a], in[base + c * stride], s);
       }
     } else {  // coarse point gd = ec pc + a
       const int ec = gd / pc, a = gd - ec * pc;
       if (a != 0) {
         for (int r = 1; r < R; r++)
-          s = fmaf(J[r * nc + a], in[base + (ec * R + r) * stride], s);
+          s = mg_fma(J[r * nc + a], in[base + (ec * R + r) * stride], s);
       } else {
         s = in[base + (ec * R) * stride];  // the coinciding vertex
         const bool left = ec > 0 || T.per, right = ec < nec;
         if (left) {
           const int el = ec > 0 ? ec - 1 : nec - 1;
           for (int r = 1; r < R; r++)
-            s = fmaf(J[r * nc + pc], in[base + (el * R + r) * stride], s);
+            s = mg_fma(J[r * nc + pc], in[base + (el * R + r) * stride], s);
         }
         if (right)
           for (int r = 1; r < R; r++)
-            s = fmaf(J[r * nc], in[base + (ec * R + r) * stride], s);
+            s = mg_fma(J[r * nc], in[base + (ec * R + r) * stride], s);
       }
     }
-    if (mode == 2 && mask && !mask[o]) s = 0.0f;
+    if (mode == 2 && mask && !mask[o]) s = 0;
     if (mode == 1) out[o] += s;
     else out[o] = s;
   }
@@ -895,15 +908,15 @@ __device__ __forceinline__ int elem_lattice(const BoxLattice &L, int c0, int c1,
 // y, z in shared memory, add into the fine lattice points the element owns
 // (local index < P, or P on a non-periodic upper face), so each point is
 // written once.
-template <int NF>
+template <int NF, typename TM>
 __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF * NF)))
-    k_pxfer_prolong(BoxLattice Lf, BoxLattice Lc, const __grid_constant__ Xfer1D T,
-                    const float *__restrict__ xc, float *__restrict__ xf, const double *stop) {
+    k_pxfer_prolong(BoxLattice Lf, BoxLattice Lc, const __grid_constant__ Xfer1D<TM> T,
+                    const TM *__restrict__ xc, TM *__restrict__ xf, const double *stop) {
   constexpr int NC = NF / 2 + 1, PF = NF - 1, NT = NF * NF;
   constexpr int EPB = (256 / NT) < 1 ? 1 : 256 / NT;
   constexpr int S0 = NC * NC * NC, S1 = NF * NC * NC, S2 = NF * NF * NC;
-  __shared__ float J[NF * NC];
-  __shared__ float sm[EPB][S0 + S1 + S2];
+  __shared__ TM J[NF * NC];
+  __shared__ TM sm[EPB][S0 + S1 + S2];
   if (stop && *stop != 0.0) return;
   const int t = threadIdx.x, slot = threadIdx.y;
   for (int i = t + NT * slot; i < NF * NC; i += NT * EPB) J[i] = T.J[i];
@@ -912,7 +925,7 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
   const int e = blockIdx.x * EPB + slot;
   const bool active = e < nel;
   const int c0 = e % ne0, r = e / ne0, c1 = r % ne1, c2 = r / ne1;
-  float *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
+  TM *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
   if (active)
     for (int i = t; i < S0; i += NT) {
       const int a = i % NC, b = (i / NC) % NC, c = i / (NC * NC);
@@ -922,18 +935,18 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
   if (active)
     for (int i = t; i < S1; i += NT) {  // s1[c][b][i0] = sum_a J[i0][a] s0[c][b][a]
       const int i0 = i % NF, cb = i / NF;
-      float v = 0.0f;
+      TM v = 0;
 #pragma unroll
-      for (int a = 0; a < NC; a++) v = fmaf(J[i0 * NC + a], s0[cb * NC + a], v);
+      for (int a = 0; a < NC; a++) v = mg_fma(J[i0 * NC + a], s0[cb * NC + a], v);
       s1[i] = v;
     }
   __syncthreads();
   if (active)
     for (int i = t; i < S2; i += NT) {  // s2[c][j][i0] = sum_b J[j][b] s1[c][b][i0]
       const int i0 = i % NF, j = (i / NF) % NF, c = i / (NF * NF);
-      float v = 0.0f;
+      TM v = 0;
 #pragma unroll
-      for (int b = 0; b < NC; b++) v = fmaf(J[j * NC + b], s1[(c * NC + b) * NF + i0], v);
+      for (int b = 0; b < NC; b++) v = mg_fma(J[j * NC + b], s1[(c * NC + b) * NF + i0], v);
       s2[i] = v;
     }
   __syncthreads();
@@ -944,9 +957,9 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
 #pragma unroll
   for (int k = 0; k < NF; k++) {
     if (k == PF && (Lf.per[2] || c2 != ne2 - 1)) continue;
-    float v = 0.0f;
+    TM v = 0;
 #pragma unroll
-    for (int c = 0; c < NC; c++) v = fmaf(J[k * NC + c], s2[(c * NF + j) * NF + i0], v);
+    for (int c = 0; c < NC; c++) v = mg_fma(J[k * NC + c], s2[(c * NF + j) * NF + i0], v);
     xf[elem_lattice(Lf, c0, c1, c2, i0, j, k)] += v;
   }
 }
@@ -954,15 +967,15 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
 // restriction into the coarse E-vector: q_c(e) = (J^T (x) J^T (x) J^T)
 // (w r_f)(e), w = 1/(number of elements sharing the fine point), so that
 // folding q_c's copies over the coarse lattice gives P^T r_f.
-template <int NF>
+template <int NF, typename TM>
 __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF * NF)))
-    k_pxfer_restrict(BoxLattice Lf, const __grid_constant__ Xfer1D T,
-                     const float *__restrict__ rf, float *__restrict__ qc, const double *stop) {
+    k_pxfer_restrict(BoxLattice Lf, const __grid_constant__ Xfer1D<TM> T,
+                     const TM *__restrict__ rf, TM *__restrict__ qc, const double *stop) {
   constexpr int NC = NF / 2 + 1, PF = NF - 1, NT = NF * NF;
   constexpr int EPB = (256 / NT) < 1 ? 1 : 256 / NT;
   constexpr int S0 = NF * NF * NF, S1 = NC * NF * NF, S2 = NC * NC * NF;
-  __shared__ float J[NF * NC];
-  __shared__ float sm[EPB][S0 + S1 + S2];
+  __shared__ TM J[NF * NC];
+  __shared__ TM sm[EPB][S0 + S1 + S2];
   if (stop && *stop != 0.0) return;
   const int t = threadIdx.x, slot = threadIdx.y;
   for (int i = t + NT * slot; i < NF * NC; i += NT * EPB) J[i] = T.J[i];
@@ -971,16 +984,16 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
   const int e = blockIdx.x * EPB + slot;
   const bool active = e < nel;
   const int cc[3] = {e % ne[0], (e / ne[0]) % ne[1], e / (ne[0] * ne[1])};
-  float *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
+  TM *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
   if (active)
     for (int i = t; i < S0; i += NT) {
       const int l[3] = {i % NF, (i / NF) % NF, i / (NF * NF)};
-      float w = 1.0f;
+      TM w = 1;
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         const bool shared = (l[d] == 0 && (Lf.per[d] || cc[d] > 0)) ||
                             (l[d] == PF && (Lf.per[d] || cc[d] < ne[d] - 1));
-        if (shared) w *= 0.5f;
+        if (shared) w *= TM(0.5);
       }
       s0[i] = w * rf[elem_lattice(Lf, cc[0], cc[1], cc[2], l[0], l[1], l[2])];
     }
@@ -988,27 +1001,27 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
   if (active)
     for (int i = t; i < S1; i += NT) {  // s1[k][j][a] = sum_i0 J[i0][a] s0[k][j][i0]
       const int a = i % NC, kj = i / NC;
-      float v = 0.0f;
+      TM v = 0;
 #pragma unroll
-      for (int i0 = 0; i0 < NF; i0++) v = fmaf(J[i0 * NC + a], s0[kj * NF + i0], v);
+      for (int i0 = 0; i0 < NF; i0++) v = mg_fma(J[i0 * NC + a], s0[kj * NF + i0], v);
       s1[i] = v;
     }
   __syncthreads();
   if (active)
     for (int i = t; i < S2; i += NT) {  // s2[k][b][a] = sum_j J[j][b] s1[k][j][a]
       const int a = i % NC, b = (i / NC) % NC, k = i / (NC * NC);
-      float v = 0.0f;
+      TM v = 0;
 #pragma unroll
-      for (int j = 0; j < NF; j++) v = fmaf(J[j * NC + b], s1[(k * NF + j) * NC + a], v);
+      for (int j = 0; j < NF; j++) v = mg_fma(J[j * NC + b], s1[(k * NF + j) * NC + a], v);
       s2[i] = v;
     }
   __syncthreads();
   if (!active) return;
   for (int i = t; i < NC * NC * NC; i += NT) {  // q[c][b][a] = sum_k J[k][c] s2[k][b][a]
     const int ab = i % (NC * NC), c = i / (NC * NC);
-    float v = 0.0f;
+    TM v = 0;
 #pragma unroll
-    for (int k = 0; k < NF; k++) v = fmaf(J[k * NC + c], s2[k * NC * NC + ab], v);
+    for (int k = 0; k < NF; k++) v = mg_fma(J[k * NC + c], s2[k * NC * NC + ab], v);
     qc[(int64_t)e * (NC * NC * NC) + i] = v;
   }
 }
@@ -1016,12 +1029,13 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
 // Chebyshev smoothing of A x = b from x = 0 (the recurrence of k_cheb_*),
 // first term: x = c0 Dinv b.  With r64 the level's b is first taken from
 // the FP64 outer residual.
-__global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, float *__restrict__ b,
-                           const float *__restrict__ dinv, float c0, float *__restrict__ x,
+template <typename TM>
+__global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, TM *__restrict__ b,
+                           const TM *__restrict__ dinv, TM c0, TM *__restrict__ x,
                            const double *stop) {
   if (stop && *stop != 0.0) return;
   GRID_STRIDE(c, nL) {
-    const float bc = r64 ? (float)r64[c] : b[c];
+    const TM bc = r64 ? (TM)r64[c] : b[c];
     if (r64) b[c] = bc;
     x[c] = c0 * (dinv[c] * bc);
   }
@@ -1059,12 +1073,12 @@ enum { DP_NONE = 0, DP_X = 1, DP_D = 2 };
 // (Measured on B200 against this form: element-ordered walks, lattice rows
 // mapped to power-of-two thread groups, several points per thread, z-column
 // walks and a lattice-row layout of qE were all slower.)
-template <int N, int MODE, bool DOTS>
+template <int N, int MODE, bool DOTS, typename TM>
 __global__ void __launch_bounds__(RED_THREADS)
     k_mg_pass_lat(MapBox<N> map, Weights wt,
-                  const float *__restrict__ qE, float *__restrict__ b,
-                  const float *__restrict__ dinv, float c1, float c2, float *__restrict__ res,
-                  float *__restrict__ d, float *__restrict__ x, int dsrc, int wd, double *scal,
+                  const TM *__restrict__ qE, TM *__restrict__ b,
+                  const TM *__restrict__ dinv, TM c1, TM c2, TM *__restrict__ res,
+                  TM *__restrict__ d, TM *__restrict__ x, int dsrc, int wd, double *scal,
                   double *partials, unsigned int *counter) {
   __shared__ double sh[32];
   if (scal[S_DONE] != 0.0) return;
@@ -1080,7 +1094,7 @@ __global__ void __launch_bounds__(RED_THREADS)
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nL;
        c = (c < nL - stride) ? c + stride : nL) {
     const bool keep = !wt.maskL || wt.maskL[c];
-    float bc = 0.0f, xo = 0.0f, dv = 0.0f, dpv = 0.0f;
+    TM bc = 0, xo = 0, dv = 0, dpv = 0;
     if (MODE == MG_STEP || MODE == MG_RESID) bc = b[c];
     if (MODE == MG_STEP || MODE == MG_START) dv = dinv[c];
     if (MODE == MG_STEP) {
@@ -1093,7 +1107,7 @@ __global__ void __launch_bounds__(RED_THREADS)
     const int nx = lattice_offsets<P>(g0, ne0, map.per[0], nn, 1, ox0, ox1);
     const int ny = lattice_offsets<P>(g1, ne1, map.per[1], sy, N, oy0, oy1);
     const int nz = d3 ? lattice_offsets<P>(g2, map.ne[2], map.per[2], sz, NN, oz0, oz1) : 1;
-    float s = 0.0f;
+    TM s = 0;
 #pragma unroll
     for (int az = 0; az < 2; az++) {
       if (az >= nz) break;
@@ -1102,11 +1116,11 @@ __global__ void __launch_bounds__(RED_THREADS)
       for (int ay = 0; ay < 2; ay++) {
         if (ay >= ny) break;
         const int o = oz + (ay ? oy1 : oy0);
-        s = __fadd_rn(s, qE[o + ox0]);
-        if (nx > 1) s = __fadd_rn(s, qE[o + ox1]);
+        s = mg_add(s, qE[o + ox0]);
+        if (nx > 1) s = mg_add(s, qE[o + ox1]);
       }
     }
-    if (!keep) s = 0.0f;
+    if (!keep) s = 0;
     if (MODE == MG_FOLDB) {
       b[c] = s;
       continue;
@@ -1116,14 +1130,14 @@ __global__ void __launch_bounds__(RED_THREADS)
       x[c] = c1 * (dv * s);
       continue;
     }
-    const float rc = bc - s;
+    const TM rc = bc - s;
     if (MODE == MG_RESID) {
       res[c] = rc;
       continue;
     }
-    const float dp = dsrc == DP_X ? xo : dpv;
-    const float dc = c1 * dp + c2 * (dv * rc);
-    const float xc = xo + dc;
+    const TM dp = dsrc == DP_X ? xo : dpv;
+    const TM dc = c1 * dp + c2 * (dv * rc);
+    const TM xc = xo + dc;
     x[c] = xc;
     if (wd) d[c] = dc;
     if (DOTS) rz += (double)bc * (double)xc;
@@ -1154,15 +1168,16 @@ __global__ void k_fill_hash(int64_t n, const uint8_t *__restrict__ mask, double 
 
 // coarsest-level solve x[free_i] = sum_j Ainv(i, j) b[free_j]: one block
 // per row (the masked points of x stay 0)
+template <typename TM>
 __global__ void __launch_bounds__(128)
-    k_dense_solve(int64_t nfree, const float *__restrict__ ainv, const int32_t *__restrict__ idx,
-                  const float *__restrict__ b, float *__restrict__ x, const double *stop) {
+    k_dense_solve(int64_t nfree, const TM *__restrict__ ainv, const int32_t *__restrict__ idx,
+                  const TM *__restrict__ b, TM *__restrict__ x, const double *stop) {
   if (stop && *stop != 0.0) return;
-  __shared__ float sh[4];
+  __shared__ TM sh[4];
   for (int64_t i = blockIdx.x; i < nfree; i += gridDim.x) {
-    const float *row = ainv + i * nfree;
-    float s = 0.0f;
-    for (int64_t j = threadIdx.x; j < nfree; j += blockDim.x) s = fmaf(row[j], b[idx[j]], s);
+    const TM *row = ainv + i * nfree;
+    TM s = 0;
+    for (int64_t j = threadIdx.x; j < nfree; j += blockDim.x) s = mg_fma(row[j], b[idx[j]], s);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -1507,13 +1522,14 @@ struct Solver {
     if (!bL || !xL || !rL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "CG work allocation failed");
     double *d64 = nullptr;
     float *d32 = nullptr;
-    if (tr.precond == GF_PRECOND_PMG) {
+    const bool pmg = tr.precond == GF_PRECOND_PMG || tr.precond == GF_PRECOND_PMG64;
+    if (pmg) {
       // the hierarchy's set-up runs its own short solves on this problem's
       // scalar block and work slots, so it comes before the solve's state
       int rc = mg_prepare(*this, tr, p, q, use_mass);
       if (rc) return rc;
     }
-    if (tr.precond != GF_PRECOND_NONE && tr.precond != GF_PRECOND_PMG) {
+    if (tr.precond != GF_PRECOND_NONE && !pmg) {
       int rc = jacobi(p, q, use_mass, &d64, &d32);
       if (rc) return gf_fail(ctx, rc, "Jacobi set-up failed");
     }
@@ -1532,7 +1548,7 @@ struct Solver {
     if (tr.precond == GF_PRECOND_CHEBYSHEV) {
       rc = solve_poly(tr, p, q, use_mass, bL, xL, rL, qE, d64, d32, hist, &total, &rn);
       if (rc < 0) return rc;
-    } else if (tr.precond == GF_PRECOND_PMG) {
+    } else if (pmg) {
       rc = solve_mg(*this, tr, p, q, use_mass, bL, xL, rL, qE, hist, &total, &rn);
       if (rc < 0) return rc;
     } else if (tr.precision == GF_CG_FP64) {
@@ -1646,31 +1662,34 @@ struct Solver {
 // with a dense inverse (one kernel), a larger one with a Chebyshev solve.
 constexpr int64_t MG_DENSE_SMALL = 512, MG_DENSE_MAX = 729;
 
+// TM: the type the level's vectors, smoother coefficients, transfers and
+// applies use (float: the FP32 V-cycle; double: the FP64 one).
+template <typename TM>
 struct MGLevelBase {
   gf_problem *prob = nullptr;
   bool owned = false;
   int dim = 3;
   int64_t nL = 0, nE = 0;
   int M[3] = {1, 1, 1};
-  float *dinv = nullptr, *b = nullptr, *x = nullptr, *res = nullptr, *d = nullptr, *qE = nullptr;
+  TM *dinv = nullptr, *b = nullptr, *x = nullptr, *res = nullptr, *d = nullptr, *qE = nullptr;
   const uint8_t *maskL = nullptr;  // lattice Dirichlet mask (null: none)
   int m = 0;  // smoothing degree (the coarsest level: its solve degree)
-  float c0 = 0.0f;
-  std::vector<float> c1, c2;
+  TM c0 = 0;
+  std::vector<TM> c1, c2;
   double lmax = 0.0;
   // coarsest level: x = Ainv b on the free lattice points (dense inverse)
   int64_t nfree = 0;
-  const float *ainv = nullptr;
+  const TM *ainv = nullptr;
   const int32_t *free_idx = nullptr;
   // transfer to the next coarser level
-  Xfer1D X[3];
-  float *t1 = nullptr, *t2 = nullptr;
+  Xfer1D<TM> X[3];
+  TM *t1 = nullptr, *t2 = nullptr;
   std::vector<void *> mem;
-  float *alloc_f(int64_t n) {
+  TM *alloc_f(int64_t n) {
     void *p = nullptr;
-    if (cudaMalloc(&p, sizeof(float) * std::max<int64_t>(n, 1)) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&p, sizeof(TM) * std::max<int64_t>(n, 1)) != cudaSuccess) return nullptr;
     mem.push_back(p);
-    return (float *)p;
+    return (TM *)p;
   }
   template <typename V>
   V *upload(const std::vector<V> &h) {
@@ -1684,9 +1703,9 @@ struct MGLevelBase {
     for (void *p : mem) cudaFree(p);
     if (owned && prob) gf_problem_destroy(prob);
   }
-  virtual int apply(const float *in, double p, double q, int use_mass, const double *stop,
+  virtual int apply(const TM *in, double p, double q, int use_mass, const double *stop,
                     cudaStream_t st) = 0;
-  virtual void pass(int mode, bool dots, float a1, float a2, int dsrc, int wd,
+  virtual void pass(int mode, bool dots, TM a1, TM a2, int dsrc, int wd,
                     gf_problem *outer, cudaStream_t st) = 0;
   virtual int jacobi(double p, double q, int use_mass) = 0;
   virtual int estimate(double p, double q, int use_mass, int64_t nfree) = 0;
@@ -1697,9 +1716,13 @@ struct MGLevelBase {
   virtual void prolong_elem(const MGLevelBase &C, gf_problem *outer, cudaStream_t st) = 0;
 };
 
-template <int N>
-struct MGLevel : MGLevelBase {
+template <int N, typename TM>
+struct MGLevel : MGLevelBase<TM> {
+  using B = MGLevelBase<TM>;
+  using B::prob, B::owned, B::dim, B::nL, B::nE, B::M, B::dinv, B::b, B::x, B::res, B::d, B::qE,
+      B::maskL, B::X, B::lmax;
   Solver<MapBox<N>> S;
+  const float *dinv32 = nullptr;  // FP32 Jacobi weights of the eigenvalue estimate
   MGLevel(gf_problem *lp, bool own, bool masked) : S(lp, MapBox<N>::make(lp->box), masked) {
     prob = lp;
     owned = own;
@@ -1709,18 +1732,18 @@ struct MGLevel : MGLevelBase {
     for (int k = 0; k < 3; k++) M[k] = (int)lp->box.M[k];
     maskL = S.wt.maskL;
   }
-  int apply(const float *in, double p, double q, int use_mass, const double *stop,
+  int apply(const TM *in, double p, double q, int use_mass, const double *stop,
             cudaStream_t st) override {
-    return launch_helm_L<float>(prob, (float)p, (float)q, use_mass, in, qE, st, stop);
+    return launch_helm_L<TM>(prob, (TM)p, (TM)q, use_mass, in, qE, st, stop);
   }
   template <int MODE, bool DOTS>
-  void run_pass(float a1, float a2, int dsrc, int wd, gf_problem *outer, cudaStream_t st) {
-    auto kern = k_mg_pass_lat<N, MODE, DOTS>;
+  void run_pass(TM a1, TM a2, int dsrc, int wd, gf_problem *outer, cudaStream_t st) {
+    auto kern = k_mg_pass_lat<N, MODE, DOTS, TM>;
     kern<<<S.rgrid(kern), RED_THREADS, 0, st>>>(S.map, S.wt, qE, b, dinv, a1, a2, res, d, x, dsrc,
                                                  wd, outer->scal_d, outer->partials,
                                                  outer->counter);
   }
-  void pass(int mode, bool dots, float a1, float a2, int dsrc, int wd, gf_problem *outer,
+  void pass(int mode, bool dots, TM a1, TM a2, int dsrc, int wd, gf_problem *outer,
             cudaStream_t st) override {
     outer->launches++;
     if (mode == MG_RESID) run_pass<MG_RESID, false>(a1, a2, dsrc, wd, outer, st);
@@ -1729,33 +1752,37 @@ struct MGLevel : MGLevelBase {
     else if (dots) run_pass<MG_STEP, true>(a1, a2, dsrc, wd, outer, st);
     else run_pass<MG_STEP, false>(a1, a2, dsrc, wd, outer, st);
   }
-  void restrict_elem(MGLevelBase &C, gf_problem *outer, cudaStream_t st) override {
+  void restrict_elem(B &C, gf_problem *outer, cudaStream_t st) override {
     constexpr int NT = N * N, EPB = (256 / NT) < 1 ? 1 : 256 / NT;
     const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
     outer->launches++;
-    k_pxfer_restrict<N><<<grid, dim3(NT, EPB), 0, st>>>(prob->box, X[0], res, C.qE,
-                                                        outer->scal_d + S_DONE);
+    k_pxfer_restrict<N, TM><<<grid, dim3(NT, EPB), 0, st>>>(prob->box, X[0], res, C.qE,
+                                                            outer->scal_d + S_DONE);
   }
-  void prolong_elem(const MGLevelBase &C, gf_problem *outer, cudaStream_t st) override {
+  void prolong_elem(const B &C, gf_problem *outer, cudaStream_t st) override {
     constexpr int NT = N * N, EPB = (256 / NT) < 1 ? 1 : 256 / NT;
     const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
     outer->launches++;
-    k_pxfer_prolong<N><<<grid, dim3(NT, EPB), 0, st>>>(prob->box, C.prob->box, X[0], C.x, x,
-                                                       outer->scal_d + S_DONE);
+    k_pxfer_prolong<N, TM><<<grid, dim3(NT, EPB), 0, st>>>(prob->box, C.prob->box, X[0], C.x, x,
+                                                           outer->scal_d + S_DONE);
   }
   int jacobi(double p, double q, int use_mass) override {
     double *d64 = nullptr;
     float *d32 = nullptr;
     int rc = S.jacobi(p, q, use_mass, &d64, &d32);
     if (rc) return rc;
-    return cudaMemcpyAsync(dinv, d32, sizeof(float) * nL, cudaMemcpyDeviceToDevice, S.st) ==
+    dinv32 = d32;
+    const void *src = std::is_same<TM, float>::value ? (const void *)d32 : (const void *)d64;
+    return cudaMemcpyAsync(dinv, src, sizeof(TM) * nL, cudaMemcpyDeviceToDevice, S.st) ==
                    cudaSuccess
                ? GF_OK
                : GF_ERR_CUDA;
   }
   // Largest eigenvalue of Dinv A: Lanczos Ritz value from min(12, nfree)
-  // FP32 PCG steps on a pseudo-random right-hand side.  Runs on the level
-  // problem's own scalar block and work slots (set-up only).
+  // FP32 PCG steps on a pseudo-random right-hand side (whatever the
+  // multigrid's type: the estimate only places the smoothing interval).
+  // Runs on the level problem's own scalar block and work slots (set-up
+  // only), right after jacobi().
   int estimate(double p, double q, int use_mass, int64_t nfree) override {
     const int K = (int)std::min<int64_t>(12, std::max<int64_t>(nfree, 1));
     gf_cg_traits tr{};
@@ -1782,13 +1809,15 @@ struct MGLevel : MGLevelBase {
     k_fill_hash<<<S.gL, 256, 0, S.st>>>(nL, S.wt.maskL, bL);
     cudaMemsetAsync(xL, 0, sizeof(double) * nL, S.st);
     cudaMemsetAsync(x32, 0, sizeof(float) * nL, S.st);
-    int rc = S.template residual<float>(p, q, use_mass, bL, xL, qE64, rL, r32, w32, dinv, 0, 1e-300);
+    if (!dinv32) return GF_ERR_ARG;
+    int rc =
+        S.template residual<float>(p, q, use_mass, bL, xL, qE64, rL, r32, w32, dinv32, 0, 1e-300);
     if (rc) return rc;
     int its = 0;
     S.ab = abd;
     S.nab = K;
-    rc = S.template iterate<float>(tr, K, p, q, use_mass, x32, r32, w32, q32, qE32, dinv, nullptr,
-                                   &its);
+    rc = S.template iterate<float>(tr, K, p, q, use_mass, x32, r32, w32, q32, qE32, dinv32,
+                                   nullptr, &its);
     S.ab = nullptr;
     S.nab = 0;
     if (rc) return rc;
@@ -1803,22 +1832,26 @@ struct MGLevel : MGLevelBase {
 
 template <int N>
 struct MakeLevel {
-  static int run(gf_problem *lp, bool own, bool masked, MGLevelBase **out) {
-    *out = new MGLevel<N>(lp, own, masked);
+  template <typename TM>
+  static int run(gf_problem *lp, bool own, bool masked, MGLevelBase<TM> **out) {
+    *out = new MGLevel<N, TM>(lp, own, masked);
     return GF_OK;
   }
 };
 
+constexpr int MG_NKEY = 7;  // p, q, use_mass, masked, degree, ratio, type
+
+template <typename TM>
 struct MGHier {
-  std::vector<MGLevelBase *> lv;
-  double key[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<MGLevelBase<TM> *> lv;
+  double key[MG_NKEY] = {0, 0, 0, 0, 0, 0, 0};
   // CUDA graph of the whole iteration loop: a WHILE conditional node whose
   // body is one CG iteration followed by k_while_more (captured on the
   // first solve with these vectors, replayed by later solves)
   cudaStream_t cs = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  // buffers the recorded loop reads, and the FP32 apply kernel it launches
+  // buffers the recorded loop reads, and the FP32 apply variant it launches
   const void *gkey[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   uint64_t glaunches = 0;  // launches per iteration
   void drop_graph() {
@@ -1834,7 +1867,11 @@ struct MGHier {
   }
 };
 
-void mg_free(void *h) { delete (MGHier *)h; }
+// the problem's hierarchy is an MGHier<TM> exactly when its mg_free is mg_free<TM>
+template <typename TM>
+void mg_free(void *h) {
+  delete (MGHier<TM> *)h;
+}
 
 // A coarser level as a light problem: what the affine K1 apply, the
 // Jacobi diagonal and the lattice assembly read.
@@ -1910,8 +1947,9 @@ int mg_light_problem(gf_context *ctx, int dim, const int (&ne)[3], const int (&p
 // of nec: the fine point at offset r in a coarse element takes the coarse
 // element's GLL Lagrange interpolant at its position (element-local
 // coordinates; the fine GLL nodes of uniform children).
-Xfer1D build_xfer(int nef, int pf, int nec, int pc, bool per) {
-  Xfer1D T{};
+template <typename TM>
+Xfer1D<TM> build_xfer(int nef, int pf, int nec, int pc, bool per) {
+  Xfer1D<TM> T{};
   const int ratio = nef / nec;
   T.R = ratio * pf;
   T.pc = pc;
@@ -1930,7 +1968,7 @@ Xfer1D build_xfer(int nef, int pf, int nec, int pc, bool per) {
       for (int bb = 0; bb <= pc; bb++)
         if (bb != a) w *= (xi - xc[bb]) / (xc[a] - xc[bb]);
       if (std::fabs(w) < 1e-13) w = 0.0;
-      T.J[r * (pc + 1) + a] = (float)w;
+      T.J[r * (pc + 1) + a] = (TM)w;
     }
   }
   return T;
@@ -1959,8 +1997,9 @@ __global__ void k_boxmask_mismatch(int64_t nL, BoxLattice L, const uint8_t *__re
 // summed into the lattice, Cholesky-factored and inverted.  Returns false
 // when the matrix is not positive definite (the level then keeps its
 // Chebyshev solve).
+template <typename TM>
 bool mg_dense_inverse(const gf_problem *lp, const std::vector<double> &eg, double p, double q,
-                      int use_mass, const uint8_t *maskL_host, std::vector<float> &ainv,
+                      int use_mass, const uint8_t *maskL_host, std::vector<TM> &ainv,
                       std::vector<int32_t> &free_idx) {
   const BoxLattice &L = lp->box;
   const int dim = lp->dim, n = lp->n;
@@ -2031,7 +2070,7 @@ bool mg_dense_inverse(const gf_problem *lp, const std::vector<double> &eg, doubl
     }
   }
   // inverse column by column: L y = e_c, L^T z = y
-  ainv.assign((size_t)nf * nf, 0.0f);
+  ainv.assign((size_t)nf * nf, TM(0));
   std::vector<double> y(nf);
   for (int64_t c = 0; c < nf; c++) {
     for (int64_t i = 0; i < nf; i++) {
@@ -2044,23 +2083,24 @@ bool mg_dense_inverse(const gf_problem *lp, const std::vector<double> &eg, doubl
       for (int64_t k = i + 1; k < nf; k++) v -= A[(size_t)k * nf + i] * y[k];
       y[i] = v / A[(size_t)i * nf + i];
     }
-    for (int64_t i = 0; i < nf; i++) ainv[(size_t)i * nf + c] = (float)y[i];
+    for (int64_t i = 0; i < nf; i++) ainv[(size_t)i * nf + c] = (TM)y[i];
   }
   return true;
 }
 
-void mg_coefficients(MGLevelBase &L, int m, double ratio) {
+template <typename TM>
+void mg_coefficients(MGLevelBase<TM> &L, int m, double ratio) {
   const double bb = 1.1 * L.lmax, a = bb / ratio;
   const double theta = 0.5 * (bb + a), delta = 0.5 * (bb - a), sigma = theta / delta;
   L.m = m;
-  L.c0 = (float)(1.0 / theta);
-  L.c1.assign(m + 1, 0.0f);
-  L.c2.assign(m + 1, 0.0f);
+  L.c0 = (TM)(1.0 / theta);
+  L.c1.assign(m + 1, TM(0));
+  L.c2.assign(m + 1, TM(0));
   double rho = 1.0 / sigma;
   for (int j = 1; j <= m; j++) {
     const double rn1 = 1.0 / (2.0 * sigma - rho);
-    L.c1[j] = (float)(rn1 * rho);
-    L.c2[j] = (float)(2.0 * rn1 / delta);
+    L.c1[j] = (TM)(rn1 * rho);
+    L.c2[j] = (TM)(2.0 * rn1 / delta);
     rho = rn1;
   }
 }
@@ -2070,8 +2110,8 @@ struct IsBox : std::false_type {};
 template <int N>
 struct IsBox<MapBox<N>> : std::true_type {};
 
-template <class MAP>
-int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass) {
+template <class MAP, typename TM>
+int mg_prepare_t(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass) {
   gf_problem *prob = S.prob;
   gf_context *ctx = S.ctx;
   if constexpr (!IsBox<MAP>::value) {
@@ -2082,10 +2122,13 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
     const bool masked = S.wt.maskL != nullptr;
     const int m = std::max(0, tr.poly_degree);
     const double ratio = tr.poly_ratio > 1.0 ? tr.poly_ratio : 8.0;
-    const double key[6] = {p, q, (double)use_mass, masked ? 1.0 : 0.0, (double)m, ratio};
+    const double key[MG_NKEY] = {p,          q,     (double)use_mass, masked ? 1.0 : 0.0,
+                                 (double)m, ratio, (double)sizeof(TM)};
     if (prob->mg) {
-      MGHier *H = (MGHier *)prob->mg;
-      if (std::equal(key, key + 6, H->key)) return GF_OK;
+      if (prob->mg_free == mg_free<TM>) {
+        MGHier<TM> *H = (MGHier<TM> *)prob->mg;
+        if (std::equal(key, key + MG_NKEY, H->key)) return GF_OK;
+      }
       prob->mg_free(prob->mg);
       prob->mg = nullptr;
     }
@@ -2161,8 +2204,8 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
       }
       ds.push_back(c);
     }
-    MGHier *H = new MGHier();
-    std::copy(key, key + 6, H->key);
+    MGHier<TM> *H = new MGHier<TM>();
+    std::copy(key, key + MG_NKEY, H->key);
     auto fail = [&](int rc, const char *what) {
       delete H;
       return gf_fail(ctx, rc, "PMG set-up: %s", what);
@@ -2174,7 +2217,7 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
         int rc = mg_light_problem(ctx, dim, ds[l].ne, per, ds[l].p, ds[l].eg, masked, &lp);
         if (rc) return fail(rc, "level allocation failed");
       }
-      MGLevelBase *L = nullptr;
+      MGLevelBase<TM> *L = nullptr;
       int rc = dispatch_n<MakeLevel>(ds[l].p + 1, lp, l > 0, masked, &L);
       if (rc || !L) {
         if (l > 0) gf_problem_destroy(lp);
@@ -2199,14 +2242,14 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
           mk.assign((size_t)L->nL, 0);
           GF_CUDA(ctx, cudaMemcpy(mk.data(), L->maskL, L->nL, cudaMemcpyDeviceToHost));
         }
-        std::vector<float> ai;
+        std::vector<TM> ai;
         std::vector<int32_t> fi;
         if (mg_dense_inverse(lp, ds[l].eg, p, q, use_mass, masked ? mk.data() : nullptr, ai, fi)) {
           L->ainv = L->upload(ai);
           L->free_idx = L->upload(fi);
           L->nfree = (int64_t)fi.size();
           if (!L->ainv || !L->free_idx) return fail(GF_ERR_NOMEM, "coarse inverse allocation failed");
-          GF_CUDA(ctx, cudaMemset(L->x, 0, sizeof(float) * L->nL));
+          GF_CUDA(ctx, cudaMemset(L->x, 0, sizeof(TM) * L->nL));
           dense = true;
         }
       }
@@ -2220,9 +2263,10 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
         else mg_coefficients(*L, m, ratio);
       }
       if (l > 0) {  // transfer between levels l-1 (fine) and l
-        MGLevelBase *F = H->lv[l - 1];
+        MGLevelBase<TM> *F = H->lv[l - 1];
         for (int k = 0; k < dim; k++)
-          F->X[k] = build_xfer(ds[l - 1].ne[k], ds[l - 1].p, ds[l].ne[k], ds[l].p, B.per[k] != 0);
+          F->X[k] = build_xfer<TM>(ds[l - 1].ne[k], ds[l - 1].p, ds[l].ne[k], ds[l].p,
+                                   B.per[k] != 0);
         // same elements, coarse order as the element kernels assume
         F->ptransfer = dim == 3 && ds[l - 1].ne[0] == ds[l].ne[0] &&
                        ds[l - 1].ne[1] == ds[l].ne[1] && ds[l - 1].ne[2] == ds[l].ne[2] &&
@@ -2239,25 +2283,26 @@ int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int u
     GF_CUDA(ctx, cudaStreamSynchronize(st));
     for (size_t l = 1; l < H->lv.size(); l++) H->lv[l]->prob->launches = 0;
     prob->mg = H;
-    prob->mg_free = mg_free;
+    prob->mg_free = mg_free<TM>;
     return GF_OK;
   }
 }
 
 // restriction lv[l].res -> lv[l+1].b (coarse mask), prolongation
 // lv[l].x += P lv[l+1].x; one k_xfer1d sweep per direction
-void mg_restrict(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t st) {
+template <typename TM>
+void mg_restrict(MGLevelBase<TM> &F, MGLevelBase<TM> &C, gf_problem *outer, cudaStream_t st) {
   const double *stop = outer->scal_d + S_DONE;
   const int dim = F.dim;
   int e[3] = {F.M[0], F.M[1], F.M[2]};
-  const float *in = F.res;
+  const TM *in = F.res;
   for (int k = 0; k < dim; k++) {
     int eo[3] = {e[0], e[1], e[2]};
     eo[k] = C.M[k];
     const bool last = k == dim - 1;
-    float *out = last ? C.b : (k == 0 ? F.t1 : F.t2);
+    TM *out = last ? C.b : (k == 0 ? F.t1 : F.t2);
     const int64_t nout = (int64_t)eo[0] * eo[1] * eo[2];
-    k_xfer1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(
+    k_xfer1d<TM><<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(
         nout, k, eo[0], eo[1], e[0], e[1], F.X[k], 1, in, out, last ? C.maskL : nullptr,
         last ? 2 : 0, stop);
     outer->launches++;
@@ -2266,20 +2311,21 @@ void mg_restrict(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t
   }
 }
 
-void mg_prolong(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t st) {
+template <typename TM>
+void mg_prolong(MGLevelBase<TM> &F, MGLevelBase<TM> &C, gf_problem *outer, cudaStream_t st) {
   const double *stop = outer->scal_d + S_DONE;
   const int dim = F.dim;
   int e[3] = {C.M[0], C.M[1], C.M[2]};
-  const float *in = C.x;
+  const TM *in = C.x;
   for (int k = 0; k < dim; k++) {
     int eo[3] = {e[0], e[1], e[2]};
     eo[k] = F.M[k];
     const bool last = k == dim - 1;
-    float *out = last ? F.x : (k == 0 ? F.t1 : F.t2);
+    TM *out = last ? F.x : (k == 0 ? F.t1 : F.t2);
     const int64_t nout = (int64_t)eo[0] * eo[1] * eo[2];
-    k_xfer1d<<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(nout, k, eo[0], eo[1], e[0], e[1],
-                                                            F.X[k], 0, in, out, nullptr,
-                                                            last ? 1 : 0, stop);
+    k_xfer1d<TM><<<grid_for(nout, 256, 148 * 16), 256, 0, st>>>(nout, k, eo[0], eo[1], e[0],
+                                                                e[1], F.X[k], 0, in, out, nullptr,
+                                                                last ? 1 : 0, stop);
     outer->launches++;
     in = out;
     e[k] = F.M[k];
@@ -2289,26 +2335,28 @@ void mg_prolong(MGLevelBase &F, MGLevelBase &C, gf_problem *outer, cudaStream_t 
 // One V-cycle from level l: lv[l].x ~= A_l^-1 lv[l].b.  At l = 0 the input
 // is the FP64 outer residual r64 and the last pass reduces <r, z> for the
 // CG step.
-void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem *outer,
+template <typename TM>
+void mg_vcycle(MGHier<TM> &H, size_t l, double p, double q, int use_mass, gf_problem *outer,
                const double *r64, bool started, cudaStream_t st) {
-  MGLevelBase &L = *H.lv[l];
+  MGLevelBase<TM> &L = *H.lv[l];
   const double *stop = outer->scal_d + S_DONE;
   const bool top = l == 0, last = l + 1 == H.lv.size();
+  const TM zero = 0;
   // b arrives as the element restriction's coarse E-vector in L.qE
   const bool folded = l > 0 && H.lv[l - 1]->ptransfer;
   if (last && L.ainv) {  // coarsest: dense solve (never the finest level)
-    if (folded) L.pass(MG_FOLDB, false, 0.0f, 0.0f, DP_NONE, 0, outer, st);
-    k_dense_solve<<<(unsigned)std::min<int64_t>(L.nfree, 148 * 8), 128, 0, st>>>(
+    if (folded) L.pass(MG_FOLDB, false, zero, zero, DP_NONE, 0, outer, st);
+    k_dense_solve<TM><<<(unsigned)std::min<int64_t>(L.nfree, 148 * 8), 128, 0, st>>>(
         L.nfree, L.ainv, L.free_idx, L.b, L.x, stop);
     outer->launches++;
     return;
   }
   // x = c0 Dinv b (the top level's b and x may come from the outer update)
   if (folded) {
-    L.pass(MG_START, false, L.c0, 0.0f, DP_NONE, 0, outer, st);
+    L.pass(MG_START, false, L.c0, zero, DP_NONE, 0, outer, st);
   } else if (!(top && started)) {
-    k_mg_start<<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(L.nL, top ? r64 : nullptr, L.b,
-                                                               L.dinv, L.c0, L.x, stop);
+    k_mg_start<TM><<<grid_for(L.nL, 256, 148 * 16), 256, 0, st>>>(L.nL, top ? r64 : nullptr, L.b,
+                                                                   L.dinv, L.c0, L.x, stop);
     outer->launches++;
   }
   // pre-smoothing x = S b (on the coarsest level: the whole Chebyshev solve)
@@ -2319,7 +2367,7 @@ void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem
   }
   if (last) return;
   L.apply(L.x, p, q, use_mass, stop, st);  // res = b - A x
-  L.pass(MG_RESID, false, 0.0f, 0.0f, DP_NONE, 0, outer, st);
+  L.pass(MG_RESID, false, zero, zero, DP_NONE, 0, outer, st);
   if (L.ptransfer) L.restrict_elem(*H.lv[l + 1], outer, st);
   else mg_restrict(L, *H.lv[l + 1], outer, st);
   mg_vcycle(H, l + 1, p, q, use_mass, outer, r64, false, st);
@@ -2327,24 +2375,26 @@ void mg_vcycle(MGHier &H, size_t l, double p, double q, int use_mass, gf_problem
   else mg_prolong(L, *H.lv[l + 1], outer, st);
   // post-smoothing x += S (b - A x): the first term from the residual
   L.apply(L.x, p, q, use_mass, stop, st);
-  L.pass(MG_STEP, top && L.m == 0, 0.0f, L.c0, DP_NONE, L.m > 0, outer, st);
+  L.pass(MG_STEP, top && L.m == 0, zero, L.c0, DP_NONE, L.m > 0, outer, st);
   for (int j = 1; j <= L.m; j++) {
     L.apply(L.x, p, q, use_mass, stop, st);
     L.pass(MG_STEP, top && j == L.m, L.c1[j], L.c2[j], DP_D, j < L.m, outer, st);
   }
 }
 
-// FP64 CG (Fletcher-Reeves beta, fcg_finish_fr) with one FP32 V-cycle as
-// the preconditioner; per iteration the FP64 apply, assembly with
-// <w,q>, the x/r update with the stop test, the V-cycle and w = z + beta w.
-template <class MAP>
-int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass,
-             const double *bL, double *xL, double *rL, double *qE, double *hist, int *total,
-             double *rn) {
+// FP64 CG (Fletcher-Reeves beta, fcg_finish_fr) with one V-cycle in TM
+// (FP32 or FP64) as the preconditioner; per iteration the FP64 apply,
+// assembly with <w,q>, the x/r update with the stop test, the V-cycle and
+// w = z + beta w.
+template <class MAP, typename TM>
+int solve_mg_t(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass,
+               const double *bL, double *xL, double *rL, double *qE, double *hist, int *total,
+               double *rn) {
   gf_problem *prob = S.prob;
   gf_context *ctx = S.ctx;
-  MGHier *H = (MGHier *)prob->mg;
-  if (!H) return gf_fail(ctx, GF_ERR_ARG, "PMG hierarchy missing");
+  if (!prob->mg || prob->mg_free != mg_free<TM>)
+    return gf_fail(ctx, GF_ERR_ARG, "PMG hierarchy missing");
+  MGHier<TM> *H = (MGHier<TM> *)prob->mg;
   cudaStream_t st = S.st;
   const int64_t nL = S.nL;
   double *w = (double *)gf_work(prob, 4, sizeof(double) * nL);
@@ -2353,20 +2403,20 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
   GF_CUDA(ctx, cudaMemsetAsync(qL, 0, sizeof(double) * nL, st));
   int rc = S.template residual<double>(p, q, use_mass, bL, xL, qE, rL, rL, w, nullptr, 0, tr.tol);
   if (rc) return gf_fail(ctx, rc, "residual failed");
-  const float *z = H->lv[0]->x;
+  const TM *z = H->lv[0]->x;
   double *scal = prob->scal_d;
-  MGLevelBase &L0 = *H->lv[0];
+  MGLevelBase<TM> &L0 = *H->lv[0];
   auto precondition = [&](cudaStream_t ls, bool started) {
     mg_vcycle(*H, 0, p, q, use_mass, prob, rL, started, ls);
     prob->launches++;
-    k_fcg_w<<<S.gL, 256, 0, ls>>>(nL, w, z, scal);
+    k_fcg_w<TM><<<S.gL, 256, 0, ls>>>(nL, w, z, scal);
   };
   auto iterations = [&](int k, cudaStream_t ls) {
     for (int i = 0; i < k; i++) {
       launch_helm_L<double>(prob, p, q, use_mass, w, qE, ls, scal + S_DONE);
       k_asm_dot<double, MAP><<<S.rgrid(k_asm_dot<double, MAP>), RED_THREADS, 0, ls>>>(
           nL, S.map, S.wt, qE, w, qL, scal, prob->partials, prob->counter);
-      k_update_mg<<<S.rgrid(k_update_mg), RED_THREADS, 0, ls>>>(
+      k_update_mg<TM><<<S.rgrid(k_update_mg<TM>), RED_THREADS, 0, ls>>>(
           nL, S.wt, xL, w, rL, qL, L0.dinv, L0.c0, L0.b, L0.x, hist, scal, prob->partials,
           prob->counter);
       prob->launches += 2;
@@ -2442,6 +2492,22 @@ int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use
   return (*total >= tr.maxit && *rn > prob->scal_h[S_RTOL]) ? GF_CG_NOCONVERGE : GF_OK;
 }
 
+// GF_PRECOND_PMG: FP32 V-cycle; GF_PRECOND_PMG64: FP64 V-cycle
+template <class MAP>
+int mg_prepare(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass) {
+  return tr.precond == GF_PRECOND_PMG64 ? mg_prepare_t<MAP, double>(S, tr, p, q, use_mass)
+                                        : mg_prepare_t<MAP, float>(S, tr, p, q, use_mass);
+}
+
+template <class MAP>
+int solve_mg(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int use_mass,
+             const double *bL, double *xL, double *rL, double *qE, double *hist, int *total,
+             double *rn) {
+  return tr.precond == GF_PRECOND_PMG64
+             ? solve_mg_t<MAP, double>(S, tr, p, q, use_mass, bL, xL, rL, qE, hist, total, rn)
+             : solve_mg_t<MAP, float>(S, tr, p, q, use_mass, bL, xL, rL, qE, hist, total, rn);
+}
+
 template <int N>
 struct BoxSolve {
   static int run(gf_problem *prob, const gf_cg_traits *tr, double p, double q, int use_mass,
@@ -2452,7 +2518,81 @@ struct BoxSolve {
   }
 };
 
+// One kernel of the multigrid solve's finest level, launched alone (see
+// gf_pmg_launch).
+template <int N>
+struct PMGLaunch {
+  template <typename TM>
+  static int level0(gf_problem *prob, Solver<MapBox<N>> &S, double p, double q, int use_mass,
+                    int which) {
+    gf_context *ctx = prob->ctx;
+    MGHier<TM> *H = (MGHier<TM> *)prob->mg;
+    MGLevelBase<TM> &L = *H->lv[0];
+    cudaStream_t st = ctx->stream;
+    double *stop = prob->scal_d + S_DONE;
+    if (which == GF_PMG_PREPARE) {
+      // finite values in every vector the launches read, and `done` clear
+      TM *const vecs[4] = {L.b, L.x, L.d, L.res};
+      for (TM *v : vecs) GF_CUDA(ctx, cudaMemsetAsync(v, 0x3c, sizeof(TM) * L.nL, st));
+      GF_CUDA(ctx, cudaMemsetAsync(L.qE, 0x3c, sizeof(TM) * L.nE, st));
+      double *xL = (double *)gf_work(prob, 1, sizeof(double) * S.nL);
+      double *qE = (double *)gf_work(prob, 3, sizeof(double) * S.nE);
+      if (!xL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "work allocation failed");
+      GF_CUDA(ctx, cudaMemsetAsync(xL, 0x3c, sizeof(double) * S.nL, st));
+      GF_CUDA(ctx, cudaMemsetAsync(stop, 0, sizeof(double), st));
+      GF_CUDA(ctx, cudaStreamSynchronize(st));
+      return GF_OK;
+    }
+    int rc = GF_OK;
+    if (which == GF_PMG_APPLY64) {
+      double *xL = (double *)gf_work(prob, 1, sizeof(double) * S.nL);
+      double *qE = (double *)gf_work(prob, 3, sizeof(double) * S.nE);
+      if (!xL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "work allocation failed");
+      rc = launch_helm_L<double>(prob, p, q, use_mass, xL, qE, st, stop);
+    } else if (which == GF_PMG_APPLY) {
+      rc = L.apply(L.x, p, q, use_mass, stop, st);
+    } else if (which == GF_PMG_STEP) {
+      L.pass(MG_STEP, false, L.c1.size() > 1 ? L.c1[1] : TM(0), L.c0, DP_D, 1, prob, st);
+    } else {
+      L.pass(MG_RESID, false, TM(0), TM(0), DP_NONE, 0, prob, st);
+    }
+    if (rc) return gf_fail(ctx, rc, "launch failed");
+    GF_CHECK_LAUNCH(ctx);
+    return GF_OK;
+  }
+  static int run(gf_problem *prob, const gf_cg_traits *tr, double p, double q, int use_mass,
+                 bool masked, int which) {
+    Solver<MapBox<N>> S(prob, MapBox<N>::make(prob->box), masked);
+    if (which == GF_PMG_PREPARE) {
+      int rc = mg_prepare(S, *tr, p, q, use_mass);
+      if (rc) return rc;
+    } else if (!prob->mg) {
+      return gf_fail(prob->ctx, GF_ERR_ARG, "no multigrid hierarchy: GF_PMG_PREPARE first");
+    }
+    return tr->precond == GF_PRECOND_PMG64 ? level0<double>(prob, S, p, q, use_mass, which)
+                                           : level0<float>(prob, S, p, q, use_mass, which);
+  }
+};
+
 }  // namespace
+
+extern "C" int gf_pmg_launch(gf_problem_t prob, const gf_cg_traits *tr, double p, double q,
+                             int use_mass, int masked, int which) {
+  if (!prob || !tr) return GF_ERR_ARG;
+  gf_context *ctx = prob->ctx;
+  GF_REQUIRE(ctx, tr->precond == GF_PRECOND_PMG || tr->precond == GF_PRECOND_PMG64,
+             "traits must name GF_PRECOND_PMG or GF_PRECOND_PMG64");
+  GF_REQUIRE(ctx, which >= GF_PMG_PREPARE && which <= GF_PMG_RESID, "bad kernel selector");
+  GF_REQUIRE(ctx, prob->has_box, "PMG needs a structured box (box_ne)");
+  GF_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (which != GF_PMG_PREPARE) {
+    const bool ok = prob->mg && prob->mg_free == (tr->precond == GF_PRECOND_PMG64
+                                                      ? mg_free<double>
+                                                      : mg_free<float>);
+    GF_REQUIRE(ctx, ok, "no multigrid hierarchy of this type: GF_PMG_PREPARE first");
+  }
+  return dispatch_n<PMGLaunch>(prob->n, prob, tr, p, q, use_mass, masked != 0, which);
+}
 
 extern "C" int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *tr, double p, double q,
                            int use_mass, const double *b, const double *xb, double *x, int *iters,
@@ -2463,7 +2603,7 @@ extern "C" int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *tr, double p, 
   GF_REQUIRE(ctx, tr->maxit >= 0, "maxit must be >= 0");
   GF_REQUIRE(ctx, tr->normtype >= GF_NORM_INF && tr->normtype <= GF_NORM_L1, "bad norm type");
   GF_REQUIRE(ctx, tr->precision == GF_CG_FP64 || tr->precision == GF_CG_MIXED, "bad precision");
-  GF_REQUIRE(ctx, tr->precond >= GF_PRECOND_NONE && tr->precond <= GF_PRECOND_PMG,
+  GF_REQUIRE(ctx, tr->precond >= GF_PRECOND_NONE && tr->precond <= GF_PRECOND_PMG64,
              "bad preconditioner");
   GF_REQUIRE(ctx, tr->precond < GF_PRECOND_CHEBYSHEV || (tr->poly_degree >= 0 &&
                                                         tr->poly_degree <= 64),

@@ -61,8 +61,16 @@ enum { GF_NORM_INF = 0, GF_NORM_EUC = 1, GF_NORM_L2 = 2, GF_NORM_L1 = 3 }; /* li
  * level (interval [lmax/poly_ratio, lmax], lmax from a Lanczos estimate).
  * Structured affine boxes only (box_ne set, GF_GEOM_AFFINE, mask absent or
  * the box-face Dirichlet mask); the hierarchy is kept with the problem and
- * reused while p, q and the traits stay the same.  No reference counterpart. */
-enum { GF_PRECOND_NONE = 0, GF_PRECOND_JACOBI = 1, GF_PRECOND_CHEBYSHEV = 2, GF_PRECOND_PMG = 3 };
+ * reused while p, q and the traits stay the same.  No reference counterpart.
+ * PMG64: the same V-cycle with every level's vectors, transfers, smoother
+ * and coarsest solve in FP64 (what the FP32 V-cycle saves, measured). */
+enum {
+  GF_PRECOND_NONE = 0,
+  GF_PRECOND_JACOBI = 1,
+  GF_PRECOND_CHEBYSHEV = 2,
+  GF_PRECOND_PMG = 3,
+  GF_PRECOND_PMG64 = 4
+};
 enum { GF_CG_FP64 = 0, GF_CG_MIXED = 1 };            /* plain FP64 / FP32 apply + FP64 refinement */
 /* see gf_problem_desc; DEFORMED = GE_DEFORMED, EMBEDDED = GE_2DEMBEDDED */
 enum { GF_GEOM_AFFINE = 0, GF_GEOM_REGULAR = 1, GF_GEOM_DEFORMED = 2, GF_GEOM_EMBEDDED = 3 };
@@ -294,6 +302,21 @@ int gf_cg_solve(gf_problem_t prob, const gf_cg_traits *traits, double p, double 
 int gf_cg_solve_host(gf_problem_t prob, const gf_cg_traits *traits, double p, double q,
                      int use_mass, const double *b, const double *xb, double *x,
                      int *iters, double *final_norm);
+
+/* Launches ONE kernel that the multigrid-preconditioned solve (precond
+ * GF_PRECOND_PMG or GF_PRECOND_PMG64) runs on its finest level, outside
+ * the solve's graph, so that a caller can time it with events on the
+ * context's stream: GF_PMG_PREPARE builds (or reuses) the hierarchy of
+ * these traits and operator (masked = 1: the Dirichlet-masked form, the
+ * solve with xb) and fills the level's vectors with finite values;
+ * GF_PMG_APPLY64 the outer FP64 lattice -> element apply; GF_PMG_APPLY the
+ * V-cycle's lattice -> element apply (FP32 or FP64); GF_PMG_STEP a
+ * smoother step pass (fold, residual, x and d update); GF_PMG_RESID the
+ * residual pass.  Overwrites the hierarchy's vectors and the problem's CG
+ * work vectors.  Not a reference interface (measurement only). */
+enum { GF_PMG_PREPARE = 0, GF_PMG_APPLY64 = 1, GF_PMG_APPLY = 2, GF_PMG_STEP = 3, GF_PMG_RESID = 4 };
+int gf_pmg_launch(gf_problem_t prob, const gf_cg_traits *traits, double p, double q, int use_mass,
+                  int masked, int which);
 
 /* ---- explicit RK (pdes/gexrk_stepper.ipp) on the GBurgers RHS ---- */
 typedef struct {

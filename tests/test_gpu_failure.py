@@ -24,6 +24,7 @@ PATHS = {
     "mixed": dict(precond=A.GF_PRECOND_JACOBI, precision=A.GF_CG_MIXED, check_every=4),
     "chebyshev": dict(precond=A.GF_PRECOND_CHEBYSHEV, poly_degree=2),
     "pmg": dict(precond=A.GF_PRECOND_PMG, poly_degree=1),
+    "pmg64": dict(precond=A.GF_PRECOND_PMG64, poly_degree=1),
 }
 
 

@@ -148,3 +148,45 @@ def test_pmg_refuses_unstructured_problem(ctx):
     it, rn = C.c_int(), C.c_double()
     assert lib.gf_cg_solve(prob.handle, C.byref(tr), 1.0, 1.0, 1, A.ptr(b), A.ptr(b), A.ptr(x),
                            C.byref(it), C.byref(rn), None) == A.GF_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("dim,ne,p,per,m", CASES)
+def test_pmg64_reaches_fp64_solution(ctx, dim, ne, p, per, m):
+    """The FP64 V-cycle (GF_PRECOND_PMG64): the same solution as Jacobi-PCG
+    and, on the same hierarchy, no more iterations than the FP32 V-cycle
+    (the two preconditioners differ by FP32 rounding only)."""
+    g = GridBox(dim, ne, p, periodic=per)
+    prob = Problem(ctx, g)
+    b = rhs(g, 3 + p)
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    xj = prob.zeros()
+    assert GCG(CGTraits(precond=A.GF_PRECOND_JACOBI, **COMMON), prob).solve(
+        H, dev(b), dev(0 * b), xj) == 0
+    its = {}
+    for pc in (A.GF_PRECOND_PMG64, A.GF_PRECOND_PMG):
+        x = prob.zeros()
+        cg = GCG(CGTraits(precond=pc, poly_degree=m, **COMMON), prob)
+        assert cg.solve(H, dev(b), dev(0 * b), x) == 0
+        assert relerr(host(x), host(xj)) < 1e-9
+        its[pc] = cg.iter_
+    assert its[A.GF_PRECOND_PMG64] <= its[A.GF_PRECOND_PMG] + 1, its
+
+
+def test_pmg64_and_pmg_alternate_on_one_problem(ctx):
+    """Switching between the FP64 and FP32 V-cycles on one problem rebuilds
+    the hierarchy each time; a repeated solve with either is bit-identical."""
+    g = GridBox(3, [4, 4, 2], 5)
+    prob = Problem(ctx, g)
+    b = dev(rhs(g, 9))
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    out = {}
+    for pc in (A.GF_PRECOND_PMG64, A.GF_PRECOND_PMG, A.GF_PRECOND_PMG64, A.GF_PRECOND_PMG):
+        x = prob.zeros()
+        cg = GCG(CGTraits(precond=pc, **COMMON), prob)
+        assert cg.solve(H, b, 0 * b, x) == 0
+        if pc in out:
+            assert bool((out[pc] == x).all())
+        out[pc] = x
+    assert relerr(host(out[A.GF_PRECOND_PMG64]), host(out[A.GF_PRECOND_PMG])) < 1e-9
