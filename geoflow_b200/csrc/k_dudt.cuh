@@ -36,6 +36,20 @@ template <int N, int NF> constexpr int epb_dudt3() {
   return (160 / (N * N)) < 1 ? 1 : (160 / (N * N));
 }
 
+// Words per element slot of k_dudt3d's shared memory: NF + 2 padded
+// volumes, plus (FP32, N <= 7) a pad that puts the next slot at the bank
+// offset (slot words mod 32) minimising the shared-memory wavefronts of the
+// x-, y- and z-line accesses of the warps that straddle two slots
+// (36-thread elements at N = 6 and so on).  The residues come from
+// counting the wavefronts of every warp of the block for each residue
+// 0..31: N = 6: 168 -> 138 per component pass, N = 5: 140 -> 120.
+template <typename T, int N, int NF> constexpr int dudt_slot() {
+  constexpr int P = (N % 2) ? N : N + 1, W = (NF + 2) * N * N * P;
+  constexpr int want = N == 3 ? 27 : N == 4 ? 16 : N == 5 ? 25 : N == 6 ? 28 : N == 7 ? 17 : -1;
+  if (sizeof(T) != 4 || want < 0) return W;
+  return W + ((want - W % 32) + 32) % 32;
+}
+
 // fields[0..NF): ADVECT: {p, c0, c1, c2}; BURGERS: {u0, u1, u2}; HEAT: {u}.
 // Evolved components: ADVECT/HEAT: field 0; BURGERS: fields 0..2.
 // AFF: affine elements (g.egeom), known at compile time, so the per-node
@@ -50,7 +64,7 @@ __global__ void __launch_bounds__(N *N *EPB)
   constexpr int NC = EQN == GF_EQN_BURGERS ? 3 : 1;  // evolved components
   constexpr int P = Pad<N>::P, PLANE = N * P, VOL = N * PLANE, NN = N * N, NNN = N * N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *s = reinterpret_cast<T *>(smem_raw) + threadIdx.y * (NF + 2) * VOL;
+  T *s = reinterpret_cast<T *>(smem_raw) + threadIdx.y * dudt_slot<T, N, NF>();
   T *sdx = s + NF * VOL, *sdy = s + (NF + 1) * VOL;
   const int t = threadIdx.x;
   const int64_t e = (int64_t)blockIdx.x * EPB + threadIdx.y;

@@ -169,7 +169,7 @@ inline void launch_dudt_kernel(gf_problem *prob, T nu, const T *const *f, T *con
   if (prob->dim == 3) {
     constexpr int NF = EQN == GF_EQN_ADVECT ? 4 : (EQN == GF_EQN_BURGERS ? 3 : 1);
     constexpr int EPB = epb_dudt3<N, NF>();
-    const size_t smem = sizeof(T) * (NF + 2) * N * N * P * EPB;
+    const size_t smem = sizeof(T) * dudt_slot<T, N, NF>() * EPB;
     auto kern = g.egeom ? k_dudt3d<T, N, EPB, EQN, MODE, true> : k_dudt3d<T, N, EPB, EQN, MODE, false>;
     set_smem(kern, smem);
     const unsigned grid = (unsigned)((prob->ne + EPB - 1) / EPB);
