@@ -190,3 +190,33 @@ def test_pmg64_and_pmg_alternate_on_one_problem(ctx):
             assert bool((out[pc] == x).all())
         out[pc] = x
     assert relerr(host(out[A.GF_PRECOND_PMG64]), host(out[A.GF_PRECOND_PMG])) < 1e-9
+
+
+@pytest.mark.parametrize("pc", [A.GF_PRECOND_PMG, A.GF_PRECOND_PMG64])
+def test_pmg_launch_single_kernels(ctx, pc):
+    """gf_pmg_launch (single finest-level kernels for timing): refused before
+    the hierarchy exists and for other preconditioners; after
+    GF_PMG_PREPARE every selector launches, and a later solve on the same
+    hierarchy is bit-identical to the one before the launches."""
+    g = GridBox(3, [4, 4, 4], 5)
+    prob = Problem(ctx, g)
+    b = dev(rhs(g, 21))
+    H = GHelmholtz(prob)
+    H.set_mass_scalar(1.0)
+    lib = A.load()
+    tr = CGTraits(precond=pc, **COMMON)
+    trc = tr.to_c()
+    assert lib.gf_pmg_launch(prob.handle, C.byref(trc), 1.0, 1.0, 1, 1,
+                             A.GF_PMG_STEP) == A.GF_ERR_ARG
+    bad = CGTraits(precond=A.GF_PRECOND_JACOBI, **COMMON).to_c()
+    assert lib.gf_pmg_launch(prob.handle, C.byref(bad), 1.0, 1.0, 1, 1,
+                             A.GF_PMG_PREPARE) == A.GF_ERR_ARG
+    cg = GCG(tr, prob)
+    x1 = prob.zeros()
+    assert cg.solve(H, b, 0 * b, x1) == 0
+    for which in (A.GF_PMG_PREPARE, A.GF_PMG_APPLY64, A.GF_PMG_APPLY, A.GF_PMG_STEP,
+                  A.GF_PMG_RESID):
+        assert lib.gf_pmg_launch(prob.handle, C.byref(trc), 1.0, 1.0, 1, 1, which) == 0
+    x2 = prob.zeros()
+    assert cg.solve(H, b, 0 * b, x2) == 0
+    assert bool((x1 == x2).all())
