@@ -72,7 +72,6 @@ __global__ void __launch_bounds__(N *N *EPB)
   const int a0 = t % N, a1 = t / N;
   const int64_t base = e * NNN;
   const T *fin[4] = {f0, f1, f2, f3};
-  T *fout[3] = {o0, o1, o2};
 
   NodeGeom<T, 3> eg;
   eg.X[0] = eg.X[1] = eg.X[2] = eg.J = T(0);
@@ -89,6 +88,11 @@ __global__ void __launch_bounds__(N *N *EPB)
 #pragma unroll 1
   for (int c = 0; c < NC; c++) {
     const T *su = s + c * VOL;
+    // output of component c: by selection in FP32 (48 registers, 8 blocks
+    // per SM at N = 6, against 56 with the array); from a small local array
+    // in FP64, where selection costs registers
+    T *fout[3] = {o0, o1, o2};
+    T *const oc = sizeof(T) == 8 ? fout[c] : (c == 0 ? o0 : (c == 1 ? o1 : o2));
     // x-lines (j=a0,k=a1) and y-lines (i=a0,k=a1): reference gradients
     {
       T a[N], d[N];
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(N *N *EPB)
     if (MODE == MODE_ADVECT) {
       if (active) {
 #pragma unroll
-        for (int k = 0; k < N; k++) fout[c][base + k * NN + a1 * N + a0] = radv[k];
+        for (int k = 0; k < N; k++) oc[base + k * NN + a1 * N + a0] = radv[k];
       }
       __syncthreads();
       continue;
@@ -191,10 +195,10 @@ __global__ void __launch_bounds__(N *N *EPB)
             const T *yc = c == 0 ? epi.y[0] : (c == 1 ? epi.y[1] : epi.y[2]);
             const T *y2c = c == 0 ? epi.y2[0] : (c == 1 ? epi.y2[1] : epi.y2[2]);
             const T uv = epi.uin_is_u ? su[sidx] : ui[node];
-            fout[c][node] = rk_euler_point(K, epi.dt, uv, epi.a, yc, epi.b, epi.a2, y2c, epi.b2,
+            oc[node] = rk_euler_point(K, epi.dt, uv, epi.a, yc, epi.b, epi.a2, y2c, epi.b2,
                                            node);
           } else {
-            fout[c][node] = K;
+            oc[node] = K;
           }
         }
       }
