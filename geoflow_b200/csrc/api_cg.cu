@@ -2240,7 +2240,8 @@ int mg_prepare_t(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int
         std::vector<uint8_t> mk;
         if (masked) {
           mk.assign((size_t)L->nL, 0);
-          GF_CUDA(ctx, cudaMemcpy(mk.data(), L->maskL, L->nL, cudaMemcpyDeviceToHost));
+          if (cudaMemcpy(mk.data(), L->maskL, L->nL, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(GF_ERR_CUDA, "mask copy failed");
         }
         std::vector<TM> ai;
         std::vector<int32_t> fi;
@@ -2249,7 +2250,8 @@ int mg_prepare_t(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int
           L->free_idx = L->upload(fi);
           L->nfree = (int64_t)fi.size();
           if (!L->ainv || !L->free_idx) return fail(GF_ERR_NOMEM, "coarse inverse allocation failed");
-          GF_CUDA(ctx, cudaMemset(L->x, 0, sizeof(TM) * L->nL));
+          if (cudaMemset(L->x, 0, sizeof(TM) * L->nL) != cudaSuccess)
+            return fail(GF_ERR_CUDA, "coarse vector clear failed");
           dense = true;
         }
       }
@@ -2280,7 +2282,7 @@ int mg_prepare_t(Solver<MAP> &S, const gf_cg_traits &tr, double p, double q, int
         if (!F->t1 || !F->t2) return fail(GF_ERR_NOMEM, "transfer allocation failed");
       }
     }
-    GF_CUDA(ctx, cudaStreamSynchronize(st));
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(GF_ERR_CUDA, "set-up failed");
     for (size_t l = 1; l < H->lv.size(); l++) H->lv[l]->prob->launches = 0;
     prob->mg = H;
     prob->mg_free = mg_free<TM>;

@@ -148,6 +148,22 @@ def test_derivatives_match_oracle(ctx, dim, ne, p):
     assert relerr(host(du), o.grefdiv(us, 1)) < 1e-13
 
 
+def test_hackathon_derivative_known_answer_on_gpu(ctx):
+    """hackathon_driver.cpp:224-252 on the device: GGrid::deriv of
+    u = x^2 y^2 z against its analytic derivatives, L2 relative error within
+    100 eps (the polynomial lies in the p = 4 space)."""
+    g, prob, o = setup(ctx, 3, [3, 2, 2], 4)
+    lib = A.load()
+    x, y, z = g.xyz[0], g.xyz[1], g.xyz[2]
+    u = x ** 2 * y ** 2 * z
+    du = prob.zeros()
+    for idir, exact in ((1, 2 * x * y ** 2 * z), (2, 2 * x ** 2 * y * z), (3, x ** 2 * y ** 2)):
+        ctx.check(lib.gf_deriv(prob.handle, A.GF_F64, A.ptr(dev(u)), idir, A.ptr(du)))
+        d = host(du)
+        err = np.sqrt(o.integrate((d - exact) ** 2) / o.integrate(exact ** 2))
+        assert err < 100 * np.finfo(float).eps, (idir, err)
+
+
 @pytest.mark.parametrize("dim,ne,p", [(3, [2, 2, 3], 6), (2, [4, 3], 4)])
 def test_advect_and_dudt_match_oracle(ctx, dim, ne, p):
     g, prob, o = setup(ctx, dim, ne, p, [1] * dim, mask=False)
@@ -414,3 +430,28 @@ def test_filter_through_tensor_apply_keeps_low_modes(ctx):
     v = np.tile(np.tile(top, n * n), g.nelems)
     tensor_apply(prob, F, F, F, dev(v), out)
     assert relerr(host(out), lam[n - 1] * v) < 1e-12
+
+
+@pytest.mark.parametrize("scheme,order", [(A.GF_RK4, 4), (A.GF_SSP33, 3), (A.GF_RK2, 2)])
+def test_rk_temporal_order_on_advected_wave(ctx, scheme, order):
+    """gtest_rk.cpp's check of the RK order, on the device stepper: a
+    periodic 2-d wave advected by a constant velocity, stepped to T with n
+    and 2n steps and compared with the same discretisation stepped 64 times
+    finer, so that only the temporal error is left: halving dt divides it
+    by about 2^order."""
+    from geoflow_b200 import GBurgers
+    g, prob, o = setup(ctx, 2, [4, 4], 4, [1, 1], mask=False)
+    x, y = g.xyz[0], g.xyz[1]
+    T = 0.1
+    u0 = np.sin(2 * np.pi * x) * np.sin(2 * np.pi * y)
+    c = [dev(np.full(g.ndof(), 1.0)), dev(np.full(g.ndof(), 0.5))]
+
+    def run(n):
+        u = [dev(u0)]
+        GBurgers(prob, GBurgers.ADVECT, 0.0, scheme=scheme).step(u, c, dt=T / n, nsteps=n)
+        return host(u[0])
+
+    ref = run(640)
+    errs = [float(np.max(np.abs(run(n) - ref))) for n in (10, 20)]
+    rate = np.log2(errs[0] / errs[1])
+    assert abs(rate - order) < 0.35, (errs, rate)
