@@ -290,7 +290,7 @@ def pmg_launches_per_iteration(m):
     the first post-smoothing term and m more steps, each step after an
     apply; plus the outer FP64 apply."""
     return {"apply_fp64": 1, "apply_vcycle": 2 * m + 2, "smoother_step": 2 * m + 1,
-            "residual": 1}
+            "residual": 1, "restrict": 1, "prolong": 1}
 
 
 def pmg_kernel_roofline(ctx, prob, traits, peaks, reps=10):
@@ -313,11 +313,19 @@ def pmg_kernel_roofline(ctx, prob, traits, peaks, reps=10):
               "gf_pmg_launch")
     nL, nE, ne, dim = g.nclass, prob.nlocal, g.nelems, g.dim
     sm = 8 if traits.precond == A.GF_PRECOND_PMG64 else 4
+    # the next level: order ceil(p/2) on the same elements (its lattice and
+    # its element-local size)
+    pc = (g.p + 1) // 2
+    nLc = int(np.prod([g.ne[d] * pc + (0 if g.periodic[d] else 1) for d in range(dim)]))
+    nEc = ne * (pc + 1) ** dim
     kinds = {
         "apply_fp64": (A.GF_PMG_APPLY64, nL * 8 + nE * 8 + ne * (dim + 1) * 8),
         "apply_vcycle": (A.GF_PMG_APPLY, nL * sm + nE * sm + ne * (dim + 1) * sm),
         "smoother_step": (A.GF_PMG_STEP, nE * sm + 6 * nL * sm + nL),
         "residual": (A.GF_PMG_RESID, nE * sm + 2 * nL * sm + nL),
+        # fine residual in, coarse E-vector out; coarse x in, fine x updated
+        "restrict": (A.GF_PMG_RESTRICT, nL * sm + nEc * sm),
+        "prolong": (A.GF_PMG_PROLONG, nLc * sm + 2 * nL * sm),
     }
     hbm = peaks.get("hbm_gbs") or 6650.0
     out = {}
@@ -1148,6 +1156,8 @@ def main():
                  "residual": f"k_mg_pass_lat<{args.p + 1},MG_RESID,{tname}> (finest-level "
                              "residual pass)",
                  "apply_fp64": f"k_helm3d_k1<double,{args.p + 1},LoadBox> (outer FP64 apply)",
+                 "restrict": f"k_pxfer_restrict<{args.p + 1},{tname}> (finest-level restriction)",
+                 "prolong": f"k_pxfer_prolong<{args.p + 1},{tname}> (finest-level prolongation)",
                  }[top]
         prof = f"mg_pass_{top}_{'f32' if path == 'pmg' else 'f64'}_{args.ne}cube_p{args.p}"
     else:

@@ -28,6 +28,7 @@ GF_PRECOND_NONE, GF_PRECOND_JACOBI, GF_PRECOND_CHEBYSHEV, GF_PRECOND_PMG, GF_PRE
     0, 1, 2, 3, 4)
 GF_CG_FP64, GF_CG_MIXED = 0, 1
 GF_PMG_PREPARE, GF_PMG_APPLY64, GF_PMG_APPLY, GF_PMG_STEP, GF_PMG_RESID = 0, 1, 2, 3, 4
+GF_PMG_RESTRICT, GF_PMG_PROLONG = 5, 6
 GF_GEOM_AFFINE, GF_GEOM_REGULAR, GF_GEOM_DEFORMED, GF_GEOM_EMBEDDED = 0, 1, 2, 3
 GF_EQN_ADVECT, GF_EQN_BURGERS, GF_EQN_HEAT = 0, 1, 2
 GF_FILTER_BOYD, GF_FILTER_PROJECTION = 0, 1

@@ -904,63 +904,112 @@ __device__ __forceinline__ int elem_lattice(const BoxLattice &L, int c0, int c1,
   return g0 + M0 * (g1 + M1 * g2);
 }
 
+// The element-wise transfers are sum-factorised one line per thread: each
+// stage contracts one direction, a thread taking a whole line of the
+// previous stage from shared memory (rows padded to an odd stride, so the
+// lines of a warp fall in distinct banks) and the 1-d weights J(r, a) as
+// compile-time operands of the kernel parameter.  Every output is the
+// same fma chain from 0 in ascending index as a staged loop would form.
+template <int K>
+struct PadOdd {
+  static constexpr int value = (K % 2) ? K : K + 1;
+};
+
 // prolongation x_f += P x_c: gather the coarse element, contract along x,
-// y, z in shared memory, add into the fine lattice points the element owns
-// (local index < P, or P on a non-periodic upper face), so each point is
-// written once.
+// y, z, add into the fine lattice points the element owns (local index < P,
+// or P on a non-periodic upper face), so each point is written once.
 template <int NF, typename TM>
 __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF * NF)))
     k_pxfer_prolong(BoxLattice Lf, BoxLattice Lc, const __grid_constant__ Xfer1D<TM> T,
                     const TM *__restrict__ xc, TM *__restrict__ xf, const double *stop) {
   constexpr int NC = NF / 2 + 1, PF = NF - 1, NT = NF * NF;
   constexpr int EPB = (256 / NT) < 1 ? 1 : 256 / NT;
-  constexpr int S0 = NC * NC * NC, S1 = NF * NC * NC, S2 = NF * NF * NC;
-  __shared__ TM J[NF * NC];
+  constexpr int CP = PadOdd<NC>::value;
+  // s0[c][b][a] (rows of CP), s1[(c NF + i0) CP + b], s2[(j NF + i0) CP + c]
+  constexpr int S0 = NC * NC * CP, S1 = NC * NF * CP, S2 = NF * NF * CP;
   __shared__ TM sm[EPB][S0 + S1 + S2];
   if (stop && *stop != 0.0) return;
   const int t = threadIdx.x, slot = threadIdx.y;
-  for (int i = t + NT * slot; i < NF * NC; i += NT * EPB) J[i] = T.J[i];
   const int ne0 = Lf.ne[0], ne1 = Lf.ne[1], ne2 = Lf.ne[2];
   const int nel = ne0 * ne1 * ne2;
   const int e = blockIdx.x * EPB + slot;
   const bool active = e < nel;
-  const int c0 = e % ne0, r = e / ne0, c1 = r % ne1, c2 = r / ne1;
+  const int r = e / ne0, c0 = e - r * ne0, c2 = r / ne1, c1 = r - c2 * ne1;
   TM *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
-  if (active)
-    for (int i = t; i < S0; i += NT) {
-      const int a = i % NC, b = (i / NC) % NC, c = i / (NC * NC);
-      s0[i] = xc[elem_lattice(Lc, c0, c1, c2, a, b, c)];
+  if (active && t < NC * NC) {  // the coarse element, one z-line (a, b) per thread
+    const int a = t % NC, b = t / NC, Pc = Lc.p;
+    const int M0 = (int)Lc.M[0], M1 = (int)Lc.M[1], M2 = (int)Lc.M[2];
+    int g0 = c0 * Pc + a, g1 = c1 * Pc + b;
+    if (Lc.per[0] && g0 == M0) g0 = 0;
+    if (Lc.per[1] && g1 == M1) g1 = 0;
+    const TM *row = xc + g0 + M0 * g1;
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      int g2 = c2 * Pc + c;
+      if (Lc.per[2] && g2 == M2) g2 = 0;
+      s0[(c * NC + b) * CP + a] = row[(int64_t)M0 * M1 * g2];
     }
+  }
   __syncthreads();
-  if (active)
-    for (int i = t; i < S1; i += NT) {  // s1[c][b][i0] = sum_a J[i0][a] s0[c][b][a]
-      const int i0 = i % NF, cb = i / NF;
+  if (active && t < NC * NC) {  // x: line (b, c) -> s1[c][i0][b]
+    const int b = t % NC, c = t / NC;
+    TM in[NC];
+#pragma unroll
+    for (int a = 0; a < NC; a++) in[a] = s0[(c * NC + b) * CP + a];
+#pragma unroll
+    for (int i0 = 0; i0 < NF; i0++) {
       TM v = 0;
 #pragma unroll
-      for (int a = 0; a < NC; a++) v = mg_fma(J[i0 * NC + a], s0[cb * NC + a], v);
-      s1[i] = v;
+      for (int a = 0; a < NC; a++) v = mg_fma(T.J[i0 * NC + a], in[a], v);
+      s1[(c * NF + i0) * CP + b] = v;
     }
+  }
   __syncthreads();
-  if (active)
-    for (int i = t; i < S2; i += NT) {  // s2[c][j][i0] = sum_b J[j][b] s1[c][b][i0]
-      const int i0 = i % NF, j = (i / NF) % NF, c = i / (NF * NF);
+  if (active && t < NC * NF) {  // y: line (i0, c) -> s2[j][i0][c]
+    const int i0 = t % NF, c = t / NF;
+    TM in[NC];
+#pragma unroll
+    for (int b = 0; b < NC; b++) in[b] = s1[(c * NF + i0) * CP + b];
+#pragma unroll
+    for (int j = 0; j < NF; j++) {
       TM v = 0;
 #pragma unroll
-      for (int b = 0; b < NC; b++) v = mg_fma(J[j * NC + b], s1[(c * NC + b) * NF + i0], v);
-      s2[i] = v;
+      for (int b = 0; b < NC; b++) v = mg_fma(T.J[j * NC + b], in[b], v);
+      s2[(j * NF + i0) * CP + c] = v;
     }
+  }
   __syncthreads();
   if (!active) return;
-  const int i0 = t % NF, j = t / NF;
+  const int i0 = t % NF, j = t / NF;  // z: line (i0, j)
   if (i0 == PF && (Lf.per[0] || c0 != ne0 - 1)) return;
   if (j == PF && (Lf.per[1] || c1 != ne1 - 1)) return;
+  TM in[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) in[c] = s2[(j * NF + i0) * CP + c];
+  const int M0 = (int)Lf.M[0], M1 = (int)Lf.M[1], M2 = (int)Lf.M[2];
+  int g0 = c0 * PF + i0, g1 = c1 * PF + j;
+  if (Lf.per[0] && g0 == M0) g0 = 0;
+  if (Lf.per[1] && g1 == M1) g1 = 0;
+  TM *row = xf + g0 + M0 * g1;
+  // the line's current values first (all loads in flight together), then
+  // x += P x_c point by point
+  const bool top = !Lf.per[2] && c2 == ne2 - 1;  // owns its k = P points
+  int64_t off[NF];
+  TM old[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    if (k == PF && (Lf.per[2] || c2 != ne2 - 1)) continue;
+    int g2 = c2 * PF + k;
+    if (Lf.per[2] && g2 == M2) g2 = 0;
+    off[k] = (int64_t)M0 * M1 * g2;
+    old[k] = (k < PF || top) ? row[off[k]] : TM(0);
+  }
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    if (k == PF && !top) continue;
     TM v = 0;
 #pragma unroll
-    for (int c = 0; c < NC; c++) v = mg_fma(J[k * NC + c], s2[(c * NF + j) * NF + i0], v);
-    xf[elem_lattice(Lf, c0, c1, c2, i0, j, k)] += v;
+    for (int c = 0; c < NC; c++) v = mg_fma(T.J[k * NC + c], in[c], v);
+    row[off[k]] = old[k] + v;
   }
 }
 
@@ -973,56 +1022,84 @@ __global__ void __launch_bounds__(NF *NF *((256 / (NF * NF)) < 1 ? 1 : 256 / (NF
                      const TM *__restrict__ rf, TM *__restrict__ qc, const double *stop) {
   constexpr int NC = NF / 2 + 1, PF = NF - 1, NT = NF * NF;
   constexpr int EPB = (256 / NT) < 1 ? 1 : 256 / NT;
-  constexpr int S0 = NF * NF * NF, S1 = NC * NF * NF, S2 = NC * NC * NF;
-  __shared__ TM J[NF * NC];
+  constexpr int FP = PadOdd<NF>::value;
+  // s0[k][j][i0] (rows of FP), s1[(k NC + a) FP + j], s2[(b NC + a) FP + k]
+  constexpr int S0 = NF * NF * FP, S1 = NF * NC * FP, S2 = NC * NC * FP;
   __shared__ TM sm[EPB][S0 + S1 + S2];
   if (stop && *stop != 0.0) return;
   const int t = threadIdx.x, slot = threadIdx.y;
-  for (int i = t + NT * slot; i < NF * NC; i += NT * EPB) J[i] = T.J[i];
   const int ne[3] = {Lf.ne[0], Lf.ne[1], Lf.ne[2]};
   const int nel = ne[0] * ne[1] * ne[2];
   const int e = blockIdx.x * EPB + slot;
   const bool active = e < nel;
-  const int cc[3] = {e % ne[0], (e / ne[0]) % ne[1], e / (ne[0] * ne[1])};
+  const int r = e / ne[0], q = r / ne[1];
+  const int cc[3] = {e - r * ne[0], r - q * ne[1], q};
   TM *s0 = sm[slot], *s1 = s0 + S0, *s2 = s1 + S1;
-  if (active)
-    for (int i = t; i < S0; i += NT) {
-      const int l[3] = {i % NF, (i / NF) % NF, i / (NF * NF)};
-      TM w = 1;
+  if (active) {
+    // the element's fine points, one z-line (l0, l1) per thread, each
+    // weighted by 1/2 per direction in which the point is shared (an exact
+    // power of two)
+    const int l0 = t % NF, l1 = t / NF;
+    const int M0 = (int)Lf.M[0], M1 = (int)Lf.M[1], M2 = (int)Lf.M[2];
+    auto shared = [&](int l, int d) {
+      return (l == 0 && (Lf.per[d] || cc[d] > 0)) || (l == PF && (Lf.per[d] || cc[d] < ne[d] - 1));
+    };
+    TM wxy = 1;
+    if (shared(l0, 0)) wxy *= TM(0.5);
+    if (shared(l1, 1)) wxy *= TM(0.5);
+    int g0 = cc[0] * PF + l0, g1 = cc[1] * PF + l1;
+    if (Lf.per[0] && g0 == M0) g0 = 0;
+    if (Lf.per[1] && g1 == M1) g1 = 0;
+    const TM *row = rf + g0 + M0 * g1;
 #pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const bool shared = (l[d] == 0 && (Lf.per[d] || cc[d] > 0)) ||
-                            (l[d] == PF && (Lf.per[d] || cc[d] < ne[d] - 1));
-        if (shared) w *= TM(0.5);
-      }
-      s0[i] = w * rf[elem_lattice(Lf, cc[0], cc[1], cc[2], l[0], l[1], l[2])];
+    for (int l2 = 0; l2 < NF; l2++) {
+      TM w = wxy;
+      if (shared(l2, 2)) w *= TM(0.5);
+      int g2 = cc[2] * PF + l2;
+      if (Lf.per[2] && g2 == M2) g2 = 0;
+      s0[(l2 * NF + l1) * FP + l0] = w * row[(int64_t)M0 * M1 * g2];
     }
+  }
   __syncthreads();
-  if (active)
-    for (int i = t; i < S1; i += NT) {  // s1[k][j][a] = sum_i0 J[i0][a] s0[k][j][i0]
-      const int a = i % NC, kj = i / NC;
+  if (active) {  // x: line (j, k) -> s1[k][a][j]
+    const int j = t % NF, k = t / NF;
+    TM in[NF];
+#pragma unroll
+    for (int i0 = 0; i0 < NF; i0++) in[i0] = s0[(k * NF + j) * FP + i0];
+#pragma unroll
+    for (int a = 0; a < NC; a++) {
       TM v = 0;
 #pragma unroll
-      for (int i0 = 0; i0 < NF; i0++) v = mg_fma(J[i0 * NC + a], s0[kj * NF + i0], v);
-      s1[i] = v;
+      for (int i0 = 0; i0 < NF; i0++) v = mg_fma(T.J[i0 * NC + a], in[i0], v);
+      s1[(k * NC + a) * FP + j] = v;
     }
+  }
   __syncthreads();
-  if (active)
-    for (int i = t; i < S2; i += NT) {  // s2[k][b][a] = sum_j J[j][b] s1[k][j][a]
-      const int a = i % NC, b = (i / NC) % NC, k = i / (NC * NC);
+  if (active && t < NF * NC) {  // y: line (a, k) -> s2[b][a][k]
+    const int a = t % NC, k = t / NC;
+    TM in[NF];
+#pragma unroll
+    for (int j = 0; j < NF; j++) in[j] = s1[(k * NC + a) * FP + j];
+#pragma unroll
+    for (int b = 0; b < NC; b++) {
       TM v = 0;
 #pragma unroll
-      for (int j = 0; j < NF; j++) v = mg_fma(J[j * NC + b], s1[(k * NF + j) * NC + a], v);
-      s2[i] = v;
+      for (int j = 0; j < NF; j++) v = mg_fma(T.J[j * NC + b], in[j], v);
+      s2[(b * NC + a) * FP + k] = v;
     }
+  }
   __syncthreads();
-  if (!active) return;
-  for (int i = t; i < NC * NC * NC; i += NT) {  // q[c][b][a] = sum_k J[k][c] s2[k][b][a]
-    const int ab = i % (NC * NC), c = i / (NC * NC);
+  if (!active || t >= NC * NC) return;
+  const int a = t % NC, b = t / NC;  // z: line (a, b) -> q[c][b][a]
+  TM in[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) in[k] = s2[(b * NC + a) * FP + k];
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
     TM v = 0;
 #pragma unroll
-    for (int k = 0; k < NF; k++) v = mg_fma(J[k * NC + c], s2[k * NC * NC + ab], v);
-    qc[(int64_t)e * (NC * NC * NC) + i] = v;
+    for (int k = 0; k < NF; k++) v = mg_fma(T.J[k * NC + c], in[k], v);
+    qc[(int64_t)e * (NC * NC * NC) + (c * NC + b) * NC + a] = v;
   }
 }
 
@@ -2537,6 +2614,8 @@ struct PMGLaunch {
       TM *const vecs[4] = {L.b, L.x, L.d, L.res};
       for (TM *v : vecs) GF_CUDA(ctx, cudaMemsetAsync(v, 0x3c, sizeof(TM) * L.nL, st));
       GF_CUDA(ctx, cudaMemsetAsync(L.qE, 0x3c, sizeof(TM) * L.nE, st));
+      if (H->lv.size() > 1)  // the next level's x, read by the prolongation
+        GF_CUDA(ctx, cudaMemsetAsync(H->lv[1]->x, 0x3c, sizeof(TM) * H->lv[1]->nL, st));
       double *xL = (double *)gf_work(prob, 1, sizeof(double) * S.nL);
       double *qE = (double *)gf_work(prob, 3, sizeof(double) * S.nE);
       if (!xL || !qE) return gf_fail(ctx, GF_ERR_NOMEM, "work allocation failed");
@@ -2555,8 +2634,18 @@ struct PMGLaunch {
       rc = L.apply(L.x, p, q, use_mass, stop, st);
     } else if (which == GF_PMG_STEP) {
       L.pass(MG_STEP, false, L.c1.size() > 1 ? L.c1[1] : TM(0), L.c0, DP_D, 1, prob, st);
-    } else {
+    } else if (which == GF_PMG_RESID) {
       L.pass(MG_RESID, false, TM(0), TM(0), DP_NONE, 0, prob, st);
+    } else {  // transfers between the finest level and the next
+      if (H->lv.size() < 2) return gf_fail(ctx, GF_ERR_ARG, "the hierarchy has one level");
+      MGLevelBase<TM> &C = *H->lv[1];
+      if (which == GF_PMG_RESTRICT) {
+        if (L.ptransfer) L.restrict_elem(C, prob, st);
+        else mg_restrict(L, C, prob, st);
+      } else {
+        if (L.ptransfer) L.prolong_elem(C, prob, st);
+        else mg_prolong(L, C, prob, st);
+      }
     }
     if (rc) return gf_fail(ctx, rc, "launch failed");
     GF_CHECK_LAUNCH(ctx);
@@ -2584,7 +2673,7 @@ extern "C" int gf_pmg_launch(gf_problem_t prob, const gf_cg_traits *tr, double p
   gf_context *ctx = prob->ctx;
   GF_REQUIRE(ctx, tr->precond == GF_PRECOND_PMG || tr->precond == GF_PRECOND_PMG64,
              "traits must name GF_PRECOND_PMG or GF_PRECOND_PMG64");
-  GF_REQUIRE(ctx, which >= GF_PMG_PREPARE && which <= GF_PMG_RESID, "bad kernel selector");
+  GF_REQUIRE(ctx, which >= GF_PMG_PREPARE && which <= GF_PMG_PROLONG, "bad kernel selector");
   GF_REQUIRE(ctx, prob->has_box, "PMG needs a structured box (box_ne)");
   GF_CUDA(ctx, cudaSetDevice(ctx->device));
   if (which != GF_PMG_PREPARE) {

@@ -312,9 +312,18 @@ int gf_cg_solve_host(gf_problem_t prob, const gf_cg_traits *traits, double p, do
  * GF_PMG_APPLY64 the outer FP64 lattice -> element apply; GF_PMG_APPLY the
  * V-cycle's lattice -> element apply (FP32 or FP64); GF_PMG_STEP a
  * smoother step pass (fold, residual, x and d update); GF_PMG_RESID the
- * residual pass.  Overwrites the hierarchy's vectors and the problem's CG
+ * residual pass; GF_PMG_RESTRICT / GF_PMG_PROLONG the transfers between the
+ * finest level and the next.  Overwrites the hierarchy's vectors and the problem's CG
  * work vectors.  Not a reference interface (measurement only). */
-enum { GF_PMG_PREPARE = 0, GF_PMG_APPLY64 = 1, GF_PMG_APPLY = 2, GF_PMG_STEP = 3, GF_PMG_RESID = 4 };
+enum {
+  GF_PMG_PREPARE = 0,
+  GF_PMG_APPLY64 = 1,
+  GF_PMG_APPLY = 2,
+  GF_PMG_STEP = 3,
+  GF_PMG_RESID = 4,
+  GF_PMG_RESTRICT = 5,
+  GF_PMG_PROLONG = 6
+};
 int gf_pmg_launch(gf_problem_t prob, const gf_cg_traits *traits, double p, double q, int use_mass,
                   int masked, int which);
 

@@ -215,7 +215,7 @@ def test_pmg_launch_single_kernels(ctx, pc):
     x1 = prob.zeros()
     assert cg.solve(H, b, 0 * b, x1) == 0
     for which in (A.GF_PMG_PREPARE, A.GF_PMG_APPLY64, A.GF_PMG_APPLY, A.GF_PMG_STEP,
-                  A.GF_PMG_RESID):
+                  A.GF_PMG_RESID, A.GF_PMG_RESTRICT, A.GF_PMG_PROLONG):
         assert lib.gf_pmg_launch(prob.handle, C.byref(trc), 1.0, 1.0, 1, 1, which) == 0
     x2 = prob.zeros()
     assert cg.solve(H, b, 0 * b, x2) == 0
