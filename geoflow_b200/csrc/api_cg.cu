@@ -891,18 +891,9 @@ __global__ void k_xfer1d(int64_t nout, int d, int eo0, int eo1, int ei0, int ei1
 // ---- transfers between p-levels (same elements), one element per
 // thread-block slot: with P = J (x) J (x) J element by element (J the
 // NF x NC interpolation of Xfer1D with ratio 1), no 1-d sweeps and no
-// intermediate lattices.  3-d box lattices.
-//
-// lattice index of local point (l0, l1, l2) of the element at (c0, c1, c2)
-__device__ __forceinline__ int elem_lattice(const BoxLattice &L, int c0, int c1, int c2, int l0,
-                                            int l1, int l2) {
-  const int P = L.p, M0 = (int)L.M[0], M1 = (int)L.M[1], M2 = (int)L.M[2];
-  int g0 = c0 * P + l0, g1 = c1 * P + l1, g2 = c2 * P + l2;
-  if (L.per[0] && g0 == M0) g0 = 0;
-  if (L.per[1] && g1 == M1) g1 = 0;
-  if (L.per[2] && g2 == M2) g2 = 0;
-  return g0 + M0 * (g1 + M1 * g2);
-}
+// intermediate lattices.  3-d box lattices.  The lattice coordinate of
+// local index l in element coordinate c along a direction is c P + l,
+// wrapped to 0 at M when the direction is periodic.
 
 // The element-wise transfers are sum-factorised one line per thread: each
 // stage contracts one direction, a thread taking a whole line of the
