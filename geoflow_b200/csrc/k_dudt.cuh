@@ -55,7 +55,7 @@ template <typename T, int N, int NF> constexpr int dudt_slot() {
 // AFF: affine elements (g.egeom), known at compile time, so the per-node
 // geometry path (node indices and loads) is not compiled in.
 template <typename T, int N, int EPB, int EQN, int MODE, bool AFF>
-__global__ void __launch_bounds__(N *N *EPB)
+__global__ void __launch_bounds__(N *N *EPB, (sizeof(T) == 4 && MODE != MODE_EULER) ? 6 : 0)
     k_dudt3d(const __grid_constant__ Basis<T, N> B, const Geom<T> g, int64_t ne, T nu,
              const T *__restrict__ f0, const T *__restrict__ f1, const T *__restrict__ f2,
              const T *__restrict__ f3, const T *__restrict__ imass, T *__restrict__ o0,
@@ -77,13 +77,33 @@ __global__ void __launch_bounds__(N *N *EPB)
   eg.X[0] = eg.X[1] = eg.X[2] = eg.J = T(0);
   if (active) elem_geom<T, 3>(g, e, eg);
 
+  // FP32 without the update epilogue: each thread keeps the fields of its
+  // own z-column (i = a0, j = a1) in registers, read by the z-line and the
+  // advection term instead of from shared memory (the kernel is bound by its
+  // shared-memory pipe; 64 registers, 6 blocks per SM: the right-hand side
+  // at 64^3 p = 5 0.748 -> 0.633 ms).  With the epilogue the extra registers
+  // cost more occupancy than they save (stage 1.72 -> 1.89 ms).
+  constexpr bool CREG = sizeof(T) == 4 && MODE != MODE_EULER;
+  T fr[CREG ? NF : 1][N];
 #pragma unroll
   for (int f = 0; f < NF; f++) {
 #pragma unroll
-    for (int k = 0; k < N; k++)
-      s[f * VOL + k * PLANE + a1 * P + a0] = active ? fin[f][base + k * NN + t] : T(0);
+    for (int k = 0; k < N; k++) {
+      const T v = active ? fin[f][base + k * NN + t] : T(0);
+      if (CREG) fr[CREG ? f : 0][k] = v;
+      s[f * VOL + k * PLANE + a1 * P + a0] = v;
+    }
   }
   __syncthreads();
+  // field f of this thread's column at level k (registers in FP32)
+  auto col = [&](int f, int k, int sidx) -> T {
+    if constexpr (CREG) {
+      return f == 0 ? fr[0][k] : (f == 1 ? fr[NF > 1 ? 1 : 0][k]
+                                         : (f == 2 ? fr[NF > 2 ? 2 : 0][k] : fr[NF > 3 ? 3 : 0][k]));
+    } else {
+      return s[f * VOL + sidx];
+    }
+  };
 
 #pragma unroll 1
   for (int c = 0; c < NC; c++) {
@@ -112,7 +132,7 @@ __global__ void __launch_bounds__(N *N *EPB)
     {
       T a[N];
 #pragma unroll
-      for (int m = 0; m < N; m++) a[m] = su[m * PLANE + a1 * P + a0];
+      for (int m = 0; m < N; m++) a[m] = col(c, m, m * PLANE + a1 * P + a0);
       line_D<T, N>(B.D, a, rz);
     }
     __syncthreads();
@@ -126,9 +146,9 @@ __global__ void __launch_bounds__(N *N *EPB)
         const T mass = B.W[k] * B.W[j] * B.W[i] * ng.J;
         if (EQN != GF_EQN_HEAT) {
           const int cb = EQN == GF_EQN_ADVECT ? 1 : 0;
-          T po = (sdx[sidx] * ng.X[0]) * s[(cb + 0) * VOL + sidx];
-          po += (sdy[sidx] * ng.X[1]) * s[(cb + 1) * VOL + sidx];
-          po += (rz[k] * ng.X[2]) * s[(cb + 2) * VOL + sidx];
+          T po = (sdx[sidx] * ng.X[0]) * col(cb + 0, k, sidx);
+          po += (sdy[sidx] * ng.X[1]) * col(cb + 1, k, sidx);
+          po += (rz[k] * ng.X[2]) * col(cb + 2, k, sidx);
           radv[k] = po * mass;
         } else {
           radv[k] = T(0);
@@ -194,7 +214,7 @@ __global__ void __launch_bounds__(N *N *EPB)
             const T *ui = c == 0 ? epi.uin[0] : (c == 1 ? epi.uin[1] : epi.uin[2]);
             const T *yc = c == 0 ? epi.y[0] : (c == 1 ? epi.y[1] : epi.y[2]);
             const T *y2c = c == 0 ? epi.y2[0] : (c == 1 ? epi.y2[1] : epi.y2[2]);
-            const T uv = epi.uin_is_u ? su[sidx] : ui[node];
+            const T uv = epi.uin_is_u ? col(c, k, sidx) : ui[node];
             oc[node] = rk_euler_point(K, epi.dt, uv, epi.a, yc, epi.b, epi.a2, y2c, epi.b2,
                                            node);
           } else {
