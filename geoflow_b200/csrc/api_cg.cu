@@ -793,7 +793,7 @@ __global__ void k_invert(int64_t n, const double *__restrict__ d, double *__rest
   }
 }
 
-// ---- multigrid preconditioner kernels (FP32, lattice L-vectors) ----
+// ---- multigrid preconditioner kernels (FP32 or FP64, lattice L-vectors) ----
 // Transfers between the lattices of two levels are tensor products of 1-d
 // operators, P = P_z (x) P_y (x) P_x: a fine lattice point takes the
 // coarse element's GLL interpolant at its position, and the restriction
@@ -1121,8 +1121,9 @@ __global__ void k_mg_start(int64_t nL, const double *__restrict__ r64, TM *__res
 //   MG_START  qE = a coarse E-vector (the element restriction's output):
 //             b = s; x = a1 Dinv b         (smoothing from zero)
 //   MG_FOLDB  b = s only (a dense coarsest level)
-// DOTS (last pass of the finest level): <b, x> (b = the FP32 copy of the
-// outer residual) for the CG step, finished by fcg_finish_fr.
+// DOTS (last pass of the finest level): <b, x> (b = the copy of the outer
+// residual in the multigrid's type) for the CG step, finished by
+// fcg_finish_fr.
 // Applying x rather than the step direction keeps the running residual out
 // of the smoother state: a step reads b, dinv, x (and d) and writes x (and
 // d); mathematically the same Chebyshev polynomial.
@@ -1718,7 +1719,7 @@ struct Solver {
 // operator rediscretised (GLL quadrature of its order, element geometry
 // merged under h-coarsening), held as a light gf_problem: basis, K1,
 // element geometry and box lattice, no gather-scatter arrays.  One V-cycle
-// in FP32 on the lattice (unique-node) vectors:
+// in FP32 (or FP64, GF_PRECOND_PMG64) on the lattice (unique-node) vectors:
 //   x = S b;  r = b - A x;  x_c = V(R r);  x += P x_c;  x += S (b - A x)
 // S = Chebyshev-Jacobi polynomial of degree m on [lmax/ratio, 1.1 lmax]
 // (the same polynomial before and after, so the cycle is symmetric), R =
